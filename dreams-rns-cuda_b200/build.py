@@ -1,0 +1,87 @@
+"""Build libdreams_b200.so (sm_100a) in-tree.
+
+    python dreams-rns-cuda_b200/build.py [--force] [--jobs N]
+
+Each translation unit under csrc/ is compiled by nvcc in parallel into
+_build/, then linked into dreams_rns/_native/libdreams_b200.so (the CUDA
+runtime is linked statically, so the library only needs the driver).
+Rebuilds a unit when it or any header in csrc/ or include/ is newer than its
+object file.
+"""
+
+from __future__ import annotations
+
+import argparse
+import glob
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+SRC = os.path.join(HERE, "csrc")
+OBJ = os.path.join(HERE, "_build")
+OUT_DIR = os.path.join(HERE, "dreams_rns", "_native")
+LIB = os.path.join(OUT_DIR, "libdreams_b200.so")
+
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+          "-I", os.path.join(REPO, "include"), "-I", SRC]
+
+
+def _headers():
+    return (glob.glob(os.path.join(SRC, "*.h")) + glob.glob(os.path.join(SRC, "*.cuh")) +
+            glob.glob(os.path.join(REPO, "include", "*.h")))
+
+
+def _units():
+    return sorted(glob.glob(os.path.join(SRC, "*.cu")) + glob.glob(os.path.join(SRC, "*.cpp")))
+
+
+def _compile(src: str, force: bool, verbose_ptxas: bool) -> str:
+    obj = os.path.join(OBJ, os.path.basename(src) + ".o")
+    newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in _headers()])
+    if not force and os.path.exists(obj) and os.path.getmtime(obj) >= newest:
+        return obj
+    cmd = [NVCC] + ARCH + COMMON
+    if verbose_ptxas and src.endswith(".cu"):
+        cmd += ["-Xptxas", "-v"]
+    cmd += ["-c", src, "-o", obj + ".tmp"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError(f"nvcc failed for {os.path.basename(src)}")
+    if verbose_ptxas:
+        with open(obj + ".ptxas.txt", "w") as f:
+            f.write(res.stderr)
+    os.replace(obj + ".tmp", obj)
+    return obj
+
+
+def build(force: bool = False, jobs: int = 0, verbose_ptxas: bool = False) -> str:
+    os.makedirs(OBJ, exist_ok=True)
+    os.makedirs(OUT_DIR, exist_ok=True)
+    units = _units()
+    jobs = jobs or min(len(units), os.cpu_count() or 4)
+    with ThreadPoolExecutor(max_workers=jobs) as ex:
+        objs = list(ex.map(lambda s: _compile(s, force, verbose_ptxas), units))
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-cudart", "static",
+                               "-o", LIB + ".tmp"] + objs + ["-lpthread"]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+            raise RuntimeError("link failed")
+        os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--jobs", type=int, default=0)
+    ap.add_argument("--ptxas", action="store_true", help="keep -Xptxas -v reports next to objects")
+    a = ap.parse_args()
+    print(build(a.force, a.jobs, a.ptxas))

@@ -1,0 +1,250 @@
+// Garner CRT to exact 32-bit limbs (reference runner.py:105-129).
+//
+// The reference's iterative CRT adds one mixed-radix digit per modulus:
+//     t_i = (a_i - x mod p_i) * inv(M_i mod p_i) mod p_i,  x += M_i t_i,
+// with M_i = p_0 ... p_{i-1}, x starting at the raw first residue and
+// inv(v) = v^(p-2) mod p (0 when p | M_i).  One warp handles one value:
+//   1. digits: for i = 1..K-1 the lane owning modulus i computes t_i and
+//      broadcasts it; every lane folds t_i into the running x mod p_j of its
+//      own moduli j > i -- K sequential steps, K/32 mulmods each per lane;
+//   2. binary: limb l of x = sum_i t_i * M_i[l] (the M_i limbs are built once
+//      per moduli set), lane-parallel over limbs, then one carry pass;
+//   3. centring x - M if x > M // 2 (runner.py:127-129) to sign + magnitude.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "launch.h"
+#include "modarith.cuh"
+
+namespace dr {
+
+__device__ __forceinline__ Mont mont_of(uint32_t p, uint32_t pinv, uint32_t r2) {
+    Mont M;
+    M.p = p;
+    M.pinv = pinv;
+    M.r2 = r2;
+    M.one = 0;
+    M.one = mmul(r2, 1u, M);
+    return M;
+}
+
+// Per moduli set: Montgomery constants, Garner inverses and the M_i limbs.
+// Thread j handles modulus j; thread 0 builds the limb table.  Setup work,
+// run once per moduli set and cached by the host.
+__global__ void k_crt_setup(const uint32_t* moduli, int K, int L, uint32_t* pinv, uint32_t* r2,
+                            uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal) {
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+        const uint32_t p = moduli[j];
+        uint32_t x = p;
+        for (int it = 0; it < 5; ++it) x *= 2u - p * x;   // Newton: p^-1 mod 2^32
+        const uint32_t pi = 0u - x;
+        const uint64_t r1 = (1ull << 32) % p;
+        const uint32_t rr = (uint32_t)((r1 * r1) % p);
+        pinv[j] = pi;
+        r2[j] = rr;
+        const Mont M = mont_of(p, pi, rr);
+        uint32_t acc = M.one;  // prod_{i<j} p_i mod p_j
+        for (int i = 0; i < j; ++i) acc = mmul(acc, mmul(moduli[i] % p, rr, M), M);
+        ginv[j] = minv_any(acc, M);
+    }
+    if (threadIdx.x == 0) {
+        for (int l = 0; l < L; ++l) Mlimbs[l] = 0u;
+        Mlimbs[0] = 1u;
+        for (int i = 1; i <= K; ++i) {
+            const uint32_t* prev = Mlimbs + (size_t)(i - 1) * L;
+            uint32_t* cur = (i < K) ? Mlimbs + (size_t)i * L : Mtotal;
+            uint64_t carry = 0;
+            for (int l = 0; l < L; ++l) {
+                const uint64_t t = (uint64_t)prev[l] * moduli[i - 1] + carry;
+                cur[l] = (uint32_t)t;
+                carry = t >> 32;
+            }
+        }
+    }
+}
+
+// Words of dynamic shared memory: block-wide moduli constants, then per warp
+// x[Lp] + dig[Kp] + col[2*Lp] (u64).
+__host__ __device__ inline size_t crt_block_words(int K) { return (size_t)4 * ((K + 1) & ~1); }
+__host__ __device__ inline size_t crt_warp_words(int K, int L) {
+    const size_t Lp = (size_t)((L + 1) & ~1), Kp = (size_t)((K + 1) & ~1);
+    return Lp + Kp + 4 * Lp;
+}
+
+template <int OWN>
+__global__ void __launch_bounds__(128) k_crt(const uint32_t* __restrict__ residues, int n,
+                                             CrtTables T, uint32_t* __restrict__ limbs, int stride,
+                                             int32_t* __restrict__ sign_out,
+                                             int32_t* __restrict__ nlimbs_out,
+                                             uint32_t* __restrict__ ulimbs,
+                                             const uint64_t* __restrict__ in_off,
+                                             const uint32_t* __restrict__ out_idx) {
+    extern __shared__ uint32_t csm[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int K = T.K, L = T.L;
+    const int Kp = (K + 1) & ~1, Lp = (L + 1) & ~1;
+    uint32_t* sp = csm;            // moduli
+    uint32_t* spi = sp + Kp;       // pinv
+    uint32_t* sr2 = spi + Kp;      // r2
+    uint32_t* sgi = sr2 + Kp;      // ginv
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+        sp[j] = T.moduli[j];
+        spi[j] = T.pinv[j];
+        sr2[j] = T.r2[j];
+        sgi[j] = T.ginv[j];
+    }
+    __syncthreads();
+    uint32_t* x = csm + crt_block_words(K) + (size_t)warp * crt_warp_words(K, L);
+    uint32_t* dig = x + Lp;
+    uint64_t* col = reinterpret_cast<uint64_t*>(dig + Kp);
+
+    for (int j = blockIdx.x * wpb + warp; j < n; j += gridDim.x * wpb) {
+        const uint32_t* a = residues + (in_off ? in_off[j] : (uint64_t)j * K);
+        const size_t v = out_idx ? out_idx[j] : (size_t)j;
+        const uint32_t r0 = __ldg(a);
+        uint32_t acc[OWN];  // x mod p_j, plain
+        uint32_t mi[OWN];   // M_i mod p_j, Montgomery form
+#pragma unroll
+        for (int o = 0; o < OWN; ++o) {
+            const int j = lane + 32 * o;
+            acc[o] = 0u;
+            mi[o] = 0u;
+            if (j < K) {
+                const Mont M = mont_of(sp[j], spi[j], sr2[j]);
+                acc[o] = r0 % M.p;
+                mi[o] = mmul(sp[0] % M.p, M.r2, M);
+            }
+        }
+        if (lane == 0) dig[0] = r0;
+        for (int i = 1; i < K; ++i) {
+            const int own = i & 31, oi = i >> 5;
+            uint32_t t = 0;
+#pragma unroll
+            for (int o = 0; o < OWN; ++o) {
+                if (o == oi && lane == own) {
+                    const Mont M = mont_of(sp[i], spi[i], sr2[i]);
+                    const uint32_t ai = __ldg(a + i) % M.p;
+                    // (a_i - x mod p_i) * inv(M_i mod p_i): plain x Montgomery -> plain
+                    t = mmul(subm(ai, acc[o], M.p), sgi[i], M);
+                    dig[i] = t;
+                }
+            }
+            t = __shfl_sync(0xffffffffu, t, own);
+            const uint32_t pi = sp[i];
+#pragma unroll
+            for (int o = 0; o < OWN; ++o) {
+                const int j = lane + 32 * o;
+                if (j > i && j < K) {
+                    const Mont M = mont_of(sp[j], spi[j], sr2[j]);
+                    acc[o] = addm(acc[o], mmul(t, mi[o], M), M.p);   // t < 2^31: t*mi < p*2^32
+                    mi[o] = mmul(mmul(mi[o], pi, M), M.r2, M);
+                }
+            }
+        }
+        __syncwarp();
+        for (int l = lane; l < L; l += 32) {
+            uint64_t lo = 0, hi = 0;
+            for (int i = 0; i < K; ++i) {
+                const uint64_t pr = (uint64_t)dig[i] * __ldg(T.Mlimbs + (size_t)i * L + l);
+                lo += pr;
+                hi += (lo < pr);
+            }
+            col[2 * l] = lo;
+            col[2 * l + 1] = hi;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            unsigned __int128 carry = 0;
+            for (int l = 0; l < L; ++l) {
+                const unsigned __int128 t = (((unsigned __int128)col[2 * l + 1]) << 64) + col[2 * l] + carry;
+                x[l] = (uint32_t)t;
+                carry = t >> 32;
+            }
+            // x >= M ?  and  2x > M ?  (M odd, so 2x > M <=> x > M // 2)
+            int ge = 1;
+            for (int l = L - 1; l >= 0; --l) {
+                const uint32_t mm = __ldg(T.Mtotal + l);
+                if (x[l] != mm) { ge = x[l] > mm; break; }
+            }
+            int twice_gt = (x[L - 1] >> 31) ? 1 : -1;
+            if (twice_gt < 0) {
+                twice_gt = 0;
+                for (int l = L - 1; l >= 0; --l) {
+                    const uint32_t tx = (x[l] << 1) | (l > 0 ? (x[l - 1] >> 31) : 0u);
+                    const uint32_t mm = __ldg(T.Mtotal + l);
+                    if (tx != mm) { twice_gt = tx > mm; break; }
+                }
+            }
+            if (ulimbs) {
+                uint32_t* uo = ulimbs + (size_t)v * stride;
+                for (int l = 0; l < stride; ++l) uo[l] = l < L ? x[l] : 0u;
+            }
+            uint32_t* out = limbs + (size_t)v * stride;
+            int sgn = 1;
+            int64_t borrow = 0;
+            if (!ge && twice_gt) {          // negative: M - x
+                sgn = -1;
+                for (int l = 0; l < L; ++l) {
+                    const int64_t d = (int64_t)__ldg(T.Mtotal + l) - (int64_t)x[l] - borrow;
+                    borrow = d < 0;
+                    out[l] = (uint32_t)(d + (borrow ? (1ll << 32) : 0));
+                }
+            } else {                        // x, or x - M when x >= M
+                for (int l = 0; l < L; ++l) {
+                    const int64_t d = (int64_t)x[l] - (ge ? (int64_t)__ldg(T.Mtotal + l) : 0) - borrow;
+                    borrow = d < 0;
+                    out[l] = (uint32_t)(d + (borrow ? (1ll << 32) : 0));
+                }
+            }
+            for (int l = L; l < stride; ++l) out[l] = 0u;
+            int nl = L;
+            while (nl > 0 && out[nl - 1] == 0u) --nl;
+            sign_out[v] = nl ? sgn : 0;
+            if (nlimbs_out) nlimbs_out[v] = nl;
+        }
+        __syncwarp();
+    }
+}
+
+// ---- host launchers -----------------------------------------------------
+cudaError_t launch_crt_setup(const uint32_t* moduli, int K, int L, uint32_t* pinv, uint32_t* r2,
+                             uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal, cudaStream_t st) {
+    k_crt_setup<<<1, 256, 0, st>>>(moduli, K, L, pinv, r2, ginv, Mlimbs, Mtotal);
+    return cudaGetLastError();
+}
+
+template <int OWN>
+static cudaError_t launch_crt_t(const uint32_t* res, int n, const CrtTables& T, uint32_t* limbs,
+                                int stride, int32_t* sign, int32_t* nl, uint32_t* ul, int sms,
+                                cudaStream_t st, const uint64_t* in_off, const uint32_t* out_idx) {
+    const int wpb = 4;
+    const size_t smem = 4 * (crt_block_words(T.K) + wpb * crt_warp_words(T.K, T.L));
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_crt<OWN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int blocks = (n + wpb - 1) / wpb;
+    const int cap = sms * 8;
+    if (blocks > cap) blocks = cap;
+    k_crt<OWN><<<blocks, 32 * wpb, smem, st>>>(res, n, T, limbs, stride, sign, nl, ul, in_off, out_idx);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_crt(const uint32_t* res, int n, const CrtTables& T, uint32_t* limbs, int stride,
+                       int32_t* sign, int32_t* nl, uint32_t* ul, int sms, cudaStream_t st,
+                       const uint64_t* in_off, const uint32_t* out_idx) {
+    if (n <= 0) return cudaSuccess;
+    const int own = (T.K + 31) / 32;
+    if (own <= 1) return launch_crt_t<1>(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
+    if (own <= 2) return launch_crt_t<2>(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
+    if (own <= 4) return launch_crt_t<4>(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
+    if (own <= 8) return launch_crt_t<8>(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
+    if (own <= 16) return launch_crt_t<16>(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
+    if (own <= 32) return launch_crt_t<32>(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace dr

@@ -1,0 +1,231 @@
+// Dreams delta from exact limbs, and top-k selection.
+//
+// delta = -(1 + ln|p/q - L| / ln|q|) (reference runner.py:151-173).  With the
+// target as a ratio L = Lnum / Lden of integers (a dyadic Lden = 2^e for a
+// decimal/binary target), the error is computed without cancellation:
+//     |p/q - L| = |p*Lden - Lnum*q| / (|q| * Lden)
+// where the numerator is an exact big-integer difference.  Each logarithm is
+// taken from the leading three limbs (relative error ~2^-53), so delta is
+// accurate to ~1e-13, far inside the 1e-9 tolerance against mpmath.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "launch.h"
+
+namespace dr {
+
+__device__ __forceinline__ int top_limb(const uint32_t* x, int n) {
+    int t = n - 1;
+    while (t >= 0 && x[t] == 0u) --t;
+    return t;  // -1 for zero
+}
+
+__device__ __forceinline__ double ln_big(const uint32_t* x, int t) {
+    // t = index of the top non-zero limb (>= 0)
+    double v = (double)x[t];
+    int e = 0;
+    if (t >= 1) { v = v * 4294967296.0 + (double)x[t - 1]; }
+    if (t >= 2) { v = v * 4294967296.0 + (double)x[t - 2]; e = 32 * (t - 2); }
+    return log(v) + (double)e * 0.69314718055994530942;
+}
+
+// out[0..na+nb) = a * b (column sums per lane, then one carry pass by lane 0)
+__device__ void big_mul(const uint32_t* a, int na, const uint32_t* b, int nb, uint32_t* out,
+                        uint64_t* col, int lane) {
+    const int nr = na + nb;
+    for (int l = lane; l < nr; l += 32) {
+        uint64_t lo = 0, hi = 0;
+        const int i0 = l - (nb - 1) > 0 ? l - (nb - 1) : 0;
+        const int i1 = l < na - 1 ? l : na - 1;
+        for (int i = i0; i <= i1; ++i) {
+            const uint64_t pr = (uint64_t)a[i] * b[l - i];
+            lo += pr;
+            hi += (lo < pr);
+        }
+        col[2 * l] = lo;
+        col[2 * l + 1] = hi;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        unsigned __int128 c = 0;
+        for (int l = 0; l < nr; ++l) {
+            const unsigned __int128 t = (((unsigned __int128)col[2 * l + 1]) << 64) + col[2 * l] + c;
+            out[l] = (uint32_t)t;
+            c = t >> 32;
+        }
+    }
+    __syncwarp();
+}
+
+// per warp smem: A[maxlen] B[maxlen] col[2*maxlen] (u64)
+__global__ void __launch_bounds__(128) k_delta(DeltaArgs D) {
+    extern __shared__ uint64_t dsmem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const int ML = D.maxlen;
+    uint64_t* col = dsmem + (size_t)warp * (2 * ML + ML);
+    uint32_t* A = reinterpret_cast<uint32_t*>(col + 2 * ML);
+    uint32_t* B = A + ML;
+    for (int v = blockIdx.x * wpb + warp; v < D.n; v += gridDim.x * wpb) {
+        const uint32_t* p = D.p + (size_t)v * D.istride;
+        const uint32_t* q = D.q + (size_t)v * D.istride;
+        const int ti = D.per_item ? v : 0;
+        const uint32_t* ln = D.ln + (size_t)ti * D.listride;
+        const uint32_t* ld = D.ld + (size_t)ti * D.listride;
+        const int ps = D.ps[(size_t)v * D.sstride], qs = D.qs[(size_t)v * D.sstride];
+        const int lns = D.lns[(size_t)ti * D.lsstride] * (D.lds ? D.lds[(size_t)ti * D.lsstride] : 1);
+        const int tp = top_limb(p, D.nl), tq = top_limb(q, D.nl);
+        const int tn = top_limb(ln, D.lnl), td = top_limb(ld, D.lnl);
+        double result;
+        if (tq < 0 || qs == 0) {
+            result = -INFINITY;                                  // q == 0
+        } else if (td < 0) {
+            result = NAN;                                        // target denominator 0
+        } else {
+            const int np = tp + 1, nq = tq + 1, nn = tn + 1, nd = td + 1;
+            // A = |p| * Lden, B = |Lnum| * |q|
+            const int na = (np > 0 && nd > 0) ? np + nd : 0;
+            const int nb = (nn > 0) ? nn + nq : 0;
+            if (na) big_mul(p, np, ld, nd, A, col, lane);
+            if (nb) big_mul(ln, nn, q, nq, B, col, lane);
+            if (lane == 0) {
+                const int sa = na ? ps : 0;
+                const int sb = nb ? lns * qs : 0;
+                const int n = na > nb ? na : nb;
+                for (int l = na; l < n; ++l) A[l] = 0u;
+                for (int l = nb; l < n; ++l) B[l] = 0u;
+                // |D| = |sa*A - sb*B| into A
+                if (sa == 0 || sb == 0 || sa != sb) {
+                    if (sb != 0 && sa != 0) {  // opposite signs: A + B
+                        uint64_t c = 0;
+                        for (int l = 0; l < n; ++l) {
+                            const uint64_t t = (uint64_t)A[l] + B[l] + c;
+                            A[l] = (uint32_t)t;
+                            c = t >> 32;
+                        }
+                        // the sum of two n-limb numbers fits in n+1 limbs; ML has room
+                        A[n] = (uint32_t)c;
+                    } else if (sa == 0) {
+                        for (int l = 0; l < n; ++l) A[l] = B[l];
+                        A[n] = 0u;
+                    } else {
+                        A[n] = 0u;
+                    }
+                } else {                        // same sign: |A - B|
+                    int cmp = 0;
+                    for (int l = n - 1; l >= 0; --l)
+                        if (A[l] != B[l]) { cmp = A[l] > B[l] ? 1 : -1; break; }
+                    const uint32_t* big = cmp >= 0 ? A : B;
+                    const uint32_t* sml = cmp >= 0 ? B : A;
+                    int64_t br = 0;
+                    for (int l = 0; l < n; ++l) {
+                        const int64_t d = (int64_t)big[l] - (int64_t)sml[l] - br;
+                        br = d < 0;
+                        A[l] = (uint32_t)(d + (br ? (1ll << 32) : 0));
+                    }
+                    A[n] = 0u;
+                }
+                const int tD = top_limb(A, n + 1);
+                if (tD < 0) {
+                    result = INFINITY;                           // p/q == L exactly
+                } else if (tq == 0 && q[0] <= 1u) {
+                    result = -INFINITY;                          // |q| <= 1
+                } else {
+                    const double lq = ln_big(q, tq);
+                    const double lerr = ln_big(A, tD) - lq - ln_big(ld, td);
+                    result = -(1.0 + lerr / lq);
+                }
+                D.out[v] = result;
+            }
+            __syncwarp();
+            continue;
+        }
+        if (lane == 0) D.out[v] = result;
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_delta(const DeltaArgs& D, int sms, cudaStream_t st) {
+    if (D.n <= 0) return cudaSuccess;
+    const int wpb = 4;
+    const size_t smem = (size_t)wpb * (3 * (size_t)D.maxlen) * 8;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_delta, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    int blocks = (D.n + wpb - 1) / wpb;
+    if (blocks > sms * 8) blocks = sms * 8;
+    k_delta<<<blocks, 32 * wpb, smem, st>>>(D);
+    return cudaGetLastError();
+}
+
+// ---- top-k -----------------------------------------------------------------
+// Keys order doubles descending (+inf first, NaN last); ties by lower index.
+__device__ __forceinline__ uint64_t desc_key(double d) {
+    if (d != d) return 0ull;                                   // NaN last
+    uint64_t b = (uint64_t)__double_as_longlong(d);
+    b = (b >> 63) ? ~b : (b | 0x8000000000000000ull);          // ascending order key
+    return b;                                                  // larger = better
+}
+
+// before(a, b): a ranks ahead of b
+__device__ __forceinline__ bool ranks_before(uint64_t ka, uint32_t ia, uint64_t kb, uint32_t ib) {
+    return ka > kb || (ka == kb && ia < ib);
+}
+
+constexpr int kTopkTile = 4096;
+
+// Sort one tile of (key, index) pairs in shared memory, keep the first k.
+__global__ void __launch_bounds__(1024) k_topk_tile(const double* __restrict__ vals,
+                                                    const uint64_t* __restrict__ in_keys,
+                                                    const uint32_t* __restrict__ in_idx, int n,
+                                                    int k, uint64_t* __restrict__ out_keys,
+                                                    uint32_t* __restrict__ out_idx) {
+    __shared__ uint64_t sk[kTopkTile];
+    __shared__ uint32_t si[kTopkTile];
+    const int base = blockIdx.x * kTopkTile;
+    for (int i = threadIdx.x; i < kTopkTile; i += blockDim.x) {
+        const int g = base + i;
+        if (g < n) {
+            sk[i] = in_keys ? in_keys[g] : desc_key(vals[g]);
+            si[i] = in_idx ? in_idx[g] : (uint32_t)g;
+        } else {
+            sk[i] = 0ull;
+            si[i] = 0xffffffffu;
+        }
+    }
+    __syncthreads();
+    for (int size = 2; size <= kTopkTile; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < kTopkTile; i += blockDim.x) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;   // segment sorted "best first" when up
+                    const bool sw = up ? ranks_before(sk[j], si[j], sk[i], si[i])
+                                       : ranks_before(sk[i], si[i], sk[j], si[j]);
+                    if (sw) {
+                        const uint64_t tk = sk[i]; sk[i] = sk[j]; sk[j] = tk;
+                        const uint32_t ti = si[i]; si[i] = si[j]; si[j] = ti;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    const int keep = k < kTopkTile ? k : kTopkTile;
+    for (int i = threadIdx.x; i < keep; i += blockDim.x) {
+        out_keys[(size_t)blockIdx.x * keep + i] = sk[i];
+        out_idx[(size_t)blockIdx.x * keep + i] = si[i];
+    }
+}
+
+cudaError_t launch_topk_tile(const double* vals, const uint64_t* in_keys, const uint32_t* in_idx,
+                             int n, int k, uint64_t* out_keys, uint32_t* out_idx, cudaStream_t st) {
+    const int tiles = (n + kTopkTile - 1) / kTopkTile;
+    k_topk_tile<<<tiles, 1024, 0, st>>>(vals, in_keys, in_idx, n, k, out_keys, out_idx);
+    return cudaGetLastError();
+}
+
+int topk_tile_size() { return kTopkTile; }
+
+}  // namespace dr

@@ -1,0 +1,107 @@
+// Internal types shared by the host planner and the device kernels.
+#pragma once
+#include <stdint.h>
+
+namespace dr {
+
+// Opcode numbers of the program wire format (reference compiler.py:14-28).
+enum Opcode : uint32_t {
+    OP_NOP = 0, OP_LOAD_X = 1, OP_LOAD_C = 2, OP_LOAD_N = 3, OP_ADD = 4, OP_SUB = 5,
+    OP_MUL = 6, OP_NEG = 7, OP_POW2 = 8, OP_POW3 = 9, OP_INV = 10, OP_STORE = 11, OP_END = 12
+};
+
+// How a program is executed.
+enum Class : uint32_t {
+    CLS_COMPANION = 1,   // M = [[0..0 c0],[1 ..  c1],...]: sub-diagonal exactly 1, no INV
+                         // of step-dependent values; entries advanced by forward
+                         // differences, P*M is a column shift plus one mat-vec.
+    CLS_RATIONAL = 2,    // companion with rational last column: M = M'/g, g = product of
+                         // the denominators; P' advances with polynomial M', the scalar
+                         // g is accumulated and divided out once per chunk combine.
+    CLS_DENSE = 3,       // dense polynomial matrix, every entry by forward differences.
+    CLS_INTERP = 4,      // anything else: bytecode interpreted every step.
+};
+
+// Per-program record in device memory.  Instructions are uint4 {op, a, b, c}
+// with compacted registers; STORE's second operand is the entry slot
+// row*m + col (original program) or the stream slot (derived program).
+struct DevProgram {
+    uint32_t m, dim, cls, degree;      // degree: max degree in s of the streams
+    uint32_t op_off, n_ops, n_regs;    // original program (compacted)
+    uint32_t dop_off, dn_ops, dn_regs; // derived stream program (FD classes)
+    uint32_t c_off, n_consts;          // int64 constant pool
+    uint32_t n_streams;                // derived outputs
+    uint32_t zero_reg;                 // compacted register that always holds 0
+    uint32_t shadow_fd;                // 1: float shadow may use integer differences
+    uint32_t pad;
+};
+
+// Per-walk record in device memory.
+struct DevWalk {
+    uint32_t prog, K, flags, q_row;
+    int64_t a0;
+    uint64_t depth, checkpoint;
+    uint64_t axis_off;                 // into the int64 axis parameter array
+    uint64_t res_off, cp_res_off;      // residue output offsets
+    uint32_t shadow_mode;              // 0 none, 1 interpret, 2 integer differences
+    uint32_t pad;
+};
+
+// One unit of walk work: a depth chunk of one (walk, prime block).
+struct DevTile {
+    uint32_t walk;
+    uint32_t group;        // (walk, prime block) combine group
+    uint32_t prime0;       // first prime index of the block
+    uint32_t nprimes;      // primes in this block (<= 32)
+    uint32_t chunk;        // chunk index within the group
+    uint32_t slot;         // chunk-product slot (unused when the group has one chunk)
+    uint64_t s0, s1;       // step range [s0, s1)
+};
+
+// Combine group: the chunks of one (walk, prime block).
+struct DevGroup {
+    uint32_t walk, prime0, nprimes, n_chunks;
+    uint32_t slot0;        // first chunk-product slot
+    uint32_t cp_chunks;    // chunks covering [0, checkpoint) (0 = no checkpoint)
+};
+
+// Shadow work item: a warp-group of up to 32 walks (integer differences) or
+// one walk (interpreted).
+struct DevShadowItem {
+    uint32_t walk0, n_walks;           // walks are listed in shadow_walks[walk0..]
+};
+
+enum ShadowMode : uint32_t { SHADOW_NONE = 0, SHADOW_INTERP = 1, SHADOW_INTFD = 2 };
+
+constexpr int kMaxM = 8;
+constexpr int kMaxAxes = 8;
+constexpr int kMaxDegree = 16;
+constexpr int kMaxConsts = 512;
+constexpr int kMaxCompactRegs = 160;
+constexpr int kMaxFdRegs = 72;     // streams * (D + 1) held in registers per lane
+
+// Difference-table depths with a compiled kernel.
+constexpr int kTemplateDegrees[] = {1, 2, 3, 4, 6, 8, 12, 16};
+
+inline int streams_for(uint32_t cls, uint32_t m) {
+    return cls == CLS_COMPANION ? (int)m : cls == CLS_RATIONAL ? (int)m + 1
+         : cls == CLS_DENSE ? (int)(m * m) : 0;
+}
+
+// Smallest compiled difference depth >= degree for (cls, m), or -1 if the
+// program must run on the interpreter.  Must agree with the instantiation
+// list in walk_kernels.cu.
+inline int template_degree(uint32_t cls, uint32_t m, uint32_t degree) {
+    bool m_ok = (cls == CLS_COMPANION && m >= 2 && m <= 6) ||
+                (cls == CLS_RATIONAL && m >= 2 && m <= 4) ||
+                (cls == CLS_DENSE && m >= 2 && m <= 3);
+    if (!m_ok) return -1;
+    for (int d : kTemplateDegrees) {
+        if ((uint32_t)d < degree) continue;
+        if (streams_for(cls, m) * (d + 1) > kMaxFdRegs) return -1;
+        return d;
+    }
+    return -1;
+}
+
+}  // namespace dr

@@ -1,0 +1,1091 @@
+// Host engine and the device-facing C ABI: context, prepared walk batches,
+// CRT, delta and top-k entry points.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "../../include/dreams_b200.h"
+#include "host_common.h"
+#include "launch.h"
+#include "shadow_impl.cuh"
+#include "walk_impl.cuh"
+
+namespace dr {
+
+
+namespace {
+Context* g_ctx = nullptr;
+std::mutex g_init_mu;
+std::mutex g_batch_mu;
+std::map<int32_t, std::unique_ptr<Batch>> g_batches;
+int32_t g_next_batch = 1;
+}  // namespace
+
+Context* ctx() { return g_ctx; }
+
+int ensure_ctx() {
+    if (!g_ctx) {
+        set_error("dr_init has not been called");
+        return DR_ERR_NOT_INIT;
+    }
+    cudaSetDevice(g_ctx->device);
+    return DR_OK;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    set_error(std::string(where) + ": " + cudaGetErrorString(e));
+    cudaGetLastError();  // clear sticky-free errors so later calls can proceed
+    return e == cudaErrorMemoryAllocation ? DR_ERR_NOMEM : DR_ERR_CUDA;
+}
+
+#define DR_CUDA(call)                                   \
+    do {                                                \
+        cudaError_t e__ = (call);                       \
+        if (e__ != cudaSuccess) return cuda_fail(e__, #call); \
+    } while (0)
+
+int get_plan(const uint8_t* blob, uint64_t size, std::shared_ptr<Plan>* out, std::string* err) {
+    std::string key(reinterpret_cast<const char*>(blob), (size_t)size);
+    {
+        std::lock_guard<std::mutex> lk(g_ctx->mu);
+        auto it = g_ctx->plan_cache.find(key);
+        if (it != g_ctx->plan_cache.end()) {
+            *out = it->second;
+            return DR_OK;
+        }
+    }
+    RawProgram raw;
+    auto plan = std::make_shared<Plan>();
+    int rc = parse_blob(blob, size, &raw, err);
+    if (rc == DR_OK) rc = plan_program(raw, plan.get(), err);
+    if (rc != DR_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_ctx->mu);
+    if (g_ctx->plan_cache.size() > 200000) g_ctx->plan_cache.clear();
+    g_ctx->plan_cache.emplace(std::move(key), plan);
+    *out = plan;
+    return DR_OK;
+}
+
+int crt_limbs_for(int K) { return (31 * K + 31) / 32 + 2; }
+
+static int build_crt_set(const uint32_t* moduli_host, int K, CrtSet& S, cudaStream_t st) {
+    S.K = K;
+    S.L = crt_limbs_for(K);
+    DR_CUDA(S.moduli.alloc(4ull * K));
+    DR_CUDA(S.pinv.alloc(4ull * K));
+    DR_CUDA(S.r2.alloc(4ull * K));
+    DR_CUDA(S.ginv.alloc(4ull * K));
+    DR_CUDA(S.Mlimbs.alloc(4ull * K * S.L));
+    DR_CUDA(S.Mtotal.alloc(4ull * S.L));
+    DR_CUDA(cudaMemcpyAsync(S.moduli.p, moduli_host, 4ull * K, cudaMemcpyHostToDevice, st));
+    DR_CUDA(launch_crt_setup(S.moduli.as<uint32_t>(), K, S.L, S.pinv.as<uint32_t>(), S.r2.as<uint32_t>(),
+                             S.ginv.as<uint32_t>(), S.Mlimbs.as<uint32_t>(), S.Mtotal.as<uint32_t>(), st));
+    DR_CUDA(cudaStreamSynchronize(st));
+    return DR_OK;
+}
+
+int crt_tables_std(int K, std::shared_ptr<CrtSet>* out) {
+    {
+        std::lock_guard<std::mutex> lk(g_ctx->mu);
+        auto it = g_ctx->crt_std.find(K);
+        if (it != g_ctx->crt_std.end()) {
+            *out = it->second;
+            return DR_OK;
+        }
+    }
+    auto S = std::make_shared<CrtSet>();
+    const auto& tab = prime_table(K);
+    int rc = build_crt_set(tab.data(), K, *S, g_ctx->stream);
+    if (rc != DR_OK) return rc;
+    std::lock_guard<std::mutex> lk(g_ctx->mu);
+    g_ctx->crt_std[K] = S;
+    *out = S;
+    return DR_OK;
+}
+
+Batch::~Batch() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    for (cudaEvent_t e : joins) cudaEventDestroy(e);
+}
+
+// ---- batch construction ---------------------------------------------------------
+
+namespace {
+
+struct LaunchKey {
+    int kind;
+    uint32_t cls, m, D;
+    bool operator<(const LaunchKey& o) const {
+        return std::tie(kind, cls, m, D) < std::tie(o.kind, o.cls, o.m, o.D);
+    }
+};
+
+template <class T>
+int upload(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+    DR_CUDA(b.alloc(sizeof(T) * std::max<size_t>(v.size(), 1)));
+    if (!v.empty()) DR_CUDA(cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st));
+    return DR_OK;
+}
+
+uint32_t chunk_policy(uint64_t total_group_steps, uint64_t n_groups, int sms, const dr_tune* tune) {
+    if (tune && tune->chunk_steps) return tune->chunk_steps;
+    // aim for ~6 tiles per resident warp slot (24 per SM) so the longest-first
+    // queue balances, with chunks no shorter than 256 steps
+    const double target_tiles = (double)sms * 24.0 * 6.0;
+    double c = (double)total_group_steps / target_tiles;
+    if (n_groups > target_tiles) c = 1e18;  // enough groups already: one chunk each
+    c = std::max(c, 256.0);
+    c = std::min(c, 4194304.0);
+    return (uint32_t)c;
+}
+
+}  // namespace
+
+int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs,
+                const uint64_t* blob_offsets, int32_t n_programs, const int64_t* axis,
+                uint64_t n_axis, const dr_tune* tune, uint64_t n_res, std::unique_ptr<Batch>* out) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Context& C = *g_ctx;
+    if (n_walks < 0 || n_programs < 0 || (n_walks > 0 && (!walks || !blob_offsets || !blobs))) {
+        set_error("null walk or program arrays");
+        return DR_ERR_ARG;
+    }
+    const uint32_t engine = tune ? tune->engine : DR_ENGINE_AUTO;
+    auto B = std::make_unique<Batch>();
+    B->n_walks = (uint32_t)n_walks;
+    B->n_res = n_res;
+
+    // ---- programs
+    std::vector<std::shared_ptr<Plan>> plans(n_programs);
+    std::vector<DevProgram> dprogs(n_programs);
+    std::vector<uint4> code;
+    std::vector<int64_t> consts;
+    for (int32_t i = 0; i < n_programs; ++i) {
+        if (blob_offsets[i + 1] < blob_offsets[i]) {
+            set_error("blob_offsets not increasing");
+            return DR_ERR_ARG;
+        }
+        std::string err;
+        rc = get_plan(blobs + blob_offsets[i], blob_offsets[i + 1] - blob_offsets[i], &plans[i], &err);
+        if (rc) {
+            set_error("program " + std::to_string(i) + ": " + err);
+            return rc;
+        }
+        const Plan& P = *plans[i];
+        DevProgram d{};
+        d.m = P.m;
+        d.dim = P.dim;
+        d.cls = (engine == DR_ENGINE_AUTO) ? (uint32_t)P.cls : (uint32_t)CLS_INTERP;
+        d.degree = P.degree;
+        d.op_off = (uint32_t)code.size();
+        d.n_ops = (uint32_t)P.ops.size();
+        for (const Insn& in : P.ops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
+        d.n_regs = P.n_regs;
+        d.dop_off = (uint32_t)code.size();
+        d.dn_ops = (uint32_t)P.dops.size();
+        for (const Insn& in : P.dops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
+        d.dn_regs = P.dn_regs;
+        d.c_off = (uint32_t)consts.size();
+        d.n_consts = (uint32_t)P.consts.size();
+        consts.insert(consts.end(), P.consts.begin(), P.consts.end());
+        d.n_streams = P.n_streams;
+        d.zero_reg = P.zero_reg;
+        d.shadow_fd = (!P.has_inv && (P.cls == CLS_COMPANION || P.cls == CLS_DENSE)) ? 1u : 0u;
+        dprogs[i] = d;
+    }
+
+    // ---- walks
+    std::vector<DevWalk> dwalks(n_walks);
+    uint64_t total_group_steps = 0, n_groups = 0;
+    for (int32_t w = 0; w < n_walks; ++w) {
+        const dr_walk_desc& W = walks[w];
+        if (W.program >= (uint32_t)n_programs) { set_error("walk program index out of range"); return DR_ERR_ARG; }
+        const DevProgram& G = dprogs[W.program];
+        if (W.K < 1 || W.K > DR_MAX_K) { set_error("K outside 1..DR_MAX_K"); return DR_ERR_UNSUPPORTED; }
+        if (W.q_row >= G.m) { set_error("q_row >= m"); return DR_ERR_ARG; }
+        if (W.checkpoint && W.checkpoint >= W.depth) { set_error("checkpoint must be < depth"); return DR_ERR_ARG; }
+        if ((W.flags & DR_WALK_INIT_PCF) && G.m < 2) { set_error("PCF initial matrix needs m >= 2"); return DR_ERR_ARG; }
+        if (W.res_offset + W.K > n_res || (W.checkpoint && W.cp_res_offset + W.K > n_res)) {
+            set_error("residue output offset out of range");
+            return DR_ERR_ARG;
+        }
+        if (W.axis_offset + 4ull * G.dim > n_axis) { set_error("axis parameters out of range"); return DR_ERR_ARG; }
+        if (W.depth > (1ull << 40)) { set_error("depth above 2^40"); return DR_ERR_UNSUPPORTED; }
+        for (uint32_t a = 0; a < G.dim; ++a) {
+            const int64_t* ax = axis + W.axis_offset + 4 * a;
+            if (ax[1] == 0 || ax[3] == 0) {
+                // the reference divides by float(sd*td) (cmf_walk.py:281): ZeroDivisionError
+                set_error("zero shift or trajectory denominator");
+                return DR_ERR_ARG;
+            }
+            const __int128 hi = (__int128)ax[0] * ax[3];
+            const __int128 st = (__int128)ax[2] * ax[1];
+            const __int128 lim = (__int128)1 << 62;
+            const __int128 span = st * (__int128)(W.depth + 64);
+            if (hi > lim || hi < -lim || span > lim || span < -lim || (__int128)ax[1] * ax[3] > lim ||
+                (__int128)ax[1] * ax[3] < -lim) {
+                set_error("axis numerators exceed 2^62 over the walk");
+                return DR_ERR_UNSUPPORTED;
+            }
+        }
+        DevWalk d{};
+        d.prog = W.program;
+        d.K = W.K;
+        d.flags = W.flags;
+        d.q_row = W.q_row;
+        d.a0 = W.a0;
+        d.depth = W.depth;
+        d.checkpoint = W.checkpoint;
+        d.axis_off = W.axis_offset;
+        d.res_off = W.res_offset;
+        d.cp_res_off = W.cp_res_offset;
+        d.shadow_mode = SHADOW_NONE;
+        if (W.flags & DR_WALK_SHADOW) {
+            d.shadow_mode = SHADOW_INTERP;
+            const Plan& P = *plans[W.program];
+            const int Dt = template_degree(P.cls, P.m, P.degree);
+            if (G.shadow_fd && G.cls != CLS_INTERP && Dt > 0) {
+                const double b = float_bound_log2(P, axis + W.axis_offset, W.depth + 1);
+                if (b < 53.0 && b + Dt < 61.0) d.shadow_mode = SHADOW_INTFD;
+            }
+            B->has_shadow = true;
+        }
+        dwalks[w] = d;
+        const uint64_t nb = (W.K + 31) / 32;
+        total_group_steps += nb * std::max<uint64_t>(W.depth, 1);
+        n_groups += nb;
+        B->prime_steps += (uint64_t)W.K * W.depth;
+    }
+
+    // ---- tiles and groups
+    const bool plain = engine == DR_ENGINE_PLAIN;
+    const uint32_t chunk = plain ? 0xffffffffu : chunk_policy(total_group_steps, n_groups, C.sms, tune);
+    std::map<LaunchKey, std::vector<DevTile>> tile_sets;
+    std::vector<DevGroup> groups;
+    uint32_t slots = 0;
+    for (int32_t w = 0; w < n_walks; ++w) {
+        const DevWalk& W = dwalks[w];
+        const DevProgram& G = dprogs[W.prog];
+        const Plan& P = *plans[W.prog];
+        LaunchKey key{0, G.cls, G.m, 0};
+        if (G.cls != CLS_INTERP) key.D = (uint32_t)template_degree(P.cls, P.m, P.degree);
+        // chunk boundaries; a checkpoint always ends a chunk
+        std::vector<std::pair<uint64_t, uint64_t>> ranges;
+        auto split = [&](uint64_t a, uint64_t b) {
+            const uint64_t len = b - a;
+            const uint64_t nc = std::max<uint64_t>(1, (len + chunk - 1) / chunk);
+            for (uint64_t c = 0; c < nc; ++c)
+                ranges.emplace_back(a + len * c / nc, a + len * (c + 1) / nc);
+        };
+        if (W.depth == 0) ranges.emplace_back(0, 0);
+        else if (W.checkpoint) { split(0, W.checkpoint); split(W.checkpoint, W.depth); }
+        else split(0, W.depth);
+        uint32_t cp_chunks = 0;
+        if (W.checkpoint)
+            for (auto& r : ranges) cp_chunks += r.second <= W.checkpoint;
+        for (uint32_t p0 = 0; p0 < W.K; p0 += 32) {
+            DevGroup g{};
+            g.walk = (uint32_t)w;
+            g.prime0 = p0;
+            g.nprimes = std::min<uint32_t>(32, W.K - p0);
+            g.n_chunks = (uint32_t)ranges.size();
+            g.cp_chunks = cp_chunks;
+            g.slot0 = g.n_chunks > 1 ? slots : 0;
+            if (g.n_chunks > 1) slots += g.n_chunks;
+            const uint32_t gi = (uint32_t)groups.size();
+            groups.push_back(g);
+            auto& vec = tile_sets[key];
+            for (uint32_t c = 0; c < g.n_chunks; ++c) {
+                DevTile t{};
+                t.walk = (uint32_t)w;
+                t.group = gi;
+                t.prime0 = p0;
+                t.nprimes = g.nprimes;
+                t.chunk = c;
+                t.slot = g.slot0 + c;
+                t.s0 = ranges[c].first;
+                t.s1 = ranges[c].second;
+                vec.push_back(t);
+            }
+        }
+    }
+    std::vector<DevTile> tiles;
+    for (auto& kv : tile_sets) {
+        auto& v = kv.second;
+        std::stable_sort(v.begin(), v.end(), [](const DevTile& a, const DevTile& b) {
+            return (a.s1 - a.s0) > (b.s1 - b.s0);
+        });
+        LaunchSpec L{};
+        L.kind = 0;
+        L.cls = kv.first.cls;
+        L.m = kv.first.m;
+        L.D = kv.first.D;
+        L.off = (uint32_t)tiles.size();
+        L.count = (uint32_t)v.size();
+        L.items = L.count;
+        uint32_t rr = 1, rc_ = 1;
+        for (const DevTile& t : v) {
+            const DevProgram& G = dprogs[dwalks[t.walk].prog];
+            rr = std::max(rr, std::max(G.n_regs, G.dn_regs));
+            rc_ = std::max(rc_, G.n_consts);
+        }
+        const uint32_t ns = (uint32_t)std::max(streams_for(L.cls, L.m), 0);
+        L.rows_regs = rr;
+        L.rows_consts = rc_;
+        L.rows_stage = std::max(L.m * L.m, (L.D + 1) * ns);
+        L.rows_per_warp = L.rows_regs + L.rows_consts + 3 * kMaxAxes + L.rows_stage;
+        tiles.insert(tiles.end(), v.begin(), v.end());
+        B->launches.push_back(L);
+    }
+    B->n_tiles = (uint32_t)tiles.size();
+    B->n_groups = (uint32_t)groups.size();
+
+    // ---- shadow work lists
+    std::map<LaunchKey, std::vector<uint32_t>> shadow_sets;
+    for (int32_t w = 0; w < n_walks; ++w) {
+        const DevWalk& W = dwalks[w];
+        if (W.shadow_mode == SHADOW_NONE) continue;
+        const DevProgram& G = dprogs[W.prog];
+        const Plan& P = *plans[W.prog];
+        if (W.shadow_mode == SHADOW_INTFD)
+            shadow_sets[LaunchKey{2, P.cls, P.m, (uint32_t)template_degree(P.cls, P.m, P.degree)}].push_back(w);
+        else
+            shadow_sets[LaunchKey{1, 0, G.m, 0}].push_back(w);
+    }
+    std::vector<uint32_t> shadow_list;
+    for (auto& kv : shadow_sets) {
+        auto& v = kv.second;
+        std::stable_sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) {
+            return dwalks[a].depth > dwalks[b].depth;
+        });
+        LaunchSpec L{};
+        L.kind = kv.first.kind;
+        L.cls = kv.first.cls;
+        L.m = kv.first.m;
+        L.D = kv.first.D;
+        L.off = (uint32_t)shadow_list.size();
+        L.count = (uint32_t)v.size();
+        L.items = L.kind == 1 ? L.count : (L.count + 31) / 32;
+        uint32_t rr = 1;
+        for (uint32_t w : v) {
+            const DevProgram& G = dprogs[dwalks[w].prog];
+            rr = std::max(rr, L.kind == 1 ? G.n_regs : G.dn_regs);
+        }
+        L.rows_regs = rr;
+        const uint32_t ns = L.kind == 2 ? (uint32_t)streams_for(L.cls, L.m) : 0;
+        L.rows_per_warp = L.kind == 1 ? rr + kMaxAxes + L.m * L.m
+                                      : rr + kMaxAxes + (L.D + 1) * ns + ns;
+        shadow_list.insert(shadow_list.end(), v.begin(), v.end());
+        B->launches.push_back(L);
+    }
+
+    // ---- launch geometry
+    const int wpb = (tune && tune->warps_per_block) ? (int)tune->warps_per_block : 4;
+    uint32_t q = 0;
+    for (LaunchSpec& L : B->launches) {
+        L.queue = q++;
+        L.block = 32 * wpb;
+        const size_t word = L.kind == 0 ? 4 : 8;
+        L.smem = (size_t)L.rows_per_warp * 32 * word * wpb;
+        if (L.smem > 227 * 1024) {
+            set_error("program needs more shared memory per warp than a block offers");
+            return DR_ERR_UNSUPPORTED;
+        }
+        int occ = 0;
+        cudaError_t e;
+        WalkArgs wa{};
+        ShadowArgs sa{};
+        if (L.kind == 0) e = walk_dispatch(L.cls, L.m, L.D, 0, L.block, L.smem, nullptr, wa, &occ);
+        else if (L.kind == 1) e = shadow_interp_dispatch(L.m, 0, L.block, L.smem, nullptr, sa, &occ);
+        else e = shadow_fd_dispatch(L.cls, L.m, L.D, 0, L.block, L.smem, nullptr, sa, &occ);
+        if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+        if (occ < 1) {
+            set_error("kernel cannot be resident with this shared memory size");
+            return DR_ERR_UNSUPPORTED;
+        }
+        const int want = (int)((L.items + wpb - 1) / wpb);
+        L.grid = std::max(1, std::min(want, occ * C.sms));
+        if (plain) L.grid = 1;
+    }
+    B->n_queues = q;
+
+    // ---- upload
+    cudaStream_t st = C.stream;
+    if ((rc = upload(B->progs, dprogs, st))) return rc;
+    if ((rc = upload(B->code, code, st))) return rc;
+    if ((rc = upload(B->consts, consts, st))) return rc;
+    if ((rc = upload(B->walks, dwalks, st))) return rc;
+    std::vector<int64_t> ax(axis, axis + n_axis);
+    if ((rc = upload(B->axis, ax, st))) return rc;
+    if ((rc = upload(B->tiles, tiles, st))) return rc;
+    if ((rc = upload(B->groups, groups, st))) return rc;
+    if ((rc = upload(B->shadow_list, shadow_list, st))) return rc;
+    DR_CUDA(B->group_done.alloc(4ull * std::max<uint32_t>(B->n_groups, 1)));
+    DR_CUDA(cudaMemsetAsync(B->group_done.p, 0, B->group_done.bytes, st));
+    uint32_t max_m = 1;
+    for (auto& d : dprogs) max_m = std::max(max_m, d.m);
+    B->chunk_stride = max_m * max_m * 32;
+    DR_CUDA(B->chunkP.alloc(4ull * std::max<uint32_t>(slots, 1) * B->chunk_stride));
+    DR_CUDA(B->chunkSig.alloc(4ull * std::max<uint32_t>(slots, 1) * 32));
+    DR_CUDA(B->queues.alloc(4ull * std::max<uint32_t>(B->n_queues, 1)));
+    DR_CUDA(B->res.alloc(8ull * std::max<uint64_t>(n_res, 1)));
+    DR_CUDA(cudaMemsetAsync(B->res.p, 0, B->res.bytes, st));
+    B->h_walk_K.resize(n_walks);
+    B->h_res_off.resize(n_walks);
+    B->h_cp_off.resize(n_walks);
+    for (int32_t w = 0; w < n_walks; ++w) {
+        B->h_walk_K[w] = walks[w].K;
+        B->h_res_off[w] = walks[w].res_offset;
+        B->h_cp_off[w] = walks[w].checkpoint ? walks[w].cp_res_offset : UINT64_MAX;
+    }
+    DR_CUDA(B->shadow.alloc(8ull * 6 * std::max<int32_t>(n_walks, 1)));
+    DR_CUDA(cudaMemsetAsync(B->shadow.p, 0, B->shadow.bytes, st));
+    DR_CUDA(B->status.alloc(4ull * std::max<int32_t>(n_walks, 1)));
+    DR_CUDA(cudaEventCreate(&B->ev0));
+    DR_CUDA(cudaEventCreate(&B->ev1));
+    DR_CUDA(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
+    DR_CUDA(cudaEventCreateWithFlags(&B->join, cudaEventDisableTiming));
+    B->joins.resize(C.pool.size());
+    for (auto& e : B->joins) DR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    DR_CUDA(cudaStreamSynchronize(st));
+    *out = std::move(B);
+    return DR_OK;
+}
+
+static CrtTables tables_of(const CrtSet& S);
+
+// CRT (one launch per K), delta and top-k passes on st after the walk.
+static int enqueue_pipeline(Batch& B, cudaStream_t st) {
+    Context& C = *g_ctx;
+    const uint64_t qoff = std::max<uint64_t>(B.n_res, 1);
+    (void)qoff;
+    for (const Batch::CrtGroup& g : B.crt_groups) {
+        std::shared_ptr<CrtSet> S;
+        int rc = crt_tables_std(g.K, &S);
+        if (rc) return rc;
+        cudaError_t e = launch_crt(B.res.as<uint32_t>(), (int)g.count, tables_of(*S), B.limbs.as<uint32_t>(),
+                                   B.Lmax, B.signs.as<int32_t>(), nullptr, nullptr, C.sms, st,
+                                   B.crt_in.as<uint64_t>() + g.off, B.crt_out.as<uint32_t>() + g.off);
+        if (e != cudaSuccess) return cuda_fail(e, "pipeline crt");
+    }
+    if (B.pipe.delta_mode != DR_DELTA_NONE) {
+        DeltaArgs D{};
+        const bool self = B.pipe.delta_mode == DR_DELTA_SELF;
+        const size_t L = (size_t)B.Lmax;
+        const uint32_t* lim = B.limbs.as<uint32_t>();
+        const int32_t* sg = B.signs.as<int32_t>();
+        D.p = lim + (self ? 2 : 0) * L;
+        D.q = lim + (self ? 3 : 1) * L;
+        D.ps = sg + (self ? 2 : 0);
+        D.qs = sg + (self ? 3 : 1);
+        D.n = (int)B.n_walks;
+        D.nl = B.Lmax;
+        D.istride = 4 * L;
+        D.sstride = 4;
+        if (self) {
+            D.ln = lim;
+            D.ld = lim + L;
+            D.lns = sg;
+            D.lds = sg + 1;
+            D.lnl = B.Lmax;
+            D.per_item = 1;
+            D.listride = 4 * L;
+            D.lsstride = 4;
+        } else {
+            D.ln = B.tgt_num.as<uint32_t>();
+            D.ld = B.tgt_den.as<uint32_t>();
+            D.lns = B.tgt_sign.as<int32_t>();
+            D.lds = nullptr;
+            D.lnl = B.pipe.l_limbs;
+            D.per_item = 0;
+            D.listride = 0;
+            D.lsstride = 0;
+        }
+        D.out = B.delta.as<double>();
+        D.maxlen = ((B.Lmax + std::max(B.Lmax, B.pipe.l_limbs) + 4) + 1) & ~1;
+        cudaError_t e = launch_delta(D, C.sms, st);
+        if (e != cudaSuccess) return cuda_fail(e, "pipeline delta");
+        for (size_t pass = 0; pass < B.tk_counts.size(); ++pass) {
+            const int src = (int)(pass & 1) ^ 1, dst = (int)(pass & 1);
+            e = launch_topk_tile(pass == 0 ? B.delta.as<double>() : nullptr,
+                                 pass == 0 ? nullptr : B.tk_keys[src].as<uint64_t>(),
+                                 pass == 0 ? nullptr : B.tk_idx[src].as<uint32_t>(),
+                                 B.tk_counts[pass], B.pipe.topk, B.tk_keys[dst].as<uint64_t>(),
+                                 B.tk_idx[dst].as<uint32_t>(), st);
+            if (e != cudaSuccess) return cuda_fail(e, "pipeline topk");
+        }
+    }
+    return DR_OK;
+}
+
+// One run of a batch: zero the work counters and status words, then every
+// launch group (shadow kernels first, they have the longest serial chains)
+// on its own stream of the pool, forked from and joined back into st.
+static int enqueue_batch(Batch& B, cudaStream_t st) {
+    Context& C = *g_ctx;
+    DR_CUDA(cudaMemsetAsync(B.queues.p, 0, B.queues.bytes, st));
+    DR_CUDA(cudaMemsetAsync(B.status.p, 0, B.status.bytes, st));
+    WalkArgs wa{};
+    wa.progs = B.progs.as<DevProgram>();
+    wa.code = B.code.as<uint4>();
+    wa.consts = B.consts.as<int64_t>();
+    wa.walks = B.walks.as<DevWalk>();
+    wa.axis = B.axis.as<int64_t>();
+    wa.groups = B.groups.as<DevGroup>();
+    wa.group_done = B.group_done.as<uint32_t>();
+    wa.chunk_P = B.chunkP.as<uint32_t>();
+    wa.chunk_stride = B.chunk_stride;
+    wa.chunk_sig = B.chunkSig.as<uint32_t>();
+    wa.primes = C.primes.as<uint32_t>();
+    wa.pinv = C.pinv.as<uint32_t>();
+    wa.r2 = C.r2.as<uint32_t>();
+    wa.p_res = B.res.as<uint32_t>();
+    wa.q_res = B.res.as<uint32_t>() + std::max<uint64_t>(B.n_res, 1);
+    wa.status = B.status.as<uint32_t>();
+    ShadowArgs sa{};
+    sa.progs = wa.progs;
+    sa.code = wa.code;
+    sa.consts = wa.consts;
+    sa.walks = wa.walks;
+    sa.axis = wa.axis;
+    sa.shadow = B.shadow.as<double>();
+    sa.n_walks = B.n_walks;
+    sa.status = wa.status;
+    DR_CUDA(cudaEventRecord(B.fork, st));
+    const size_t np = C.pool.size();
+    size_t used = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (const LaunchSpec& L : B.launches) {
+            if (L.items == 0 || (pass == 0) != (L.kind != 0)) continue;
+            cudaStream_t s = C.pool[used % np];
+            if (used < np) DR_CUDA(cudaStreamWaitEvent(s, B.fork, 0));
+            ++used;
+            cudaError_t e;
+            if (L.kind == 0) {
+                wa.tiles = B.tiles.as<DevTile>() + L.off;
+                wa.n_tiles = L.count;
+                wa.queue = B.queues.as<uint32_t>() + L.queue;
+                wa.rows_regs = L.rows_regs;
+                wa.rows_consts = L.rows_consts;
+                wa.rows_stage = L.rows_stage;
+                wa.rows_per_warp = L.rows_per_warp;
+                e = walk_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, wa, nullptr);
+            } else {
+                sa.list = B.shadow_list.as<uint32_t>() + L.off;
+                sa.n_items = L.items;
+                sa.n_list = L.count;
+                sa.queue = B.queues.as<uint32_t>() + L.queue;
+                sa.rows_regs = L.rows_regs;
+                sa.rows_per_warp = L.rows_per_warp;
+                e = L.kind == 1 ? shadow_interp_dispatch(L.m, L.grid, L.block, L.smem, s, sa, nullptr)
+                                : shadow_fd_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, sa, nullptr);
+            }
+            if (e != cudaSuccess) {
+                // rejoin what was forked so a capture can end cleanly
+                for (size_t i = 0; i < std::min(used, np); ++i) {
+                    cudaEventRecord(B.joins[i], C.pool[i]);
+                    cudaStreamWaitEvent(st, B.joins[i], 0);
+                }
+                return cuda_fail(e, L.kind == 0 ? "walk launch" : "shadow launch");
+            }
+        }
+    }
+    for (size_t i = 0; i < std::min(used, np); ++i) {
+        DR_CUDA(cudaEventRecord(B.joins[i], C.pool[i]));
+        DR_CUDA(cudaStreamWaitEvent(st, B.joins[i], 0));
+    }
+    if (B.pipe_on) return enqueue_pipeline(B, st);
+    return DR_OK;
+}
+
+int batch_run(Batch& B, cudaStream_t st) {
+    Context& C = *g_ctx;
+    if (!st) st = C.stream;
+    if (!B.graph) {
+        cudaStream_t cap;
+        DR_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        int rc = DR_OK;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeRelaxed);
+        if (e != cudaSuccess) { cudaStreamDestroy(cap); return cuda_fail(e, "begin capture"); }
+        rc = enqueue_batch(B, cap);
+        e = cudaStreamEndCapture(cap, &g);
+        cudaStreamDestroy(cap);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_fail(e, "end capture");
+        e = cudaGraphInstantiate(&B.graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) { B.graph = nullptr; return cuda_fail(e, "graph instantiate"); }
+    }
+    DR_CUDA(cudaEventRecord(B.ev0, st));
+    DR_CUDA(cudaGraphLaunch(B.graph, st));
+    DR_CUDA(cudaEventRecord(B.ev1, st));
+    return DR_OK;
+}
+
+int batch_read(Batch& B, uint32_t* p_res, uint32_t* q_res, uint64_t n_res, double* shadow,
+               uint32_t* status) {
+    Context& C = *g_ctx;
+    DR_CUDA(cudaStreamSynchronize(C.stream));
+    DR_CUDA(cudaEventSynchronize(B.ev1));
+    cudaEventElapsedTime(&B.last_ms, B.ev0, B.ev1);
+    const uint64_t n = std::min(n_res, B.n_res);
+    if (p_res) DR_CUDA(cudaMemcpy(p_res, B.res.p, 4 * n, cudaMemcpyDeviceToHost));
+    if (q_res)
+        DR_CUDA(cudaMemcpy(q_res, B.res.as<uint32_t>() + std::max<uint64_t>(B.n_res, 1), 4 * n,
+                           cudaMemcpyDeviceToHost));
+    if (shadow) DR_CUDA(cudaMemcpy(shadow, B.shadow.p, 8ull * 6 * B.n_walks, cudaMemcpyDeviceToHost));
+    if (status) DR_CUDA(cudaMemcpy(status, B.status.p, 4ull * B.n_walks, cudaMemcpyDeviceToHost));
+    return DR_OK;
+}
+
+}  // namespace dr
+
+// =============================================================================
+// C ABI
+// =============================================================================
+using namespace dr;
+
+namespace dr {
+
+static CrtTables tables_of(const CrtSet& S) {
+    CrtTables T;
+    T.moduli = S.moduli.as<uint32_t>();
+    T.pinv = S.pinv.as<uint32_t>();
+    T.r2 = S.r2.as<uint32_t>();
+    T.ginv = S.ginv.as<uint32_t>();
+    T.Mlimbs = S.Mlimbs.as<uint32_t>();
+    T.Mtotal = S.Mtotal.as<uint32_t>();
+    T.K = S.K;
+    T.L = S.L;
+    return T;
+}
+
+static int moduli_ok(const uint32_t* m, int K) {
+    for (int k = 0; k < K; ++k)
+        if (m[k] < 3u || m[k] >= (1u << 31) || !(m[k] & 1u)) {
+            set_error("CRT modulus " + std::to_string(m[k]) + " outside odd [3, 2^31)");
+            return DR_ERR_MODULUS;
+        }
+    return DR_OK;
+}
+
+// CRT on device pointers; custom moduli are copied to the host for validation.
+static int crt_device(const uint32_t* res_d, int32_t K, int32_t n, const uint32_t* moduli_host,
+                      uint32_t* limbs_d, int32_t stride, int32_t* sign_d, int32_t* nl_d,
+                      uint32_t* ul_d, cudaStream_t st) {
+    if (K < 1 || K > 1024 || n < 0) { set_error("CRT supports 1 <= K <= 1024"); return K > 1024 ? DR_ERR_UNSUPPORTED : DR_ERR_ARG; }
+    std::shared_ptr<CrtSet> S;
+    CrtSet custom;
+    if (moduli_host) {
+        int rc = moduli_ok(moduli_host, K);
+        if (rc) return rc;
+        rc = build_crt_set(moduli_host, K, custom, g_ctx->stream);
+        if (rc) return rc;
+    } else {
+        int rc = crt_tables_std(K, &S);
+        if (rc) return rc;
+    }
+    const CrtSet& set = moduli_host ? custom : *S;
+    if (stride < set.L) { set_error("limb_stride below ceil(31K/32)+2"); return DR_ERR_ARG; }
+    cudaError_t e = launch_crt(res_d, n, tables_of(set), limbs_d, stride, sign_d, nl_d, ul_d, g_ctx->sms, st);
+    if (e != cudaSuccess) return cuda_fail(e, "crt launch");
+    if (moduli_host) DR_CUDA(cudaStreamSynchronize(st));  // custom tables die with this call
+    return DR_OK;
+}
+
+}  // namespace dr
+
+extern "C" {
+
+int dr_init(int device) {
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    if (g_ctx) {
+        if (g_ctx->device == device) return DR_OK;
+        set_error("dr_init: already initialised on another device");
+        return DR_ERR_ARG;
+    }
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return cuda_fail(e == cudaSuccess ? cudaErrorNoDevice : e, "dr_init");
+    if (device < 0 || device >= n) { set_error("dr_init: no such device"); return DR_ERR_ARG; }
+    DR_CUDA(cudaSetDevice(device));
+    auto* c = new Context();
+    c->device = device;
+    DR_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
+    DR_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    DR_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    c->pool.resize(8);
+    for (auto& s : c->pool) DR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const auto& tab = prime_table(DR_MAX_K);
+    std::vector<uint32_t> pinv(DR_MAX_K), r2(DR_MAX_K);
+    for (int k = 0; k < DR_MAX_K; ++k) {
+        PrimeMeta m = prime_meta(tab[k]);
+        pinv[k] = m.pinv;
+        r2[k] = m.r2;
+    }
+    DR_CUDA(c->primes.alloc(4ull * DR_MAX_K));
+    DR_CUDA(c->pinv.alloc(4ull * DR_MAX_K));
+    DR_CUDA(c->r2.alloc(4ull * DR_MAX_K));
+    DR_CUDA(cudaMemcpy(c->primes.p, tab.data(), 4ull * DR_MAX_K, cudaMemcpyHostToDevice));
+    DR_CUDA(cudaMemcpy(c->pinv.p, pinv.data(), 4ull * DR_MAX_K, cudaMemcpyHostToDevice));
+    DR_CUDA(cudaMemcpy(c->r2.p, r2.data(), 4ull * DR_MAX_K, cudaMemcpyHostToDevice));
+    g_ctx = c;
+    return DR_OK;
+}
+
+int dr_walk_batch(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs,
+                  const uint64_t* blob_offsets, int32_t n_programs, const int64_t* axis_params,
+                  uint64_t n_axis_params, const dr_tune* tune, uint32_t* p_res, uint32_t* q_res,
+                  uint64_t n_res, double* shadow, uint32_t* status) {
+    std::unique_ptr<Batch> B;
+    int rc = batch_build(walks, n_walks, blobs, blob_offsets, n_programs, axis_params,
+                         n_axis_params, tune, n_res, &B);
+    if (rc) return rc;
+    if (n_walks == 0) return DR_OK;
+    rc = batch_run(*B, ctx()->stream);
+    if (rc) return rc;
+    return batch_read(*B, p_res, q_res, n_res, shadow, status);
+}
+
+int dr_batch_create(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs,
+                    const uint64_t* blob_offsets, int32_t n_programs, const int64_t* axis_params,
+                    uint64_t n_axis_params, const dr_tune* tune, int32_t* batch_out) {
+    if (!batch_out) return DR_ERR_ARG;
+    uint64_t n_res = 0;
+    for (int32_t w = 0; w < n_walks; ++w) {
+        n_res = std::max<uint64_t>(n_res, walks[w].res_offset + walks[w].K);
+        if (walks[w].checkpoint) n_res = std::max<uint64_t>(n_res, walks[w].cp_res_offset + walks[w].K);
+    }
+    std::unique_ptr<Batch> B;
+    int rc = batch_build(walks, n_walks, blobs, blob_offsets, n_programs, axis_params,
+                         n_axis_params, tune, n_res, &B);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    const int32_t id = g_next_batch++;
+    B->id = id;
+    g_batches[id] = std::move(B);
+    *batch_out = id;
+    return DR_OK;
+}
+
+static Batch* find_batch(int32_t id) {
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    auto it = g_batches.find(id);
+    return it == g_batches.end() ? nullptr : it->second.get();
+}
+
+int dr_batch_run(int32_t batch, void* stream) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    if (B->n_walks == 0) return DR_OK;
+    return batch_run(*B, static_cast<cudaStream_t>(stream));
+}
+
+int dr_batch_read(int32_t batch, uint32_t* p_res, uint32_t* q_res, uint64_t n_res, double* shadow,
+                  uint32_t* status) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    DR_CUDA(cudaDeviceSynchronize());
+    return batch_read(*B, p_res, q_res, n_res, shadow, status);
+}
+
+int dr_batch_stats(int32_t batch, uint64_t* prime_steps, uint32_t* n_tiles, uint32_t* n_launches,
+                   float* last_ms) {
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    if (prime_steps) *prime_steps = B->prime_steps;
+    if (n_tiles) *n_tiles = B->n_tiles;
+    if (n_launches) {
+        uint32_t k = 0;
+        for (auto& L : B->launches) k += L.items > 0;
+        *n_launches = k;
+    }
+    if (last_ms) {
+        if (B->ev1 && cudaEventQuery(B->ev1) == cudaSuccess) cudaEventElapsedTime(&B->last_ms, B->ev0, B->ev1);
+        *last_ms = B->last_ms;
+    }
+    return DR_OK;
+}
+
+int dr_batch_set_pipeline(int32_t batch, const dr_pipeline* pl) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    if (!pl) return DR_ERR_ARG;
+    if (pl->delta_mode < DR_DELTA_NONE || pl->delta_mode > DR_DELTA_SELF || pl->topk < 0 ||
+        (pl->delta_mode != DR_DELTA_NONE && !pl->crt) || (pl->topk && pl->delta_mode == DR_DELTA_NONE)) {
+        set_error("inconsistent pipeline (delta needs crt, top-k needs delta)");
+        return DR_ERR_ARG;
+    }
+    if (pl->topk > topk_tile_size() / 2) { set_error("top-k above 2048"); return DR_ERR_UNSUPPORTED; }
+    const uint32_t n = B->n_walks;
+    int Kmax = 1;
+    for (uint32_t w = 0; w < n; ++w) {
+        Kmax = std::max<int>(Kmax, (int)B->h_walk_K[w]);
+        if (pl->delta_mode == DR_DELTA_SELF && B->h_cp_off[w] == UINT64_MAX) {
+            set_error("DR_DELTA_SELF needs a checkpoint on every walk");
+            return DR_ERR_ARG;
+        }
+    }
+    if (pl->crt && Kmax > 1024) { set_error("device CRT supports K <= 1024"); return DR_ERR_UNSUPPORTED; }
+    if (pl->delta_mode == DR_DELTA_FIXED && (!pl->lnum || !pl->lden || pl->l_limbs < 1)) return DR_ERR_ARG;
+    cudaStream_t st = g_ctx->stream;
+    DR_CUDA(cudaDeviceSynchronize());
+    if (B->graph) { cudaGraphExecDestroy(B->graph); B->graph = nullptr; }
+    B->pipe = *pl;
+    B->pipe.lnum = nullptr;
+    B->pipe.lden = nullptr;
+    B->pipe_on = pl->crt != 0;
+    if (!B->pipe_on) return DR_OK;
+    B->Lmax = crt_limbs_for(Kmax);
+    // CRT values grouped by K: rows 4w + {p, q, checkpoint p, checkpoint q}
+    const uint64_t qoff = std::max<uint64_t>(B->n_res, 1);
+    std::map<int, std::vector<std::pair<uint64_t, uint32_t>>> byK;
+    for (uint32_t w = 0; w < n; ++w) {
+        auto& v = byK[(int)B->h_walk_K[w]];
+        v.emplace_back(B->h_res_off[w], 4 * w);
+        v.emplace_back(qoff + B->h_res_off[w], 4 * w + 1);
+        if (B->h_cp_off[w] != UINT64_MAX) {
+            v.emplace_back(B->h_cp_off[w], 4 * w + 2);
+            v.emplace_back(qoff + B->h_cp_off[w], 4 * w + 3);
+        }
+    }
+    std::vector<uint64_t> in;
+    std::vector<uint32_t> out;
+    B->crt_groups.clear();
+    for (auto& kv : byK) {
+        std::shared_ptr<CrtSet> S;
+        rc = crt_tables_std(kv.first, &S);   // build tables now, outside any capture
+        if (rc) return rc;
+        B->crt_groups.push_back({kv.first, (uint32_t)in.size(), (uint32_t)kv.second.size()});
+        for (auto& e : kv.second) { in.push_back(e.first); out.push_back(e.second); }
+    }
+    if ((rc = upload(B->crt_in, in, st))) return rc;
+    if ((rc = upload(B->crt_out, out, st))) return rc;
+    DR_CUDA(B->limbs.alloc(4ull * 4 * std::max<uint32_t>(n, 1) * B->Lmax));
+    DR_CUDA(cudaMemsetAsync(B->limbs.p, 0, B->limbs.bytes, st));
+    DR_CUDA(B->signs.alloc(4ull * 4 * std::max<uint32_t>(n, 1)));
+    DR_CUDA(cudaMemsetAsync(B->signs.p, 0, B->signs.bytes, st));
+    DR_CUDA(B->delta.alloc(8ull * std::max<uint32_t>(n, 1)));
+    if (pl->delta_mode == DR_DELTA_FIXED) {
+        std::vector<uint32_t> ln(pl->lnum, pl->lnum + pl->l_limbs), ld(pl->lden, pl->lden + pl->l_limbs);
+        std::vector<int32_t> sg{pl->lnum_sign};
+        if ((rc = upload(B->tgt_num, ln, st))) return rc;
+        if ((rc = upload(B->tgt_den, ld, st))) return rc;
+        if ((rc = upload(B->tgt_sign, sg, st))) return rc;
+    }
+    B->tk_counts.clear();
+    if (pl->topk > 0 && n > 0) {
+        const int tile = topk_tile_size();
+        int cnt = (int)n;
+        size_t cap = 16;
+        do {
+            B->tk_counts.push_back(cnt);
+            cnt = ((cnt + tile - 1) / tile) * std::min(pl->topk, tile);
+            cap = std::max(cap, (size_t)cnt);
+        } while (cnt > pl->topk);
+        for (int i = 0; i < 2; ++i) {
+            DR_CUDA(B->tk_keys[i].alloc(8 * cap));
+            DR_CUDA(B->tk_idx[i].alloc(4 * cap));
+        }
+        B->tk_final = (int)((B->tk_counts.size() - 1) & 1);
+    }
+    DR_CUDA(cudaStreamSynchronize(st));
+    return DR_OK;
+}
+
+int dr_batch_read_pipeline(int32_t batch, double* delta, int32_t* topk_idx, double* topk_val,
+                           uint32_t* limbs, int32_t* signs, int32_t limb_stride) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    if (!B->pipe_on) { set_error("no pipeline set on this batch"); return DR_ERR_ARG; }
+    DR_CUDA(cudaDeviceSynchronize());
+    const uint32_t n = B->n_walks;
+    std::vector<double> dl;
+    if ((delta || topk_val) && B->pipe.delta_mode != DR_DELTA_NONE) {
+        dl.resize(n);
+        DR_CUDA(cudaMemcpy(dl.data(), B->delta.p, 8ull * n, cudaMemcpyDeviceToHost));
+        if (delta) std::memcpy(delta, dl.data(), 8ull * n);
+    }
+    if ((topk_idx || topk_val) && !B->tk_counts.empty()) {
+        const int keep = std::min<int>(B->pipe.topk, (int)n);
+        std::vector<uint32_t> idx(keep);
+        DR_CUDA(cudaMemcpy(idx.data(), B->tk_idx[B->tk_final].p, 4ull * keep, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < keep; ++i) {
+            if (topk_idx) topk_idx[i] = (int32_t)idx[i];
+            if (topk_val) topk_val[i] = dl[idx[i]];
+        }
+    }
+    if (limbs) {
+        if (limb_stride < B->Lmax) { set_error("limb_stride below the batch's limb count"); return DR_ERR_ARG; }
+        std::vector<uint32_t> tmp(4ull * n * B->Lmax);
+        DR_CUDA(cudaMemcpy(tmp.data(), B->limbs.p, 4ull * tmp.size(), cudaMemcpyDeviceToHost));
+        for (size_t r = 0; r < 4ull * n; ++r) {
+            std::memcpy(limbs + r * limb_stride, tmp.data() + r * B->Lmax, 4ull * B->Lmax);
+            std::memset(limbs + r * limb_stride + B->Lmax, 0, 4ull * (limb_stride - B->Lmax));
+        }
+    }
+    if (signs) DR_CUDA(cudaMemcpy(signs, B->signs.p, 4ull * 4 * n, cudaMemcpyDeviceToHost));
+    return DR_OK;
+}
+
+int dr_batch_destroy(int32_t batch) {
+    std::unique_ptr<Batch> B;
+    {
+        std::lock_guard<std::mutex> lk(g_batch_mu);
+        auto it = g_batches.find(batch);
+        if (it == g_batches.end()) return DR_ERR_HANDLE;
+        B = std::move(it->second);
+        g_batches.erase(it);
+    }
+    if (g_ctx) cudaDeviceSynchronize();
+    return DR_OK;
+}
+
+int dr_crt_batch(const uint32_t* residues, int32_t K, int32_t n, const uint32_t* moduli, uint32_t* limbs,
+                 int32_t limb_stride, int32_t* sign_out, int32_t* nlimbs_out, uint32_t* unsigned_limbs) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    if (n == 0) return DR_OK;
+    if (!residues || !limbs || !sign_out || !nlimbs_out || n < 0) return DR_ERR_ARG;
+    if (K < 1 || K > 1024) { set_error("CRT supports 1 <= K <= 1024"); return K > 1024 ? DR_ERR_UNSUPPORTED : DR_ERR_ARG; }
+    if (limb_stride < crt_limbs_for(K)) { set_error("limb_stride below ceil(31K/32)+2"); return DR_ERR_ARG; }
+    cudaStream_t st = g_ctx->stream;
+    DevBuf r, l, s, nl, ul;
+    DR_CUDA(r.alloc(4ull * K * n));
+    DR_CUDA(l.alloc(4ull * limb_stride * n));
+    DR_CUDA(s.alloc(4ull * n));
+    DR_CUDA(nl.alloc(4ull * n));
+    if (unsigned_limbs) DR_CUDA(ul.alloc(4ull * limb_stride * n));
+    DR_CUDA(cudaMemcpyAsync(r.p, residues, 4ull * K * n, cudaMemcpyHostToDevice, st));
+    rc = crt_device(r.as<uint32_t>(), K, n, moduli, l.as<uint32_t>(), limb_stride, s.as<int32_t>(),
+                    nl.as<int32_t>(), unsigned_limbs ? ul.as<uint32_t>() : nullptr, st);
+    if (rc) return rc;
+    DR_CUDA(cudaMemcpyAsync(limbs, l.p, 4ull * limb_stride * n, cudaMemcpyDeviceToHost, st));
+    DR_CUDA(cudaMemcpyAsync(sign_out, s.p, 4ull * n, cudaMemcpyDeviceToHost, st));
+    DR_CUDA(cudaMemcpyAsync(nlimbs_out, nl.p, 4ull * n, cudaMemcpyDeviceToHost, st));
+    if (unsigned_limbs) DR_CUDA(cudaMemcpyAsync(unsigned_limbs, ul.p, 4ull * limb_stride * n, cudaMemcpyDeviceToHost, st));
+    DR_CUDA(cudaStreamSynchronize(st));
+    return DR_OK;
+}
+
+int dr_crt_batch_device(const uint32_t* residues_d, int32_t K, int32_t n, const uint32_t* moduli_d,
+                        uint32_t* limbs_d, int32_t limb_stride, int32_t* sign_d, int32_t* nlimbs_d,
+                        void* stream) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    if (n == 0) return DR_OK;
+    std::vector<uint32_t> mh;
+    if (moduli_d) {
+        if (K < 1 || K > 1024) return DR_ERR_UNSUPPORTED;
+        mh.resize(K);
+        DR_CUDA(cudaMemcpy(mh.data(), moduli_d, 4ull * K, cudaMemcpyDeviceToHost));
+    }
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g_ctx->stream;
+    return crt_device(residues_d, K, n, moduli_d ? mh.data() : nullptr, limbs_d, limb_stride, sign_d,
+                      nlimbs_d, nullptr, st);
+}
+
+int dr_delta_batch(const uint32_t* p_limbs, const int32_t* p_sign, const uint32_t* q_limbs,
+                   const int32_t* q_sign, int32_t n, int32_t limb_stride, const uint32_t* lnum_limbs,
+                   const int32_t* lnum_sign, const uint32_t* lden_limbs, int32_t l_stride,
+                   int32_t per_item_target, double* delta_out) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    if (n == 0) return DR_OK;
+    if (n < 0 || !p_limbs || !q_limbs || !p_sign || !q_sign || !lnum_limbs || !lnum_sign ||
+        !lden_limbs || !delta_out || limb_stride < 1 || l_stride < 1)
+        return DR_ERR_ARG;
+    if (limb_stride + l_stride > 4096) { set_error("delta limbs above 4096"); return DR_ERR_UNSUPPORTED; }
+    const int nt = per_item_target ? n : 1;
+    cudaStream_t st = g_ctx->stream;
+    DevBuf p, ps, q, qs, ln, lns, ld, out;
+    DR_CUDA(p.alloc(4ull * limb_stride * n));
+    DR_CUDA(q.alloc(4ull * limb_stride * n));
+    DR_CUDA(ps.alloc(4ull * n));
+    DR_CUDA(qs.alloc(4ull * n));
+    DR_CUDA(ln.alloc(4ull * l_stride * nt));
+    DR_CUDA(lns.alloc(4ull * nt));
+    DR_CUDA(ld.alloc(4ull * l_stride * nt));
+    DR_CUDA(out.alloc(8ull * n));
+    DR_CUDA(cudaMemcpyAsync(p.p, p_limbs, 4ull * limb_stride * n, cudaMemcpyHostToDevice, st));
+    DR_CUDA(cudaMemcpyAsync(q.p, q_limbs, 4ull * limb_stride * n, cudaMemcpyHostToDevice, st));
+    DR_CUDA(cudaMemcpyAsync(ps.p, p_sign, 4ull * n, cudaMemcpyHostToDevice, st));
+    DR_CUDA(cudaMemcpyAsync(qs.p, q_sign, 4ull * n, cudaMemcpyHostToDevice, st));
+    DR_CUDA(cudaMemcpyAsync(ln.p, lnum_limbs, 4ull * l_stride * nt, cudaMemcpyHostToDevice, st));
+    DR_CUDA(cudaMemcpyAsync(lns.p, lnum_sign, 4ull * nt, cudaMemcpyHostToDevice, st));
+    DR_CUDA(cudaMemcpyAsync(ld.p, lden_limbs, 4ull * l_stride * nt, cudaMemcpyHostToDevice, st));
+    DeltaArgs D{};
+    D.p = p.as<uint32_t>(); D.ps = ps.as<int32_t>();
+    D.q = q.as<uint32_t>(); D.qs = qs.as<int32_t>();
+    D.n = n; D.nl = limb_stride; D.istride = (size_t)limb_stride; D.sstride = 1;
+    D.ln = ln.as<uint32_t>(); D.lns = lns.as<int32_t>(); D.ld = ld.as<uint32_t>(); D.lds = nullptr;
+    D.lnl = l_stride; D.listride = (size_t)l_stride; D.lsstride = 1;
+    D.per_item = per_item_target ? 1 : 0;
+    D.out = out.as<double>();
+    D.maxlen = ((limb_stride + l_stride + 4) + 1) & ~1;
+    cudaError_t e = launch_delta(D, g_ctx->sms, st);
+    if (e != cudaSuccess) return cuda_fail(e, "delta launch");
+    DR_CUDA(cudaMemcpyAsync(delta_out, out.p, 8ull * n, cudaMemcpyDeviceToHost, st));
+    DR_CUDA(cudaStreamSynchronize(st));
+    return DR_OK;
+}
+
+int dr_topk(const double* delta, int32_t n, int32_t k, int32_t* idx_out, double* val_out) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    if (n < 0 || k < 0 || (n > 0 && !delta)) return DR_ERR_ARG;
+    const int tile = topk_tile_size();
+    if (k > tile / 2) { set_error("k above 2048"); return DR_ERR_UNSUPPORTED; }
+    const int keep = std::min(k, n);
+    if (keep == 0) return DR_OK;
+    cudaStream_t st = g_ctx->stream;
+    DevBuf v, k1, i1, k2, i2;
+    DR_CUDA(v.alloc(8ull * n));
+    DR_CUDA(cudaMemcpyAsync(v.p, delta, 8ull * n, cudaMemcpyHostToDevice, st));
+    const size_t cap = (size_t)((n + tile - 1) / tile) * k + 16;
+    DR_CUDA(k1.alloc(8 * cap)); DR_CUDA(i1.alloc(4 * cap));
+    DR_CUDA(k2.alloc(8 * cap)); DR_CUDA(i2.alloc(4 * cap));
+    int cnt = n;
+    cudaError_t e = launch_topk_tile(v.as<double>(), nullptr, nullptr, cnt, k, k1.as<uint64_t>(), i1.as<uint32_t>(), st);
+    if (e != cudaSuccess) return cuda_fail(e, "topk");
+    cnt = ((cnt + tile - 1) / tile) * std::min(k, tile);
+    bool flip = false;
+    while (cnt > k) {
+        uint64_t* ik = flip ? k2.as<uint64_t>() : k1.as<uint64_t>();
+        uint32_t* ii = flip ? i2.as<uint32_t>() : i1.as<uint32_t>();
+        uint64_t* ok = flip ? k1.as<uint64_t>() : k2.as<uint64_t>();
+        uint32_t* oi = flip ? i1.as<uint32_t>() : i2.as<uint32_t>();
+        e = launch_topk_tile(nullptr, ik, ii, cnt, k, ok, oi, st);
+        if (e != cudaSuccess) return cuda_fail(e, "topk");
+        cnt = ((cnt + tile - 1) / tile) * std::min(k, tile);
+        flip = !flip;
+        if (cnt <= k) break;
+    }
+    std::vector<uint32_t> idx(keep);
+    DR_CUDA(cudaMemcpyAsync(idx.data(), flip ? i2.p : i1.p, 4ull * keep, cudaMemcpyDeviceToHost, st));
+    DR_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < keep; ++i) {
+        idx_out[i] = (int32_t)idx[i];
+        if (val_out) val_out[i] = delta[idx[i]];
+    }
+    return DR_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,121 @@
+// Host engine: device context, prepared walk batches, CRT/delta/top-k helpers.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/dreams_b200.h"
+#include "dr_types.h"
+#include "program.h"
+
+namespace dr {
+
+// Owning device allocation.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        if (n == 0) n = 16;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e == cudaSuccess) bytes = n;
+        return e;
+    }
+    template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct CrtSet {
+    int K = 0, L = 0;
+    DevBuf moduli, pinv, r2, ginv, Mlimbs, Mtotal;
+};
+
+struct Context {
+    int device = -1;
+    int sms = 0;
+    cudaStream_t stream = nullptr, side = nullptr;
+    std::vector<cudaStream_t> pool;   // launch groups of a batch run concurrently on these
+    DevBuf primes, pinv, r2;   // DR_MAX_K-entry prime table
+    std::mutex mu;
+    std::unordered_map<std::string, std::shared_ptr<Plan>> plan_cache;
+    std::map<int, std::shared_ptr<CrtSet>> crt_std;  // CRT tables of the standard primes
+};
+
+Context* ctx();           // nullptr before dr_init
+int ensure_ctx();         // DR_OK or DR_ERR_NOT_INIT
+
+// Get (and cache) the plan of a program blob.
+int get_plan(const uint8_t* blob, uint64_t size, std::shared_ptr<Plan>* out, std::string* err);
+
+// Standard-prime CRT tables for K (cached).
+int crt_tables_std(int K, std::shared_ptr<CrtSet>* out);
+int crt_limbs_for(int K);  // L: limbs of prod(moduli) + 1
+
+struct LaunchSpec {
+    int kind;                  // 0 walk, 1 shadow (interpreted), 2 shadow (integer differences)
+    uint32_t cls, m, D;
+    uint32_t off, count;       // tiles / list entries of this launch
+    uint32_t items;            // work items (tiles, walks or 32-walk groups)
+    uint32_t queue;            // queue counter index
+    uint32_t rows_regs, rows_consts, rows_stage, rows_per_warp;
+    size_t smem;
+    int grid, block;
+};
+
+struct Batch {
+    int32_t id = 0;
+    uint32_t n_walks = 0;
+    uint64_t n_res = 0;
+    uint64_t prime_steps = 0;
+    std::vector<LaunchSpec> launches;
+    uint32_t n_tiles = 0, n_groups = 0, n_queues = 0;
+    uint32_t chunk_stride = 0;   // words per chunk-product slot
+    DevBuf progs, code, consts, walks, axis, tiles, groups, group_done, chunkP, chunkSig;
+    DevBuf shadow_list, queues, res, shadow, status;   // res: p residues then q residues
+    // device pipeline (CRT -> delta -> top-k)
+    dr_pipeline pipe{};
+    bool pipe_on = false;
+    int Lmax = 0;                       // limbs per reconstructed value
+    struct CrtGroup { int K; uint32_t off, count; };
+    std::vector<CrtGroup> crt_groups;
+    DevBuf crt_in, crt_out, limbs, signs, delta, tgt_num, tgt_den, tgt_sign;
+    DevBuf tk_keys[2], tk_idx[2];
+    std::vector<int> tk_counts;         // values entering each top-k pass
+    int tk_final = 0;                   // buffer holding the final top-k
+    std::vector<uint32_t> h_walk_K;
+    std::vector<uint64_t> h_res_off, h_cp_off;
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr, join = nullptr;
+    std::vector<cudaEvent_t> joins;
+    float last_ms = 0.f;
+    bool has_shadow = false;
+    ~Batch();
+};
+
+// Build a batch (validation, planning, upload).  engine_override forces an engine.
+int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs,
+                const uint64_t* blob_offsets, int32_t n_programs, const int64_t* axis_params,
+                uint64_t n_axis_params, const dr_tune* tune, uint64_t n_res,
+                std::unique_ptr<Batch>* out);
+int batch_run(Batch& B, cudaStream_t st);
+int batch_read(Batch& B, uint32_t* p_res, uint32_t* q_res, uint64_t n_res, double* shadow,
+               uint32_t* status);
+
+int cuda_fail(cudaError_t e, const char* where);
+
+}  // namespace dr

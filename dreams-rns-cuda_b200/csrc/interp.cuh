@@ -1,0 +1,143 @@
+// Warp-uniform bytecode interpreters.
+//
+// All 32 lanes of a warp run the same program at the same time, so every
+// dispatch (instruction fetch from global memory through the read-only path,
+// jump on the opcode) is uniform and never diverges; lanes differ only in
+// their data (one prime per lane for the residue interpreter, one step or one
+// walk per lane for the float interpreters).  The register file lives in
+// shared memory as [register][lane], so every access is bank-conflict free.
+// Programs arrive compacted by the host planner (a few live registers, NOPs
+// and everything after END removed, STORE's operand b = output slot).
+#pragma once
+#include <stdint.h>
+
+#include "dr_types.h"
+#include "modarith.cuh"
+
+namespace dr {
+
+// Residue interpreter (reference runner.py:246-308): registers, constants and
+// axis values are Montgomery residues [slot*32 + lane].  Returns true when an
+// INV met a zero operand (the reference's "dead lane", config.h:166-169).
+__device__ __forceinline__ bool interp_modp(const uint4* __restrict__ code, uint32_t n,
+                                            uint32_t* __restrict__ rf,
+                                            const uint32_t* __restrict__ cst,
+                                            const uint32_t* __restrict__ axv, uint32_t step_m,
+                                            uint32_t* __restrict__ out, const Mont& M, int lane) {
+    bool inv0 = false;
+#pragma unroll 1
+    for (uint32_t pc = 0; pc < n; ++pc) {
+        const uint4 in = __ldg(code + pc);
+        switch (in.x) {
+            case OP_LOAD_X: rf[in.z * 32 + lane] = axv[in.y * 32 + lane]; break;
+            case OP_LOAD_C: rf[in.z * 32 + lane] = cst[in.y * 32 + lane]; break;
+            case OP_LOAD_N: rf[in.y * 32 + lane] = step_m; break;
+            case OP_ADD: rf[in.w * 32 + lane] = addm(rf[in.y * 32 + lane], rf[in.z * 32 + lane], M.p); break;
+            case OP_SUB: rf[in.w * 32 + lane] = subm(rf[in.y * 32 + lane], rf[in.z * 32 + lane], M.p); break;
+            case OP_MUL: rf[in.w * 32 + lane] = mmul(rf[in.y * 32 + lane], rf[in.z * 32 + lane], M); break;
+            case OP_NEG: rf[in.z * 32 + lane] = negm(rf[in.y * 32 + lane], M.p); break;
+            case OP_POW2: {
+                const uint32_t v = rf[in.y * 32 + lane];
+                rf[in.z * 32 + lane] = mmul(v, v, M);
+                break;
+            }
+            case OP_POW3: {
+                const uint32_t v = rf[in.y * 32 + lane];
+                rf[in.z * 32 + lane] = mmul(mmul(v, v, M), v, M);
+                break;
+            }
+            case OP_INV: {
+                const uint32_t v = rf[in.y * 32 + lane];
+                inv0 |= (v == 0u);
+                rf[in.z * 32 + lane] = minv(v, M);
+                break;
+            }
+            case OP_STORE: out[in.z * 32 + lane] = rf[in.y * 32 + lane]; break;
+            default: break;
+        }
+    }
+    return inv0;
+}
+
+// x^3 rounded once to nearest from the exact product (error-free
+// transformations), the rounding the reference's float64 x**3 delivers
+// whenever the platform pow is correctly rounded.
+__device__ __forceinline__ double cube_rn(double x) {
+    const double h = __dmul_rn(x, x);
+    const double e = __fma_rn(x, x, -h);        // x*x = h + e exactly
+    const double p1 = __dmul_rn(h, x);
+    const double e1 = __fma_rn(h, x, -p1);      // h*x = p1 + e1 exactly
+    return __dadd_rn(p1, __fma_rn(e, x, e1));
+}
+
+// Float64 interpreter (reference runner.py:311-364, cmf_walk.py:261-313).
+// rf is a [register][32] double array; axv holds the axis values of each
+// lane's step.  No contraction: every operation is an explicit IEEE op.
+__device__ __forceinline__ void interp_f64(const uint4* __restrict__ code, uint32_t n,
+                                           double* __restrict__ rf,
+                                           const int64_t* __restrict__ consts,
+                                           const double* __restrict__ axv, double step,
+                                           double* __restrict__ out, int lane) {
+#pragma unroll 1
+    for (uint32_t pc = 0; pc < n; ++pc) {
+        const uint4 in = __ldg(code + pc);
+        switch (in.x) {
+            case OP_LOAD_X: rf[in.z * 32 + lane] = axv[in.y * 32 + lane]; break;
+            case OP_LOAD_C: rf[in.z * 32 + lane] = __ll2double_rn(__ldg(consts + in.y)); break;
+            case OP_LOAD_N: rf[in.y * 32 + lane] = step; break;
+            case OP_ADD: rf[in.w * 32 + lane] = __dadd_rn(rf[in.y * 32 + lane], rf[in.z * 32 + lane]); break;
+            case OP_SUB: rf[in.w * 32 + lane] = __dsub_rn(rf[in.y * 32 + lane], rf[in.z * 32 + lane]); break;
+            case OP_MUL: rf[in.w * 32 + lane] = __dmul_rn(rf[in.y * 32 + lane], rf[in.z * 32 + lane]); break;
+            case OP_NEG: rf[in.z * 32 + lane] = -rf[in.y * 32 + lane]; break;
+            case OP_POW2: {
+                const double v = rf[in.y * 32 + lane];
+                rf[in.z * 32 + lane] = __dmul_rn(v, v);
+                break;
+            }
+            case OP_POW3: rf[in.z * 32 + lane] = cube_rn(rf[in.y * 32 + lane]); break;
+            case OP_INV: {
+                const double v = rf[in.y * 32 + lane];
+                rf[in.z * 32 + lane] = fabs(v) > 1e-300 ? __ddiv_rn(1.0, v) : 0.0;
+                break;
+            }
+            case OP_STORE: out[in.z * 32 + lane] = rf[in.y * 32 + lane]; break;
+            default: break;
+        }
+    }
+}
+
+// Exact int64 interpreter for programs without INV whose values the host has
+// bounded below 2^53 (integer-valued float shadow).
+__device__ __forceinline__ void interp_i64(const uint4* __restrict__ code, uint32_t n,
+                                           int64_t* __restrict__ rf,
+                                           const int64_t* __restrict__ consts,
+                                           const int64_t* __restrict__ axv, int64_t step,
+                                           int64_t* __restrict__ out, int lane) {
+#pragma unroll 1
+    for (uint32_t pc = 0; pc < n; ++pc) {
+        const uint4 in = __ldg(code + pc);
+        switch (in.x) {
+            case OP_LOAD_X: rf[in.z * 32 + lane] = axv[in.y * 32 + lane]; break;
+            case OP_LOAD_C: rf[in.z * 32 + lane] = __ldg(consts + in.y); break;
+            case OP_LOAD_N: rf[in.y * 32 + lane] = step; break;
+            case OP_ADD: rf[in.w * 32 + lane] = rf[in.y * 32 + lane] + rf[in.z * 32 + lane]; break;
+            case OP_SUB: rf[in.w * 32 + lane] = rf[in.y * 32 + lane] - rf[in.z * 32 + lane]; break;
+            case OP_MUL: rf[in.w * 32 + lane] = rf[in.y * 32 + lane] * rf[in.z * 32 + lane]; break;
+            case OP_NEG: rf[in.z * 32 + lane] = -rf[in.y * 32 + lane]; break;
+            case OP_POW2: {
+                const int64_t v = rf[in.y * 32 + lane];
+                rf[in.z * 32 + lane] = v * v;
+                break;
+            }
+            case OP_POW3: {
+                const int64_t v = rf[in.y * 32 + lane];
+                rf[in.z * 32 + lane] = v * v * v;
+                break;
+            }
+            case OP_STORE: out[in.z * 32 + lane] = rf[in.y * 32 + lane]; break;
+            default: break;
+        }
+    }
+}
+
+}  // namespace dr

@@ -1,0 +1,81 @@
+// Launch entry points of the kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dr {
+
+struct WalkArgs;
+struct ShadowArgs;
+
+// Garner CRT tables of one moduli set (crt.cu).
+struct CrtTables {
+    const uint32_t* moduli;   // [K]
+    const uint32_t* pinv;     // [K]
+    const uint32_t* r2;       // [K]
+    const uint32_t* ginv;     // [K]  inv(M_i mod p_i), Montgomery form mod p_i
+    const uint32_t* Mlimbs;   // [K][L]  M_i (M_0 = 1), little-endian limbs
+    const uint32_t* Mtotal;   // [L]  product of all moduli
+    int K, L;
+};
+
+// Delta kernel arguments (delta_topk.cu).  Item i reads p at p + i*istride,
+// q at q + i*istride (nl limbs each), signs at ps/qs + i*sstride, and target
+// t = per_item ? i : 0 as ln/ld + t*listride (lnl limbs), sign lns[t*lsstride]
+// times (lds ? lds[t*lsstride] : 1); the target denominator's magnitude is used.
+struct DeltaArgs {
+    const uint32_t* p; const uint32_t* q;
+    const int32_t* ps; const int32_t* qs;
+    int n, nl;
+    size_t istride, sstride;
+    const uint32_t* ln; const uint32_t* ld;
+    const int32_t* lns; const int32_t* lds;
+    int lnl, per_item;
+    size_t listride, lsstride;
+    double* out;
+    int maxlen;                              // product length bound (limbs)
+};
+
+cudaError_t launch_crt_setup(const uint32_t* moduli, int K, int L, uint32_t* pinv, uint32_t* r2,
+                             uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal, cudaStream_t st);
+// in_off[j]: offset of value j's K residues (null: j*K); out_idx[j]: output
+// row of value j in limbs/sign/nl (null: j).
+cudaError_t launch_crt(const uint32_t* res, int n, const CrtTables& T, uint32_t* limbs, int stride,
+                       int32_t* sign, int32_t* nl, uint32_t* ul, int sms, cudaStream_t st,
+                       const uint64_t* in_off = nullptr, const uint32_t* out_idx = nullptr);
+cudaError_t launch_delta(const DeltaArgs& D, int sms, cudaStream_t st);
+cudaError_t launch_topk_tile(const double* vals, const uint64_t* in_keys, const uint32_t* in_idx,
+                             int n, int k, uint64_t* out_keys, uint32_t* out_idx, cudaStream_t st);
+int topk_tile_size();
+
+// occ != nullptr: only report resident blocks per SM for (block, smem).
+cudaError_t walk_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block, size_t smem,
+                          cudaStream_t st, const WalkArgs& a, int* occ);
+cudaError_t shadow_interp_dispatch(uint32_t m, int grid, int block, size_t smem, cudaStream_t st,
+                                   const ShadowArgs& a, int* occ);
+cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block,
+                               size_t smem, cudaStream_t st, const ShadowArgs& a, int* occ);
+
+// per-class dispatchers (one translation unit each, compiled in parallel)
+cudaError_t walk_dispatch_companion(uint32_t m, uint32_t D, int grid, int block, size_t smem,
+                                    cudaStream_t st, const WalkArgs& a, int* occ);
+cudaError_t walk_dispatch_rational(uint32_t m, uint32_t D, int grid, int block, size_t smem,
+                                   cudaStream_t st, const WalkArgs& a, int* occ);
+cudaError_t walk_dispatch_dense(uint32_t m, uint32_t D, int grid, int block, size_t smem,
+                                cudaStream_t st, const WalkArgs& a, int* occ);
+cudaError_t walk_dispatch_interp(uint32_t m, int grid, int block, size_t smem, cudaStream_t st,
+                                 const WalkArgs& a, int* occ);
+
+template <typename KernelT, typename ArgT>
+inline cudaError_t run_kernel(KernelT k, int grid, int block, size_t smem, cudaStream_t st,
+                              const ArgT& a, int* occ) {
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, block, smem);
+    k<<<grid, block, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace dr

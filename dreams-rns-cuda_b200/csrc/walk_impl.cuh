@@ -1,0 +1,418 @@
+// Persistent walk kernels.
+//
+// Work unit = tile: one depth chunk [s0, s1) of one (walk, block of <= 32
+// primes).  Each warp of a persistent grid pops tiles from a device counter
+// (tiles are sorted longest first on the host) and runs the whole chunk in
+// registers, lane = prime.  A chunk computes the product of its step
+// matrices, starting from the walk's initial matrix (chunk 0) or I.  The
+// warp that completes the last chunk of a (walk, prime block) -- detected by
+// an atomic counter, so nobody ever waits -- multiplies the chunk products in
+// order (matrix products are associative and the arithmetic is exact mod p),
+// divides out the accumulated denominator once, and writes the residues.
+//
+// Per step the step matrix comes from forward-difference streams (classes
+// COMPANION, RATIONAL, DENSE; streams initialised by interpreting the derived
+// program at D+1 steps) or from the bytecode interpreter (class INTERP).
+#pragma once
+#include <stdint.h>
+
+#include "../../include/dreams_b200.h"
+#include "dr_types.h"
+#include "interp.cuh"
+#include "modarith.cuh"
+
+namespace dr {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+struct WalkArgs {
+    const DevProgram* progs;
+    const uint4* code;          // instructions of every program
+    const int64_t* consts;      // constant pools
+    const DevWalk* walks;
+    const int64_t* axis;        // 4 int64 per axis per walk
+    const DevTile* tiles;       // this launch's tiles
+    const DevGroup* groups;
+    uint32_t n_tiles;
+    uint32_t* queue;            // tile counter of this launch (zeroed before launch)
+    uint32_t* group_done;       // per-group completion counters (self re-arming)
+    uint32_t* chunk_P;          // [slot][m*m][32], slots chunk_stride words apart
+    uint32_t chunk_stride;      // words per slot: max m*m of the batch times 32
+    uint32_t* chunk_sig;        // [slot][32]
+    const uint32_t* primes;     // prime table and Montgomery constants
+    const uint32_t* pinv;
+    const uint32_t* r2;
+    uint32_t* p_res;
+    uint32_t* q_res;
+    uint32_t* status;
+    // per-warp shared memory layout, in 32-word rows
+    uint32_t rows_regs, rows_consts, rows_stage;
+    uint32_t rows_per_warp;
+};
+
+struct WarpMem {
+    uint32_t* rf;
+    uint32_t* cst;
+    uint32_t* x0;
+    uint32_t* dx;
+    uint32_t* cur;
+    uint32_t* stage;
+};
+
+__device__ __forceinline__ WarpMem warp_mem(const WalkArgs& A, uint32_t* smem, int warp) {
+    WarpMem w;
+    uint32_t* base = smem + (size_t)warp * A.rows_per_warp * 32;
+    w.rf = base;
+    w.cst = w.rf + A.rows_regs * 32;
+    w.x0 = w.cst + A.rows_consts * 32;
+    w.dx = w.x0 + kMaxAxes * 32;
+    w.cur = w.dx + kMaxAxes * 32;
+    w.stage = w.cur + kMaxAxes * 32;
+    return w;
+}
+
+// Per-lane setup at the start of a tile: modulus, constants and axis
+// progressions in Montgomery form.  LOAD_X of axis a at step s is
+// x0_a + s * dx_a with x0 = sn*td*inv(sd*td), dx = tn*sd*inv(sd*td)
+// (reference cmf_walk.py:221-224, 348-358: the same residues).
+__device__ __forceinline__ Mont tile_setup(const WalkArgs& A, const DevTile& T, const DevWalk& W,
+                                           const DevProgram& G, const WarpMem& wm, int lane) {
+    const uint32_t k = T.prime0 + min((uint32_t)lane, T.nprimes - 1u);
+    const Mont M = make_mont(__ldg(A.primes + k), __ldg(A.pinv + k), __ldg(A.r2 + k));
+    for (uint32_t i = 0; i < G.n_consts; ++i)
+        wm.cst[i * 32 + lane] = to_mont_i64(__ldg(A.consts + G.c_off + i), M);
+    for (uint32_t a = 0; a < G.dim; ++a) {
+        const int64_t* ax = A.axis + W.axis_off + 4 * a;
+        const uint32_t sn = to_mont_i64(__ldg(ax + 0), M), sd = to_mont_i64(__ldg(ax + 1), M);
+        const uint32_t tn = to_mont_i64(__ldg(ax + 2), M), td = to_mont_i64(__ldg(ax + 3), M);
+        const uint32_t icd = minv(mmul(sd, td, M), M);
+        wm.x0[a * 32 + lane] = mmul(mmul(sn, td, M), icd, M);
+        wm.dx[a * 32 + lane] = mmul(mmul(tn, sd, M), icd, M);
+    }
+    if (G.zero_reg != 0xffffffffu) wm.rf[G.zero_reg * 32 + lane] = 0u;
+    __syncwarp();
+    return M;
+}
+
+__device__ __forceinline__ void set_axes(const WarpMem& wm, uint32_t dim, uint32_t s_m,
+                                         const Mont& M, int lane) {
+    for (uint32_t a = 0; a < dim; ++a)
+        wm.cur[a * 32 + lane] = addm(wm.x0[a * 32 + lane], mmul(s_m, wm.dx[a * 32 + lane], M), M.p);
+}
+
+// Evaluate the original program at step s into stage[entry][lane] (m*m entries,
+// zero where not stored, as the reference's fresh zero matrix).
+__device__ __forceinline__ bool eval_original(const WalkArgs& A, const DevProgram& G,
+                                              const WarpMem& wm, uint64_t s, const Mont& M,
+                                              int lane) {
+    const uint32_t s_m = to_mont_u64(s, M);
+    set_axes(wm, G.dim, s_m, M, lane);
+    for (uint32_t e = 0; e < G.m * G.m; ++e) wm.stage[e * 32 + lane] = 0u;
+    // the derived program may have used the zero register's slot
+    if (G.zero_reg != 0xffffffffu) wm.rf[G.zero_reg * 32 + lane] = 0u;
+    __syncwarp();
+    const bool z = interp_modp(A.code + G.op_off, G.n_ops, wm.rf, wm.cst, wm.cur, s_m, wm.stage, M, lane);
+    __syncwarp();
+    return z;
+}
+
+// Initial chunk matrix: P0 of the walk for chunk 0, else I (Montgomery form).
+template <int M_>
+__device__ __forceinline__ void init_P(uint32_t (&P)[M_][M_], const DevWalk& W, bool first,
+                                       const Mont& M) {
+#pragma unroll
+    for (int i = 0; i < M_; ++i)
+#pragma unroll
+        for (int j = 0; j < M_; ++j) P[i][j] = (i == j) ? M.one : 0u;
+    if (first && (W.flags & DR_WALK_INIT_PCF) && M_ >= 2) P[0][1] = to_mont_i64(W.a0, M);
+}
+
+// P <- P * X for a dense X given per lane
+template <int M_>
+__device__ __forceinline__ void mat_mul_dense(uint32_t (&P)[M_][M_], const uint32_t (&X)[M_][M_],
+                                              const Mont& M) {
+    uint32_t R[M_][M_];
+#pragma unroll
+    for (int i = 0; i < M_; ++i)
+#pragma unroll
+        for (int j = 0; j < M_; ++j) {
+            uint32_t col[M_];
+#pragma unroll
+            for (int k = 0; k < M_; ++k) col[k] = X[k][j];
+            R[i][j] = mdot<M_>(P[i], col, M);
+        }
+#pragma unroll
+    for (int i = 0; i < M_; ++i)
+#pragma unroll
+        for (int j = 0; j < M_; ++j) P[i][j] = R[i][j];
+}
+
+// P <- P * X for X read from stage[entry][lane]
+template <int M_>
+__device__ __forceinline__ void mat_mul_stage(uint32_t (&P)[M_][M_], const uint32_t* stage,
+                                              const Mont& M, int lane) {
+    uint32_t X[M_][M_];
+#pragma unroll
+    for (int i = 0; i < M_; ++i)
+#pragma unroll
+        for (int j = 0; j < M_; ++j) X[i][j] = stage[(i * M_ + j) * 32 + lane];
+    mat_mul_dense<M_>(P, X, M);
+}
+
+// Write p = P[0][m-1], q = P[q_row][m-1] divided by sig (Montgomery) as plain
+// residues for the active lanes.
+template <int M_>
+__device__ __forceinline__ void emit(const WalkArgs& A, const DevTile& T, const DevWalk& W,
+                                     uint64_t res_off, const uint32_t (&P)[M_][M_], uint32_t sig,
+                                     bool scaled, const Mont& M, int lane) {
+    uint32_t pv = P[0][M_ - 1];
+    uint32_t qv = P[0][M_ - 1];
+#pragma unroll
+    for (int i = 0; i < M_; ++i)
+        if ((uint32_t)i == W.q_row) qv = P[i][M_ - 1];
+    if (scaled) {
+        const uint32_t iv = minv(sig, M);
+        pv = mmul(pv, iv, M);
+        qv = mmul(qv, iv, M);
+    }
+    if ((uint32_t)lane < T.nprimes) {
+        A.p_res[res_off + T.prime0 + lane] = from_mont(pv, M);
+        A.q_res[res_off + T.prime0 + lane] = from_mont(qv, M);
+    }
+}
+
+// End of a tile: write outputs directly (single chunk) or publish the chunk
+// product; the last chunk of the group combines all chunks in order.
+template <int M_>
+__device__ __forceinline__ void finish_tile(const WalkArgs& A, const DevTile& T, const DevWalk& W,
+                                            const uint32_t (&P)[M_][M_], uint32_t sig, bool scaled,
+                                            const Mont& M, int lane) {
+    const DevGroup Gr = A.groups[T.group];
+    if (Gr.n_chunks == 1) {
+        emit<M_>(A, T, W, W.res_off, P, sig, scaled, M, lane);
+        return;
+    }
+    uint32_t* dst = A.chunk_P + (size_t)T.slot * A.chunk_stride;
+#pragma unroll
+    for (int e = 0; e < M_ * M_; ++e) __stcg(dst + e * 32 + lane, P[e / M_][e % M_]);
+    if (scaled) __stcg(A.chunk_sig + (size_t)T.slot * 32 + lane, sig);
+    __threadfence();
+    __syncwarp();
+    uint32_t old = 0;
+    if (lane == 0) old = atomicAdd(A.group_done + T.group, 1u);
+    old = __shfl_sync(kFull, old, 0);
+    if (old != Gr.n_chunks - 1) return;
+    __threadfence();
+    uint32_t Q[M_][M_];
+    uint32_t acc = M.one;
+    for (uint32_t c = 0; c < Gr.n_chunks; ++c) {
+        const uint32_t* src = A.chunk_P + (size_t)(Gr.slot0 + c) * A.chunk_stride;
+        if (c == 0) {
+#pragma unroll
+            for (int e = 0; e < M_ * M_; ++e) Q[e / M_][e % M_] = __ldcg(src + e * 32 + lane);
+        } else {
+            uint32_t X[M_][M_];
+#pragma unroll
+            for (int e = 0; e < M_ * M_; ++e) X[e / M_][e % M_] = __ldcg(src + e * 32 + lane);
+            mat_mul_dense<M_>(Q, X, M);
+        }
+        if (scaled) acc = mmul(acc, __ldcg(A.chunk_sig + (size_t)(Gr.slot0 + c) * 32 + lane), M);
+        if (c + 1 == Gr.cp_chunks) emit<M_>(A, T, W, W.cp_res_off, Q, acc, scaled, M, lane);
+    }
+    emit<M_>(A, T, W, W.res_off, Q, acc, scaled, M, lane);
+    if (lane == 0) A.group_done[T.group] = 0u;  // re-armed for the next run of this batch
+}
+
+// Difference tables: fd[i][j] = Delta^j stream_i(s0), from the derived
+// program evaluated at s0 .. s0+Dp (Dp = program degree <= D).
+template <int NS, int D>
+__device__ __forceinline__ bool fd_init(uint32_t (&fd)[NS][D + 1], const WalkArgs& A,
+                                        const DevProgram& G, const WarpMem& wm, uint64_t s0,
+                                        const Mont& M, int lane) {
+    const uint32_t Dp = G.degree;
+    bool inv0 = false;
+    for (uint32_t j = 0; j <= Dp; ++j) {
+        const uint32_t s_m = to_mont_u64(s0 + j, M);
+        set_axes(wm, G.dim, s_m, M, lane);
+        __syncwarp();
+        inv0 |= interp_modp(A.code + G.dop_off, G.dn_ops, wm.rf, wm.cst, wm.cur, s_m,
+                            wm.stage + j * NS * 32, M, lane);
+        __syncwarp();
+    }
+#pragma unroll
+    for (int j = 0; j <= D; ++j)
+#pragma unroll
+        for (int i = 0; i < NS; ++i) fd[i][j] = ((uint32_t)j <= Dp) ? wm.stage[(j * NS + i) * 32 + lane] : 0u;
+#pragma unroll
+    for (int lvl = 1; lvl <= D; ++lvl)
+#pragma unroll
+        for (int j = D; j >= lvl; --j)
+            if ((uint32_t)j <= Dp)
+#pragma unroll
+                for (int i = 0; i < NS; ++i) fd[i][j] = subm(fd[i][j], fd[i][j - 1], M.p);
+    __syncwarp();
+    return inv0;
+}
+
+template <int NS, int D>
+__device__ __forceinline__ void fd_step(uint32_t (&fd)[NS][D + 1], uint32_t p) {
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+        for (int j = 0; j < D; ++j) fd[i][j] = addm(fd[i][j], fd[i][j + 1], p);
+}
+
+// ---- class bodies -----------------------------------------------------------
+
+// COMPANION: new column j = old column j+1, new last column = P * c.
+template <int M_, int D>
+__device__ __forceinline__ void tile_companion(const WalkArgs& A, const DevTile& T, const DevWalk& W,
+                                               const DevProgram& G, const WarpMem& wm, int lane) {
+    const Mont M = tile_setup(A, T, W, G, wm, lane);
+    uint32_t fd[M_][D + 1];
+    bool inv0 = fd_init<M_, D>(fd, A, G, wm, T.s0, M, lane);
+    uint32_t P[M_][M_];
+    init_P<M_>(P, W, T.chunk == 0, M);
+    const uint32_t n = (uint32_t)(T.s1 - T.s0);
+#pragma unroll 2
+    for (uint32_t t = 0; t < n; ++t) {
+        uint32_t c[M_];
+#pragma unroll
+        for (int i = 0; i < M_; ++i) c[i] = fd[i][0];
+        uint32_t nc[M_];
+#pragma unroll
+        for (int i = 0; i < M_; ++i) nc[i] = mdot<M_>(P[i], c, M);
+#pragma unroll
+        for (int i = 0; i < M_; ++i) {
+#pragma unroll
+            for (int j = 0; j + 1 < M_; ++j) P[i][j] = P[i][j + 1];
+            P[i][M_ - 1] = nc[i];
+        }
+        fd_step<M_, D>(fd, M.p);
+    }
+    if (__any_sync(kFull, inv0 && (uint32_t)lane < T.nprimes) && lane == 0)
+        atomicOr(A.status + T.walk, DR_STATUS_INV0);
+    finish_tile<M_>(A, T, W, P, M.one, false, M, lane);
+}
+
+// RATIONAL: M' = g*M with streams c'_0..c'_{m-1} (last column) and g (stream m).
+template <int M_, int D>
+__device__ __forceinline__ void tile_rational(const WalkArgs& A, const DevTile& T, const DevWalk& W,
+                                              const DevProgram& G, const WarpMem& wm, int lane) {
+    const Mont M = tile_setup(A, T, W, G, wm, lane);
+    uint32_t fd[M_ + 1][D + 1];
+    bool inv0 = fd_init<M_ + 1, D>(fd, A, G, wm, T.s0, M, lane);
+    uint32_t P[M_][M_];
+    init_P<M_>(P, W, T.chunk == 0, M);
+    uint32_t sig = M.one;
+    const uint32_t n = (uint32_t)(T.s1 - T.s0);
+#pragma unroll 1
+    for (uint32_t t = 0; t < n; ++t) {
+        const uint32_t g = fd[M_][0];
+        if (__any_sync(kFull, g == 0u)) {
+            // some denominator is 0 mod p: the reference's INV(0) -> 0 step,
+            // re-evaluated exactly from the original bytecode
+            inv0 = true;
+            eval_original(A, G, wm, T.s0 + t, M, lane);
+            mat_mul_stage<M_>(P, wm.stage, M, lane);
+        } else {
+            uint32_t c[M_];
+#pragma unroll
+            for (int i = 0; i < M_; ++i) c[i] = fd[i][0];
+            uint32_t nc[M_];
+#pragma unroll
+            for (int i = 0; i < M_; ++i) nc[i] = mdot<M_>(P[i], c, M);
+#pragma unroll
+            for (int i = 0; i < M_; ++i) {
+#pragma unroll
+                for (int j = 0; j + 1 < M_; ++j) P[i][j] = mmul(P[i][j + 1], g, M);
+                P[i][M_ - 1] = nc[i];
+            }
+            sig = mmul(sig, g, M);
+        }
+        fd_step<M_ + 1, D>(fd, M.p);
+    }
+    if (__any_sync(kFull, inv0 && (uint32_t)lane < T.nprimes) && lane == 0)
+        atomicOr(A.status + T.walk, DR_STATUS_INV0);
+    finish_tile<M_>(A, T, W, P, sig, true, M, lane);
+}
+
+// DENSE: every entry is a stream; full P * M.
+template <int M_, int D>
+__device__ __forceinline__ void tile_dense(const WalkArgs& A, const DevTile& T, const DevWalk& W,
+                                           const DevProgram& G, const WarpMem& wm, int lane) {
+    const Mont M = tile_setup(A, T, W, G, wm, lane);
+    uint32_t fd[M_ * M_][D + 1];
+    bool inv0 = fd_init<M_ * M_, D>(fd, A, G, wm, T.s0, M, lane);
+    uint32_t P[M_][M_];
+    init_P<M_>(P, W, T.chunk == 0, M);
+    const uint32_t n = (uint32_t)(T.s1 - T.s0);
+#pragma unroll 1
+    for (uint32_t t = 0; t < n; ++t) {
+        uint32_t X[M_][M_];
+#pragma unroll
+        for (int e = 0; e < M_ * M_; ++e) X[e / M_][e % M_] = fd[e][0];
+        mat_mul_dense<M_>(P, X, M);
+        fd_step<M_ * M_, D>(fd, M.p);
+    }
+    if (__any_sync(kFull, inv0 && (uint32_t)lane < T.nprimes) && lane == 0)
+        atomicOr(A.status + T.walk, DR_STATUS_INV0);
+    finish_tile<M_>(A, T, W, P, M.one, false, M, lane);
+}
+
+// INTERP: the bytecode is interpreted at every step (reference semantics
+// directly; also the plain one-walk-per-launch baseline).
+template <int M_>
+__device__ __forceinline__ void tile_interp(const WalkArgs& A, const DevTile& T, const DevWalk& W,
+                                            const DevProgram& G, const WarpMem& wm, int lane) {
+    const Mont M = tile_setup(A, T, W, G, wm, lane);
+    uint32_t P[M_][M_];
+    init_P<M_>(P, W, T.chunk == 0, M);
+    bool inv0 = false;
+    // axis values advance by dx per step; the step counter by one
+    uint32_t s_m = to_mont_u64(T.s0, M);
+    set_axes(wm, G.dim, s_m, M, lane);
+    const uint32_t n = (uint32_t)(T.s1 - T.s0);
+#pragma unroll 1
+    for (uint32_t t = 0; t < n; ++t) {
+        for (uint32_t e = 0; e < (uint32_t)(M_ * M_); ++e) wm.stage[e * 32 + lane] = 0u;
+        __syncwarp();
+        inv0 |= interp_modp(A.code + G.op_off, G.n_ops, wm.rf, wm.cst, wm.cur, s_m, wm.stage, M, lane);
+        __syncwarp();
+        mat_mul_stage<M_>(P, wm.stage, M, lane);
+        s_m = addm(s_m, M.one, M.p);
+        for (uint32_t a = 0; a < G.dim; ++a)
+            wm.cur[a * 32 + lane] = addm(wm.cur[a * 32 + lane], wm.dx[a * 32 + lane], M.p);
+        __syncwarp();
+    }
+    if (__any_sync(kFull, inv0 && (uint32_t)lane < T.nprimes) && lane == 0)
+        atomicOr(A.status + T.walk, DR_STATUS_INV0 | DR_STATUS_FALLBACK);
+    else if (lane == 0 && T.chunk == 0)
+        atomicOr(A.status + T.walk, DR_STATUS_FALLBACK);
+    finish_tile<M_>(A, T, W, P, M.one, false, M, lane);
+}
+
+// ---- persistent kernel ----------------------------------------------------
+template <int CLS, int M_, int D>
+__global__ void __launch_bounds__(128) k_walk(const WalkArgs A) {
+    extern __shared__ uint32_t smem[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const WarpMem wm = warp_mem(A, smem, warp);
+    for (;;) {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(A.queue, 1u);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= A.n_tiles) break;
+        const DevTile T = A.tiles[t];
+        const DevWalk W = A.walks[T.walk];
+        const DevProgram G = A.progs[W.prog];
+        if (CLS == CLS_COMPANION) tile_companion<M_, D>(A, T, W, G, wm, lane);
+        else if (CLS == CLS_RATIONAL) tile_rational<M_, D>(A, T, W, G, wm, lane);
+        else if (CLS == CLS_DENSE) tile_dense<M_, D>(A, T, W, G, wm, lane);
+        else tile_interp<M_>(A, T, W, G, wm, lane);
+        __syncwarp();
+    }
+}
+
+}  // namespace dr

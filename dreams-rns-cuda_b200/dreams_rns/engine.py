@@ -1,0 +1,309 @@
+"""Batched walk execution on the B200 engine (host side of the C ABI).
+
+A :class:`WalkRequest` describes one walk; :func:`run_walks` runs a list of
+them in one engine call (host buffers in, host results out) and
+:class:`WalkBatch` keeps a prepared batch resident on the device so the same
+walks can be re-run with no host work (CUDA-graph replay).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from fractions import Fraction
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _native as N
+from .compiler import CmfProgram
+
+__all__ = ["WalkRequest", "pcf_request", "cmf_request", "run_walks", "WalkBatch", "program_blob"]
+
+
+def program_blob(program) -> bytes:
+    if isinstance(program, (bytes, bytearray)):
+        return bytes(program)
+    if isinstance(program, CmfProgram):
+        return program.serialize()
+    if hasattr(program, "serialize"):
+        return program.serialize()
+    raise TypeError("program must be a CmfProgram or its serialized bytes")
+
+
+def _directions(blob: bytes) -> List[int]:
+    m, dim, n_ops, n_consts = np.frombuffer(blob[:16], dtype="<u4")
+    off = 16 + 16 * int(n_ops) + 8 * int(n_consts)
+    return [int(v) for v in np.frombuffer(blob[off:off + 4 * int(dim)], dtype="<i4")]
+
+
+def _dims(blob: bytes) -> Tuple[int, int]:
+    m, dim = np.frombuffer(blob[:8], dtype="<u4")
+    return int(m), int(dim)
+
+
+def _rational(v) -> Tuple[int, int]:
+    """cmf_walk.py:332-345: int, Fraction or (num, den)."""
+    if isinstance(v, Fraction):
+        return v.numerator, v.denominator
+    if isinstance(v, (tuple, list)):
+        return int(v[0]), int(v[1])
+    return int(v), 1
+
+
+@dataclass
+class WalkRequest:
+    blob: bytes
+    K: int
+    depth: int
+    axis: List[Tuple[int, int, int, int]]   # per program axis: (sn, sd, tn, td)
+    a0: int = 0
+    pcf_init: bool = False
+    q_row: int = 1
+    checkpoint: int = 0
+    shadow: bool = True
+    tag: dict = field(default_factory=dict)
+
+
+def pcf_request(program, a0: int, depth: int, K: int = 32, shift_val: int = 1,
+                checkpoint: int = 0, shadow: bool = True) -> WalkRequest:
+    """PCF walk: P0 = [[1, a0], [0, 1]], LOAD_X = shift + step * direction
+    (reference runner.py:386-461)."""
+    blob = program_blob(program)
+    dirs = _directions(blob)
+    return WalkRequest(blob=blob, K=K, depth=depth, a0=int(a0), pcf_init=True, q_row=1,
+                       axis=[(int(shift_val), 1, d, 1) for d in dirs], checkpoint=checkpoint,
+                       shadow=shadow)
+
+
+def cmf_request(program, depth: int, K: int, shift_vals, trajectory_vals=None,
+                checkpoint: int = 0, shadow: bool = True) -> WalkRequest:
+    """CMF walk: P0 = I, rational per-axis shift/trajectory, q = P[m-1][m-1]
+    (reference cmf_walk.py:363-431)."""
+    blob = program_blob(program)
+    m, dim = _dims(blob)
+    sh = [_rational(v) for v in shift_vals]
+    if trajectory_vals is not None:
+        tr = [_rational(v) for v in trajectory_vals]
+    else:
+        tr = [(d, 1) for d in _directions(blob)]
+    if len(sh) < dim or len(tr) < dim:
+        raise IndexError("fewer shift/trajectory values than program axes")
+    return WalkRequest(blob=blob, K=K, depth=depth, pcf_init=False, q_row=m - 1,
+                       axis=[(sh[a][0], sh[a][1], tr[a][0], tr[a][1]) for a in range(dim)],
+                       checkpoint=checkpoint, shadow=shadow)
+
+
+class _Packed:
+    """Flat C-ABI arrays for a list of requests."""
+
+    def __init__(self, reqs: Sequence[WalkRequest]):
+        index: Dict[bytes, int] = {}
+        blobs: List[bytes] = []
+        for r in reqs:
+            if r.blob not in index:
+                index[r.blob] = len(blobs)
+                blobs.append(r.blob)
+        self.n_programs = len(blobs)
+        offs = np.zeros(len(blobs) + 1, dtype=np.uint64)
+        np.cumsum([len(b) for b in blobs], out=offs[1:])
+        self.offsets = offs
+        self.blobs = np.frombuffer(b"".join(blobs) or b"\0", dtype=np.uint8).copy()
+        n = len(reqs)
+        desc = np.zeros(n, dtype=N.WALK_DTYPE)
+        axis: List[int] = []
+        res = 0
+        self.res_off = np.zeros(n, dtype=np.int64)
+        self.cp_off = np.full(n, -1, dtype=np.int64)
+        for i, r in enumerate(reqs):
+            if r.K < 1 or r.K > N.DR_MAX_K:
+                raise ValueError(f"K must be in 1..{N.DR_MAX_K}")
+            if r.depth < 0:
+                r.depth = 0
+            d = desc[i]
+            d["program"] = index[r.blob]
+            d["K"] = r.K
+            d["depth"] = r.depth
+            d["checkpoint"] = r.checkpoint
+            if not -(1 << 63) <= r.a0 < (1 << 63):
+                raise OverflowError("a0 outside int64")
+            d["a0"] = r.a0
+            d["flags"] = (N.DR_WALK_INIT_PCF if r.pcf_init else 0) | (N.DR_WALK_SHADOW if r.shadow else 0)
+            d["q_row"] = r.q_row
+            d["axis_offset"] = len(axis)
+            for t in r.axis:
+                for v in t:
+                    if not -(1 << 63) <= v < (1 << 63):
+                        raise OverflowError("axis parameter outside int64")
+                axis.extend(int(v) for v in t)
+            d["res_offset"] = res
+            self.res_off[i] = res
+            res += r.K
+            if r.checkpoint:
+                d["cp_res_offset"] = res
+                self.cp_off[i] = res
+                res += r.K
+        self.desc = desc
+        self.axis = np.array(axis or [0], dtype=np.int64)
+        self.n_axis = len(axis)
+        self.n_res = max(res, 1)
+        self.n = n
+
+
+def _tune(chunk_steps=0, engine=N.DR_ENGINE_AUTO, warps_per_block=0):
+    t = N.Tune()
+    t.chunk_steps = chunk_steps
+    t.engine = engine
+    t.warps_per_block = warps_per_block
+    return t
+
+
+def _unpack(pk: _Packed, reqs, p, q, sh, st):
+    out = []
+    primes_cache: Dict[int, np.ndarray] = {}
+    for i, r in enumerate(reqs):
+        if r.K not in primes_cache:
+            primes_cache[r.K] = N.prime_table(r.K).astype(np.int64)
+        o = int(pk.res_off[i])
+        d = {"p_residues": p[o:o + r.K].astype(np.int64), "q_residues": q[o:o + r.K].astype(np.int64),
+             "p_float": float(sh[3 * i]), "q_float": float(sh[3 * i + 1]),
+             "log_scale": float(sh[3 * i + 2]), "primes": primes_cache[r.K],
+             "status": int(st[i])}
+        if r.checkpoint:
+            c = int(pk.cp_off[i])
+            j = 3 * (pk.n + i)
+            d["checkpoint"] = {"depth": r.checkpoint, "p_residues": p[c:c + r.K].astype(np.int64),
+                               "q_residues": q[c:c + r.K].astype(np.int64), "p_float": float(sh[j]),
+                               "q_float": float(sh[j + 1]), "log_scale": float(sh[j + 2])}
+        out.append(d)
+    return out
+
+
+def run_walks(reqs: Sequence[WalkRequest], chunk_steps: int = 0,
+              engine: int = N.DR_ENGINE_AUTO) -> List[dict]:
+    """Run every request in one engine call; one result dict per request."""
+    N.init()
+    reqs = list(reqs)
+    if not reqs:
+        return []
+    pk = _Packed(reqs)
+    p = np.zeros(pk.n_res, dtype=np.uint32)
+    q = np.zeros(pk.n_res, dtype=np.uint32)
+    sh = np.zeros(6 * pk.n, dtype=np.float64)
+    st = np.zeros(pk.n, dtype=np.uint32)
+    t = _tune(chunk_steps, engine)
+    N.check(N.lib().dr_walk_batch(N.ptr(pk.desc), pk.n, N.ptr(pk.blobs), N.ptr(pk.offsets),
+                                  pk.n_programs, N.ptr(pk.axis), pk.n_axis, ctypes.byref(t),
+                                  N.ptr(p), N.ptr(q), pk.n_res, N.ptr(sh), N.ptr(st)),
+            "dr_walk_batch")
+    return _unpack(pk, reqs, p, q, sh, st)
+
+
+class WalkBatch:
+    """A batch of walks prepared once and resident on the device."""
+
+    def __init__(self, reqs: Sequence[WalkRequest], chunk_steps: int = 0,
+                 engine: int = N.DR_ENGINE_AUTO, warps_per_block: int = 0):
+        N.init()
+        self.reqs = list(reqs)
+        self.pk = _Packed(self.reqs)
+        t = _tune(chunk_steps, engine, warps_per_block)
+        h = ctypes.c_int32(0)
+        N.check(N.lib().dr_batch_create(N.ptr(self.pk.desc), self.pk.n, N.ptr(self.pk.blobs),
+                                        N.ptr(self.pk.offsets), self.pk.n_programs,
+                                        N.ptr(self.pk.axis), self.pk.n_axis, ctypes.byref(t),
+                                        ctypes.byref(h)), "dr_batch_create")
+        self.handle = h.value
+
+    def run(self, stream: Optional[int] = None) -> None:
+        """Enqueue one run on ``stream`` (a cudaStream_t as int; None = the engine's
+        own stream).  Use a created stream: handle 0, the legacy default
+        stream, also selects the engine's stream."""
+        N.check(N.lib().dr_batch_run(self.handle, ctypes.c_void_p(stream) if stream else None),
+                "dr_batch_run")
+
+    def read(self) -> List[dict]:
+        pk = self.pk
+        p = np.zeros(pk.n_res, dtype=np.uint32)
+        q = np.zeros(pk.n_res, dtype=np.uint32)
+        sh = np.zeros(6 * pk.n, dtype=np.float64)
+        st = np.zeros(pk.n, dtype=np.uint32)
+        N.check(N.lib().dr_batch_read(self.handle, N.ptr(p), N.ptr(q), pk.n_res, N.ptr(sh), N.ptr(st)),
+                "dr_batch_read")
+        return _unpack(pk, self.reqs, p, q, sh, st)
+
+    def set_pipeline(self, delta: Optional[str] = None, target: Optional[Tuple[int, int]] = None,
+                     topk: int = 0, crt: bool = True) -> None:
+        """Run CRT (and optionally delta and top-k) on the device after every walk.
+
+        ``delta="fixed"`` scores each final convergent against ``target`` =
+        (Lnum, Lden); ``delta="self"`` scores each checkpoint convergent against
+        the walk's own final convergent (every walk needs a checkpoint).
+        """
+        pl = N.Pipeline()
+        pl.crt = 1 if crt else 0
+        pl.delta_mode = {None: N.DR_DELTA_NONE, "fixed": N.DR_DELTA_FIXED,
+                         "self": N.DR_DELTA_SELF}[delta]
+        pl.topk = int(topk)
+        self._tgt = None
+        if delta == "fixed":
+            from .runner import int_to_limbs
+            num, den = target
+            if den <= 0:
+                raise ValueError("target denominator must be positive")
+            width = max(abs(num).bit_length(), den.bit_length(), 1)
+            nl = (width + 31) // 32 + 1
+            sgn, ln = int_to_limbs(int(num), nl)
+            _, ld = int_to_limbs(int(den), nl)
+            self._tgt = (ln, ld)
+            pl.l_limbs = nl
+            pl.lnum = ln.ctypes.data
+            pl.lden = ld.ctypes.data
+            pl.lnum_sign = sgn
+        N.check(N.lib().dr_batch_set_pipeline(self.handle, ctypes.byref(pl)), "dr_batch_set_pipeline")
+        self.pipeline = {"delta": delta, "topk": int(topk), "crt": crt}
+
+    def read_pipeline(self, values: bool = False) -> dict:
+        """Deltas, top-k and (with ``values``) the centred p, q as Python ints."""
+        n = self.pk.n
+        k = min(self.pipeline["topk"], n)
+        delta = np.zeros(max(n, 1), dtype=np.float64)
+        ti = np.zeros(max(k, 1), dtype=np.int32)
+        tv = np.zeros(max(k, 1), dtype=np.float64)
+        Kmax = max(r.K for r in self.reqs)
+        stride = (31 * Kmax + 31) // 32 + 2
+        limbs = np.zeros((4 * n, stride), dtype=np.uint32) if values else None
+        signs = np.zeros(4 * n, dtype=np.int32) if values else None
+        N.check(N.lib().dr_batch_read_pipeline(
+            self.handle, N.ptr(delta) if self.pipeline["delta"] else None,
+            N.ptr(ti) if k else None, N.ptr(tv) if k else None,
+            N.ptr(limbs) if values else None, N.ptr(signs) if values else None, stride),
+            "dr_batch_read_pipeline")
+        out = {"delta": delta[:n] if self.pipeline["delta"] else None,
+               "topk_idx": ti[:k], "topk_val": tv[:k]}
+        if values:
+            from .runner import limbs_to_int
+            vals = [limbs_to_int(limbs[i], int(signs[i])) for i in range(4 * n)]
+            out["p"] = vals[0::4]
+            out["q"] = vals[1::4]
+            out["cp_p"] = vals[2::4]
+            out["cp_q"] = vals[3::4]
+        return out
+
+    def stats(self) -> dict:
+        ps, nt, nl, ms = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_float()
+        N.check(N.lib().dr_batch_stats(self.handle, ctypes.byref(ps), ctypes.byref(nt),
+                                       ctypes.byref(nl), ctypes.byref(ms)), "dr_batch_stats")
+        return {"prime_steps": ps.value, "tiles": nt.value, "launches": nl.value,
+                "last_ms": ms.value}
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().dr_batch_destroy(self.handle)
+            self.handle = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass

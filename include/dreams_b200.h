@@ -1,0 +1,220 @@
+/*
+ * dreams_b200.h -- C ABI of the B200 RNS walk engine (libdreams_b200.so).
+ *
+ * Plain C types only: pointers, sizes, status codes.  Every function returns
+ * an int status (DR_OK = 0, negative = error; see dr_strerror).  Functions
+ * named *_device take device pointers and a CUDA stream passed as void*;
+ * all others take host pointers and synchronise before returning.
+ *
+ * The reference has no native ABI for this path (its C++ declarations in
+ * include/dreams/walk_kernel.h:51-61 are never defined or exported, and its
+ * only working engine is Python: python/dreams_rns/runner.py).  Each entry
+ * point below names the reference function whose behaviour it provides.
+ */
+#ifndef DREAMS_B200_H
+#define DREAMS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define DR_OK                 0
+#define DR_ERR_CUDA          -1   /* CUDA runtime error (message: dr_last_error) */
+#define DR_ERR_ARG           -2   /* bad argument (null pointer, size)        */
+#define DR_ERR_BLOB          -3   /* malformed program blob (truncated)       */
+#define DR_ERR_OPCODE        -4   /* unknown opcode (reference: ValueError)   */
+#define DR_ERR_INDEX         -5   /* register/constant/axis/entry index out of
+                                     range (reference: IndexError)            */
+#define DR_ERR_UNSUPPORTED   -6   /* outside this engine's limits (m, K, dim)  */
+#define DR_ERR_NOMEM         -7   /* device memory exhausted / admission cap   */
+#define DR_ERR_NOT_INIT      -8   /* dr_init not called                        */
+#define DR_ERR_HANDLE        -9   /* unknown batch / server / request handle   */
+#define DR_ERR_TIMEOUT      -10   /* a bounded wait expired                    */
+#define DR_ERR_MODULUS      -11   /* CRT modulus outside odd [3, 2^31)         */
+#define DR_ERR_BUSY         -12   /* request not finished yet (poll again)     */
+
+/* ---- limits --------------------------------------------------------------- */
+#define DR_MAX_M        8        /* matrix size (reference config.h MAX_M)     */
+#define DR_MAX_AXES     8        /* axes per program (config.h MAX_AXES)       */
+#define DR_MAX_K        8192     /* primes per walk                            */
+#define DR_MAX_REGS     512      /* virtual registers (compiler.py MAX_REGS)   */
+
+/* ---- walk descriptor ------------------------------------------------------
+ * One walk: P = P0 * M(s0) * ... * M(depth-1), residues mod the first K primes
+ * of dr_prime_table.  The step matrix M(s) is the program's bytecode evaluated
+ * at 0-based step s, where LOAD_X of axis a yields
+ *     (sn_a*td_a + s*tn_a*sd_a) * inv(sd_a*td_a)  (mod p)
+ * with (sn, sd, tn, td) = axis_params[axis_offset + 4a .. +3]
+ * (reference cmf_walk.py:221-224; the PCF walk is sn = shift, tn = direction,
+ * sd = td = 1, runner.py:273-275).
+ * Outputs: p = P[0][m-1], q = P[q_row][m-1] (PCF: q_row = 1, runner.py:449-450;
+ * CMF: q_row = m-1, cmf_walk.py:419-420) written to
+ * p_res[res_offset + k], q_res[res_offset + k] for k < K.  With a non-zero
+ * checkpoint the same outputs after `checkpoint` steps go to
+ * cp_res_offset.  The FP64 shadow (p_float, q_float, log_scale) goes to
+ * shadow[3*w], and shadow[3*(n_walks + w)] for the checkpoint.            */
+#define DR_WALK_INIT_PCF   0x1u   /* P0 = [[1, a0], [0, 1]], else P0 = I     */
+#define DR_WALK_SHADOW     0x2u   /* compute the FP64 shadow                  */
+
+typedef struct dr_walk_desc {
+    uint32_t program;       /* index into the program blob list              */
+    uint32_t K;             /* number of primes, 1..DR_MAX_K                  */
+    uint64_t depth;         /* steps                                          */
+    uint64_t checkpoint;    /* 0 = none, else 0 < checkpoint < depth          */
+    int64_t  a0;            /* PCF initial value a(0)                         */
+    uint32_t flags;         /* DR_WALK_*                                      */
+    uint32_t q_row;         /* row of q in the last column                    */
+    uint64_t axis_offset;   /* index of this walk's first axis parameter     */
+    uint64_t res_offset;    /* residue output offset                         */
+    uint64_t cp_res_offset; /* checkpoint residue output offset              */
+} dr_walk_desc;
+
+/* walk status bits (status_out[w]) */
+#define DR_STATUS_INV0        0x1u  /* some INV met 0 (returned 0; reference
+                                       config.h:166-169 "dead lane")         */
+#define DR_STATUS_SHADOW_NAN  0x2u  /* shadow became non-finite               */
+#define DR_STATUS_FALLBACK    0x4u  /* walk ran on the per-step interpreter   */
+
+/* engine selection for dr_walk_batch */
+#define DR_ENGINE_AUTO    0   /* planned fast path (difference tables), else
+                                 the per-step interpreter                    */
+#define DR_ENGINE_INTERP  1   /* per-step bytecode interpreter, chunked      */
+#define DR_ENGINE_PLAIN   2   /* one walk per launch, per-step interpreter,
+                                 no depth chunks (the baseline path)         */
+
+typedef struct dr_tune {
+    uint32_t chunk_steps;     /* depth-chunk length; 0 = autotuned           */
+    uint32_t warps_per_block; /* 0 = default                                  */
+    uint32_t engine;          /* DR_ENGINE_*                                  */
+    uint32_t reserved;
+} dr_tune;
+
+/* ---- context ---------------------------------------------------------- */
+int dr_init(int device);
+const char *dr_strerror(int status);
+const char *dr_last_error(void);
+int dr_version(void);
+
+/* The first K primes below 2^31 in descending order (reference
+ * runner.py:81-100 generate_rns_primes). */
+int dr_prime_table(int K, uint32_t *out);
+
+/* Validate a program blob (reference compiler.py:64-89 layout) and report how
+ * the engine will run it: *cls_out = 1 companion polynomial, 2 companion
+ * rational, 3 dense polynomial, 4 per-step interpreter; *degree_out = degree
+ * of the step matrix in the step index (difference-table depth). */
+int dr_program_info(const uint8_t *blob, uint64_t size, int32_t *cls_out,
+                    int32_t *degree_out, int32_t *n_regs_out);
+
+/* ---- walks ------------------------------------------------------------
+ * Batch of walks, host buffers (reference runner.py:386-461 run_pcf_walk and
+ * cmf_walk.py:363-431 run_cmf_walk, one dict per walk).  blobs: all program
+ * blobs back to back, blob_offsets[n_programs + 1].  tune may be NULL.     */
+int dr_walk_batch(const dr_walk_desc *walks, int32_t n_walks,
+                  const uint8_t *blobs, const uint64_t *blob_offsets, int32_t n_programs,
+                  const int64_t *axis_params, uint64_t n_axis_params,
+                  const dr_tune *tune,
+                  uint32_t *p_res, uint32_t *q_res, uint64_t n_res,
+                  double *shadow, uint32_t *status);
+
+/* ---- prepared batches (inputs resident on the device) -------------------
+ * dr_batch_create uploads programs and descriptors once; dr_batch_run runs
+ * walk -> CRT -> delta -> top-k entirely on the device (captured in a CUDA
+ * graph after the first run); dr_batch_read copies results to the host.     */
+int dr_batch_create(const dr_walk_desc *walks, int32_t n_walks,
+                    const uint8_t *blobs, const uint64_t *blob_offsets, int32_t n_programs,
+                    const int64_t *axis_params, uint64_t n_axis_params,
+                    const dr_tune *tune, int32_t *batch_out);
+int dr_batch_run(int32_t batch, void *stream);
+int dr_batch_read(int32_t batch, uint32_t *p_res, uint32_t *q_res, uint64_t n_res,
+                  double *shadow, uint32_t *status);
+int dr_batch_stats(int32_t batch, uint64_t *prime_steps, uint32_t *n_tiles,
+                   uint32_t *n_launches, float *last_ms);
+
+/* Device pipeline after the walk, part of every dr_batch_run once set:
+ * CRT of p, q (and the checkpoint's p, q) to centred limbs, the Dreams delta
+ * (reference runner.py:151-173) and top-k by delta.  DR_DELTA_FIXED scores the
+ * final convergent against one target L = lnum_sign * lnum / lden; DR_DELTA_SELF
+ * scores the checkpoint convergent against the walk's own final convergent.   */
+#define DR_DELTA_NONE   0
+#define DR_DELTA_FIXED  1
+#define DR_DELTA_SELF   2
+
+typedef struct dr_pipeline {
+    int32_t crt;            /* 1: reconstruct on the device                  */
+    int32_t delta_mode;     /* DR_DELTA_* (needs crt)                        */
+    int32_t topk;           /* 0 = none, else 1..2048                        */
+    int32_t l_limbs;        /* limbs of lnum / lden (DR_DELTA_FIXED)         */
+    const uint32_t *lnum;   /* |Lnum| little-endian limbs (host pointer)     */
+    const uint32_t *lden;   /* Lden limbs, > 0 (host pointer)                */
+    int32_t lnum_sign;
+    int32_t reserved;
+} dr_pipeline;
+
+int dr_batch_set_pipeline(int32_t batch, const dr_pipeline *pl);
+/* delta[n_walks]; topk_idx/topk_val[k]; limbs[4*n_walks][limb_stride] with rows
+ * 4w+0 p, 4w+1 q, 4w+2 checkpoint p, 4w+3 checkpoint q and signs[4*n_walks].
+ * Any output may be NULL. */
+int dr_batch_read_pipeline(int32_t batch, double *delta, int32_t *topk_idx, double *topk_val,
+                           uint32_t *limbs, int32_t *signs, int32_t limb_stride);
+int dr_batch_destroy(int32_t batch);
+
+/* ---- CRT (reference runner.py:105-129 crt_reconstruct + centered) --------
+ * residues[i*K + k] mod moduli[k] for n values.  Outputs the centred value
+ * x - M if x > M/2 else x, where x in [0, M) is the reference's CRT result,
+ * as sign (+1, -1 or 0) and magnitude limbs (little-endian u32,
+ * limbs[i*limb_stride ..]), nlimbs_out[i] = significant limbs.  The reference
+ * result x itself is available as unsigned limbs (unsigned_limbs != NULL).
+ * moduli must be odd in [3, 2^31); NULL selects dr_prime_table(K).
+ * limb_stride >= ceil(31*K/32) + 1.                                          */
+int dr_crt_batch(const uint32_t *residues, int32_t K, int32_t n, const uint32_t *moduli,
+                 uint32_t *limbs, int32_t limb_stride, int32_t *sign_out,
+                 int32_t *nlimbs_out, uint32_t *unsigned_limbs);
+int dr_crt_batch_device(const uint32_t *residues_d, int32_t K, int32_t n,
+                        const uint32_t *moduli_d, uint32_t *limbs_d, int32_t limb_stride,
+                        int32_t *sign_d, int32_t *nlimbs_d, void *stream);
+
+/* ---- delta (reference runner.py:151-173 compute_dreams_delta_exact) -----
+ * delta = -(1 + ln|p/q - L| / ln|q|), q = 0 -> -inf, p/q == L -> +inf,
+ * |q| <= 1 -> -inf.  p, q: sign + magnitude limbs as produced by dr_crt_batch
+ * (stride limb_stride).  L = Lnum / Lden given as sign + limbs (stride
+ * l_stride); per_item_target != 0 means item i uses target i, else target 0.  */
+int dr_delta_batch(const uint32_t *p_limbs, const int32_t *p_sign, const uint32_t *q_limbs,
+                   const int32_t *q_sign, int32_t n, int32_t limb_stride,
+                   const uint32_t *lnum_limbs, const int32_t *lnum_sign,
+                   const uint32_t *lden_limbs, int32_t l_stride, int32_t per_item_target,
+                   double *delta_out);
+
+/* Top-k by delta, highest first, ties by lower index (the reference's
+ * threshold filter persistent_kernel.cu:796-841 kept no order). */
+int dr_topk(const double *delta, int32_t n, int32_t k, int32_t *idx_out, double *val_out);
+
+/* ---- serving: continuous batching of walk requests ---------------------- */
+typedef struct dr_serve_config {
+    uint64_t mem_cap_bytes;     /* admission cap on device state (0 = 50% free) */
+    uint32_t max_inflight;      /* waves in flight (streams), 0 = 2           */
+    uint32_t chunk_steps;       /* yield granularity of long walks, 0 = auto    */
+    uint32_t max_wave_tiles;    /* tiles per wave, 0 = auto                      */
+    uint32_t reserved[3];
+} dr_serve_config;
+
+int dr_serve_open(const dr_serve_config *cfg, int32_t *server_out);
+/* Submit one walk (walk->program indexes the single blob given here). */
+int dr_serve_submit(int32_t server, const dr_walk_desc *walk, const uint8_t *blob,
+                    uint64_t blob_size, const int64_t *axis_params, int64_t *request_out);
+/* Non-blocking: DR_OK with results when done, DR_ERR_BUSY otherwise.
+ * p_res/q_res hold K entries; shadow 3 doubles; latency in seconds. */
+int dr_serve_poll(int32_t server, int64_t request, uint32_t *p_res, uint32_t *q_res,
+                  double *shadow, uint32_t *status, double *latency_s);
+int dr_serve_cancel(int32_t server, int64_t request);
+int dr_serve_stats(int32_t server, uint64_t *completed, uint64_t *prime_steps,
+                   uint64_t *admitted_bytes, uint32_t *queue_depth);
+int dr_serve_close(int32_t server);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DREAMS_B200_H */

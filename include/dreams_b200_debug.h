@@ -1,0 +1,37 @@
+/*
+ * dreams_b200_debug.h -- test hooks of libdreams_b200.so (not a production API).
+ *
+ * No reference counterpart: these expose host-side re-statements of the
+ * device algorithms so the planner can be checked on machines without a GPU.
+ */
+#ifndef DREAMS_B200_DEBUG_H
+#define DREAMS_B200_DEBUG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Run the device walk schedule (depth chunks, difference tables, exceptional
+ * steps, ordered combine) on the CPU for the first K primes.  axis_params:
+ * 4 int64 per program axis.  chunk_steps = 0 means one chunk.  force_interp
+ * runs the per-step interpreter schedule instead of the planned class.      */
+int dr_debug_sim_walk(const uint8_t *blob, uint64_t size, int32_t K, uint64_t depth,
+                      uint64_t checkpoint, const int64_t *axis_params, int32_t pcf_init,
+                      int64_t a0, uint32_t q_row, uint64_t chunk_steps, int32_t force_interp,
+                      uint32_t *p_out, uint32_t *q_out, uint32_t *cp_p_out, uint32_t *cp_q_out);
+
+/* Difference-table depth of the compiled kernel the engine uses for a
+ * (class, m, degree) program, or -1 when it runs on the interpreter. */
+int dr_debug_template_degree(int32_t cls, int32_t m, int32_t degree);
+
+/* Integer-pipe issue peak on the current device, lane-instructions per
+ * second: kind 0 wide multiply-add, 1 add+min, 2 their 1:2 mix.  The
+ * denominator of the walk kernels' roofline. */
+int dr_bench_int_peak(int32_t kind, double *lane_ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DREAMS_B200_DEBUG_H */

@@ -1,0 +1,258 @@
+"""GPU parity: the CUDA engine against the reference fixtures and the C oracle.
+
+Residues, CRT values: bit-exact.  Float shadow: identical when the engine
+uses integer differences (all reference intermediates exact), otherwise
+within 1e-12 relative (the reference's own pow() is not correctly rounded,
+so only the shadow may differ, by ulps).  Delta: within 1e-9 of mpmath.
+"""
+
+import math
+import random
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+import dreams_rns as dr
+from dreams_rns import _native as N
+from dreams_rns.engine import WalkBatch, WalkRequest, cmf_request, pcf_request, run_walks
+from oracle import walk_c
+from progfuzz import random_axis, random_program
+
+pytestmark = pytest.mark.gpu
+
+SHADOW_RTOL = 1e-12
+
+
+def _close(a, b, rtol=SHADOW_RTOL):
+    if a == b:
+        return True
+    if math.isnan(a) and math.isnan(b):
+        return True
+    return abs(a - b) <= rtol * max(abs(a), abs(b), 1e-300)
+
+
+def _shadow_ok(r, w):
+    pf, qf, ls = (float.fromhex(w[k]) for k in ("p_float", "q_float", "log_scale"))
+    return _close(r["p_float"], pf) and _close(r["q_float"], qf) and _close(r["log_scale"], ls, 1e-13)
+
+
+@pytest.mark.parametrize("engine", [N.DR_ENGINE_AUTO, N.DR_ENGINE_INTERP])
+def test_pcf_fixtures(golden, engine):
+    reqs = [pcf_request(bytes.fromhex(w["blob"]), w["a0"], w["depth"], w["K"], w["shift"])
+            for w in golden["pcf_walks"]]
+    for chunk in (0, 97):
+        res = run_walks(reqs, chunk_steps=chunk, engine=engine)
+        for w, r in zip(golden["pcf_walks"], res):
+            assert list(r["p_residues"]) == w["p_residues"], (w["name"], engine, chunk)
+            assert list(r["q_residues"]) == w["q_residues"], (w["name"], engine, chunk)
+            assert _shadow_ok(r, w), (w["name"], r["p_float"], w["p_float"])
+
+
+def test_inv0_status(golden):
+    by = {w["name"]: w for w in golden["pcf_walks"]}
+    reqs = [pcf_request(bytes.fromhex(by[n]["blob"]), by[n]["a0"], by[n]["depth"], by[n]["K"])
+            for n in ("inv0_one_prime", "int_root_inv0", "config1")]
+    res = run_walks(reqs)
+    assert res[0]["status"] & N.DR_STATUS_INV0
+    assert res[1]["status"] & N.DR_STATUS_INV0
+    assert not res[2]["status"] & N.DR_STATUS_INV0
+
+
+def test_cmf_fixtures(golden):
+    reqs = []
+    for w in golden["cmf_walks"]:
+        tr = w["trajectory"]
+        reqs.append(cmf_request(bytes.fromhex(w["blob"]), w["depth"], w["K"],
+                                [tuple(x) for x in w["shifts"]],
+                                None if tr is None else [tuple(x) for x in tr]))
+    for engine in (N.DR_ENGINE_AUTO, N.DR_ENGINE_INTERP):
+        res = run_walks(reqs, engine=engine)
+        for w, r in zip(golden["cmf_walks"], res):
+            assert list(r["p_residues"]) == w["p_residues"], w["name"]
+            assert list(r["q_residues"]) == w["q_residues"], w["name"]
+            assert _shadow_ok(r, w), w["name"]
+
+
+def test_dropin_run_pcf_walk_config1(golden):
+    w = golden["pcf_walks"][0]
+    prog = dr.compile_pcf("2", "n**2")
+    r = dr.run_pcf_walk(prog, dr.pcf_initial_values("2"), 2000, 32)
+    assert r["p_residues"].dtype == np.int64 and r["p_residues"].shape == (32,)
+    assert list(r["p_residues"]) == w["p_residues"]
+    assert list(r["q_residues"]) == w["q_residues"]
+    assert list(r["primes"]) == golden["primes_512"][:32]
+    assert r["p_float"] == float.fromhex(w["p_float"])
+    assert r["q_float"] == float.fromhex(w["q_float"])
+    with pytest.raises(AssertionError):
+        dr.run_pcf_walk(dr.compile_cmf_from_dict({(0, 0): "x0"}, 1, 1), 0, 10, 8)
+
+
+def test_crt_fixtures(golden):
+    for c in golden["crt"]:
+        x, M = dr.crt_reconstruct(c["residues"], c["primes"])
+        assert hex(x) == c["x"] and hex(M) == c["M"]
+        assert hex(dr.centered(x, M)) == c["centered"]
+
+
+def test_crt_batch_matches_oracle():
+    from oracle.walk_np import centered, crt
+    rng = np.random.default_rng(5)
+    for K in (1, 2, 16, 31, 32, 33, 64, 100, 512):
+        pr = [int(p) for p in dr.generate_rns_primes(K)]
+        res = np.stack([rng.integers(0, p, size=40) for p in pr], axis=1).astype(np.uint32)
+        res[0, :] = 0
+        res[1, :] = 1
+        res[2, :] = [p - 1 for p in pr]
+        got = dr.crt_batch(res, K)
+        for i in range(res.shape[0]):
+            x, M = crt([int(v) for v in res[i]], pr)
+            assert got[i] == centered(x, M), (K, i)
+
+
+def test_delta_fixtures(golden):
+    for d in golden["delta_exact"]:
+        got = dr.compute_dreams_delta_exact(int(d["p"], 16), int(d["q"], 16), d["target"], d["dps"])
+        want = float(d["delta"])
+        if math.isinf(want) or math.isinf(got):
+            assert got == want, d["name"]
+        else:
+            assert abs(got - want) < 1e-9, (d["name"], got, want)
+
+
+def test_verify_pcf(golden):
+    for v in golden["verify_pcf"]:
+        r = dr.verify_pcf(v["a"], v["b"], v["limit"], v["depth"], v["K"])
+        want = v["result"]
+        assert r["p_bits"] == want["p_bits"]
+        assert abs(r["delta_exact"] - float(want["delta_exact"])) < 1e-9
+        assert abs(r["delta_float"] - float(want["delta_float"])) < 1e-9
+        assert r["target"] == float(want["target"])
+
+
+def test_random_programs_vs_oracle():
+    rng = random.Random(11)
+    reqs, refs = [], []
+    for trial in range(300):
+        blob, m, dim = random_program(rng)
+        try:
+            N.program_info(blob)
+        except Exception:
+            continue
+        K = rng.choice([1, 5, 32, 40, 64])
+        depth = rng.randrange(0, 300)
+        axis = random_axis(rng, dim, rng.random() < 0.4)
+        pcf = m == 2 and rng.random() < 0.5
+        a0 = rng.randrange(-9, 10)
+        cp = rng.randrange(1, depth) if depth > 2 and rng.random() < 0.4 else 0
+        req = WalkRequest(blob=blob, K=K, depth=depth, a0=a0, pcf_init=pcf, q_row=1 if pcf else m - 1,
+                          axis=[tuple(axis[4 * a:4 * a + 4]) for a in range(dim)], checkpoint=cp,
+                          shadow=False)
+        init = np.eye(m, dtype=np.int64)
+        if pcf:
+            init[0, 1] = a0
+        refs.append((blob, K, depth, np.array(axis, np.int64), init, req.q_row, cp))
+        reqs.append(req)
+    for chunk in (0, 16):
+        res = run_walks(reqs, chunk_steps=chunk)
+        for (blob, K, depth, axis, init, qrow, cp), r in zip(refs, res):
+            o = walk_c.walk(blob, depth, K, axis, init, 0, qrow, shadow=False)
+            assert list(r["p_residues"]) == list(o["p_residues"])
+            assert list(r["q_residues"]) == list(o["q_residues"])
+            if cp:
+                o2 = walk_c.walk(blob, cp, K, axis, init, 0, qrow, shadow=False)
+                assert list(r["checkpoint"]["p_residues"]) == list(o2["p_residues"])
+
+
+def test_shadow_vs_oracle():
+    rng = random.Random(3)
+    reqs = []
+    for trial in range(60):
+        a = dr.synth.poly_str([rng.randrange(-9, 10) for _ in range(rng.randrange(1, 4))])
+        b = dr.synth.poly_str([rng.randrange(-9, 10) for _ in range(rng.randrange(1, 6))])
+        if rng.random() < 0.3:
+            b = f"({b})/({dr.synth.poly_str([rng.randrange(1, 9), rng.randrange(-3, 4)])})"
+        prog = dr.compile_pcf(a, b)
+        reqs.append((prog, pcf_request(prog, dr.pcf_initial_values(a), rng.randrange(1, 3000), 32,
+                                       rng.randrange(-3, 4))))
+    res = run_walks([r for _, r in reqs])
+    for (prog, req), r in zip(reqs, res):
+        o = walk_c.pcf_walk(req.blob, req.a0, req.depth, 32, req.axis[0][0])
+        assert list(r["p_residues"]) == list(o["p_residues"])
+        assert _close(r["p_float"], o["p_float"]) and _close(r["q_float"], o["q_float"])
+        assert _close(r["log_scale"], o["log_scale"], 1e-13)
+
+
+def test_prepared_batch_replay():
+    ws = dr.synth.uniform_pcfs(64, seed=9, depth=500, limit_depth=1200)
+    reqs = [pcf_request(dr.compile_pcf(w.a, w.b), w.a0, w.depth, 32, checkpoint=w.checkpoint)
+            for w in ws]
+    b = WalkBatch(reqs)
+    b.run()
+    r1 = b.read()
+    b.run()
+    b.run()
+    r2 = b.read()
+    for x, y, req in zip(r1, r2, reqs):
+        assert list(x["p_residues"]) == list(y["p_residues"])
+        assert list(x["checkpoint"]["q_residues"]) == list(y["checkpoint"]["q_residues"])
+        o = walk_c.pcf_walk(req.blob, req.a0, req.checkpoint, 32)
+        assert list(x["checkpoint"]["p_residues"]) == list(o["p_residues"])
+    assert b.stats()["prime_steps"] == 64 * 1200 * 32
+    b.close()
+
+
+def test_topk():
+    rng = np.random.default_rng(1)
+    for n, k in ((10, 3), (5000, 100), (20000, 256), (3, 10)):
+        v = rng.standard_normal(n)
+        v[rng.integers(0, n, size=min(n, 5))] = np.inf
+        v[: min(n, 2)] = v[-1]  # ties
+        idx = np.zeros(min(n, k), dtype=np.int32)
+        val = np.zeros(min(n, k))
+        N.init()
+        N.check(N.lib().dr_topk(N.ptr(v), n, k, N.ptr(idx), N.ptr(val)))
+        order = sorted(range(n), key=lambda i: (-v[i], i))[:k]
+        assert list(idx) == order
+
+
+def test_pipeline_self_and_fixed():
+    import mpmath as mp
+    from oracle import walk_np
+    ws = dr.synth.uniform_pcfs(48, seed=17, depth=300, limit_depth=900)
+    reqs = [pcf_request(dr.compile_pcf(w.a, w.b), w.a0, w.depth, 32, checkpoint=w.checkpoint)
+            for w in ws]
+    b = WalkBatch(reqs)
+    b.set_pipeline(delta="self", topk=10)
+    b.run()
+    res = b.read()
+    pl = b.read_pipeline(values=True)
+    pr = [int(p) for p in dr.generate_rns_primes(32)]
+    want = []
+    for i, r in enumerate(res):
+        vals = []
+        for arr in (r["p_residues"], r["q_residues"], r["checkpoint"]["p_residues"],
+                    r["checkpoint"]["q_residues"]):
+            x, M = walk_np.crt([int(v) for v in arr], pr)
+            vals.append(walk_np.centered(x, M))
+        assert [pl["p"][i], pl["q"][i], pl["cp_p"][i], pl["cp_q"][i]] == vals
+        mp.mp.dps = 200
+        L = mp.mpf(vals[0]) / mp.mpf(vals[1])
+        d = walk_np.delta_exact(vals[2], vals[3], L, 200)
+        want.append(d)
+        if math.isinf(d):
+            assert pl["delta"][i] == d
+        else:
+            assert abs(pl["delta"][i] - d) < 1e-9, (i, pl["delta"][i], d)
+    order = sorted(range(len(want)), key=lambda i: (-pl["delta"][i], i))[:10]
+    assert list(pl["topk_idx"]) == order
+    # fixed target: pi as an exact binary ratio at dps 200
+    mp.mp.dps = 200
+    num, den = dr.runner.target_ratio(mp.pi)
+    b.set_pipeline(delta="fixed", target=(num, den), topk=5)
+    b.run()
+    pl2 = b.read_pipeline(values=True)
+    for i in range(len(res)):
+        d = walk_np.delta_exact(pl2["p"][i], pl2["q"][i], mp.pi, 200)
+        assert (pl2["delta"][i] == d) if math.isinf(d) else abs(pl2["delta"][i] - d) < 1e-9
+    b.close()

@@ -1,0 +1,157 @@
+"""Native library checks that need no GPU: exports, prime table, planner,
+and the host re-statement of the device schedule against the C oracle."""
+
+import ctypes
+import os
+import random
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, native_lib_path
+from oracle import walk_c
+from progfuzz import random_axis, random_program
+
+
+@pytest.fixture(scope="module")
+def L():
+    path = native_lib_path()
+    if not os.path.exists(path):
+        pytest.skip("libdreams_b200.so not built")
+    lib = ctypes.CDLL(path)
+    lib.dr_debug_sim_walk.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint64,
+                                      ctypes.c_uint64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64,
+                                      ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    lib.dr_program_info.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p]
+    lib.dr_last_error.restype = ctypes.c_char_p
+    return lib
+
+
+def _declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*|int32_t)\s*(dr_\w+)\s*\(", text, re.M)))
+
+
+def test_exports_every_declared_symbol(L):
+    names = _declared("dreams_b200.h") + _declared("dreams_b200_debug.h")
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_prime_table(L, golden):
+    out = np.zeros(512, dtype=np.uint32)
+    assert L.dr_prime_table(512, out.ctypes.data_as(ctypes.c_void_p)) == 0
+    assert list(out) == golden["primes_512"]
+
+
+def _info(L, blob):
+    c, d, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    rc = L.dr_program_info(blob, len(blob), ctypes.byref(c), ctypes.byref(d), ctypes.byref(r))
+    return rc, c.value, d.value
+
+
+def test_program_errors(L, golden):
+    blob = bytes.fromhex(golden["pcf_walks"][0]["blob"])
+    assert _info(L, blob)[0] == 0
+    assert _info(L, blob[:20])[0] == -3                     # truncated
+    bad = bytearray(blob)
+    bad[16] = 77                                             # opcode 77
+    assert _info(L, bytes(bad))[0] == -4
+    bad = bytearray(blob)
+    bad[16 + 4:16 + 8] = (5).to_bytes(4, "little")           # LOAD_X axis 5 of 1
+    assert _info(L, bytes(bad))[0] == -5
+
+
+def test_classes_of_reference_programs(L, golden):
+    seen = {}
+    for w in golden["pcf_walks"] + golden["cmf_walks"]:
+        rc, cls, deg = _info(L, bytes.fromhex(w["blob"]))
+        assert rc == 0
+        seen.setdefault(cls, []).append(w["name"])
+    assert "config1" in seen[1]                              # b = n^2: companion polynomial
+    assert "rational" in seen[2] and "inv0_one_prime" in seen[2]
+    assert "config4_full" in seen[1]
+
+
+def test_instances_cover_planner(L):
+    L.dr_debug_template_degree.argtypes = [ctypes.c_int32] * 3
+    text = open(os.path.join(ROOT, "dreams-rns-cuda_b200", "csrc", "instances.h")).read()
+    lists = {}
+    for name, cls in (("COMPANION", 1), ("RATIONAL", 2), ("DENSE", 3)):
+        body = text.split(f"DR_{name}_INSTANCES(X)")[1].split("\n\n")[0]
+        lists[cls] = set((int(a), int(b)) for a, b in re.findall(r"X\((\d+), (\d+)\)", body))
+    for cls in (1, 2, 3):
+        for m in range(1, 9):
+            for deg in range(0, 18):
+                D = L.dr_debug_template_degree(cls, m, deg)
+                if D >= 0:
+                    assert (m, D) in lists[cls], (cls, m, deg, D)
+
+
+def _sim(L, blob, K, depth, axis, pcf, a0, qrow, chunk, cp=0, force=0):
+    p = np.zeros(K, np.uint32)
+    q = np.zeros(K, np.uint32)
+    cpp = np.zeros(K, np.uint32)
+    cpq = np.zeros(K, np.uint32)
+    axis = np.ascontiguousarray(axis, np.int64)
+    rc = L.dr_debug_sim_walk(blob, len(blob), K, depth, cp, axis.ctypes.data, pcf, a0, qrow,
+                             chunk, force, p.ctypes.data, q.ctypes.data, cpp.ctypes.data,
+                             cpq.ctypes.data)
+    assert rc == 0, L.dr_last_error()
+    return p, q, cpp, cpq
+
+
+def test_schedule_matches_reference_fixtures(L, golden):
+    from oracle.walk_np import parse_blob
+    for w in golden["pcf_walks"]:
+        blob = bytes.fromhex(w["blob"])
+        dirs = parse_blob(blob)[4]
+        axis = np.array([[w["shift"], 1, d, 1] for d in dirs]).reshape(-1)
+        for chunk in (0, 7):
+            p, q, _, _ = _sim(L, blob, w["K"], w["depth"], axis, 1, w["a0"], 1, chunk)
+            assert list(p) == w["p_residues"] and list(q) == w["q_residues"], w["name"]
+    for w in golden["cmf_walks"]:
+        blob = bytes.fromhex(w["blob"])
+        m, dim, _, _, dirs = parse_blob(blob)
+        sh = w["shifts"]
+        tr = w["trajectory"] or [[d, 1] for d in dirs]
+        axis = np.array([[sh[a][0], sh[a][1], tr[a][0], tr[a][1]] for a in range(dim)]).reshape(-1)
+        p, q, _, _ = _sim(L, blob, w["K"], w["depth"], axis, 0, 0, m - 1, 13)
+        assert list(p) == w["p_residues"] and list(q) == w["q_residues"], w["name"]
+
+
+def test_schedule_random_programs(L):
+    rng = random.Random(7)
+    for trial in range(250):
+        blob, m, dim = random_program(rng)
+        if _info(L, blob)[0] != 0:
+            continue
+        K = rng.choice([1, 3, 8])
+        depth = rng.randrange(0, 50)
+        axis = np.array(random_axis(rng, dim, rng.random() < 0.4), np.int64)
+        pcf = int(m == 2 and rng.random() < 0.5)
+        a0 = rng.randrange(-9, 10)
+        init = np.eye(m, dtype=np.int64)
+        if pcf:
+            init[0, 1] = a0
+        qrow = 1 if pcf else m - 1
+        ref = walk_c.walk(blob, depth, K, axis, init, 0, qrow, shadow=False)
+        cp = rng.randrange(1, depth) if depth > 2 and rng.random() < 0.5 else 0
+        p, q, cpp, cpq = _sim(L, blob, K, depth, axis, pcf, a0, qrow, rng.choice([0, 1, 5, 17]), cp)
+        assert list(p) == list(ref["p_residues"]) and list(q) == list(ref["q_residues"]), trial
+        if cp:
+            r2 = walk_c.walk(blob, cp, K, axis, init, 0, qrow, shadow=False)
+            assert list(cpp) == list(r2["p_residues"]) and list(cpq) == list(r2["q_residues"])
+
+
+def test_walk_without_init_is_an_error():
+    import subprocess, sys
+    code = ("import sys; sys.path.insert(0, %r); import ctypes; from dreams_rns import _native as N; "
+            "L = N.lib(); rc = L.dr_walk_batch(None, 0, None, None, 0, None, 0, None, None, None, 0, None, None); "
+            "print(rc)") % os.path.join(ROOT, "dreams-rns-cuda_b200")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
+    assert out.stdout.strip() == "-8", out.stderr
