@@ -13,6 +13,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dreams_b200.h"
+#include "host_common.h"
 #include "launch.h"
 #include "modarith.cuh"
 
@@ -248,3 +254,93 @@ cudaError_t launch_crt(const uint32_t* res, int n, const CrtTables& T, uint32_t*
 }
 
 }  // namespace dr
+
+// ---- allocation-free CRT ----------------------------------------------------
+// For callers that may not allocate device memory themselves, for instance code
+// that runs under a framework which owns every byte of device memory through
+// its own pool, or that must not trigger the device-wide synchronisation a
+// cudaFree implies.  The per-moduli tables that dr_crt_batch_device keeps in
+// cudaMalloc'd buffers live here in one file-scope device array instead:
+// every GPU that loads the library holds it (about 66 KB) until the process
+// exits, and every call rebuilds the tables in it, so calls that overlap on
+// the GPU race on its contents.
+namespace dr {
+
+constexpr int kStaticCrtMaxK = 128;
+constexpr int kStaticCrtL = (31 * kStaticCrtMaxK + 31) / 32 + 2;
+constexpr int kStaticCrtWords = 4 * kStaticCrtMaxK + kStaticCrtMaxK * kStaticCrtL + kStaticCrtL;
+
+static __device__ __align__(256) uint32_t g_crt_static[kStaticCrtWords];
+
+namespace {
+std::mutex g_static_mu;
+void* g_static_addr[64] = {nullptr};   // host view of g_crt_static's device address, per device
+}  // namespace
+
+}  // namespace dr
+
+extern "C" int dr_crt_batch_device_noalloc(const uint32_t* residues_d, int32_t K, int32_t n,
+                                           uint32_t* limbs_d, int32_t limb_stride, int32_t* sign_d,
+                                           void* stream) {
+    using namespace dr;
+    if (K < 1 || K > kStaticCrtMaxK) {
+        set_error("dr_crt_batch_device_noalloc: K must be in 1..128 (size of its static tables)");
+        return K < 1 ? DR_ERR_ARG : DR_ERR_UNSUPPORTED;
+    }
+    if (n < 0 || (n > 0 && (!residues_d || !limbs_d || !sign_d))) {
+        set_error("dr_crt_batch_device_noalloc: null buffer");
+        return DR_ERR_ARG;
+    }
+    const int L = (31 * K + 31) / 32 + 2;
+    if (limb_stride < L) {
+        set_error("dr_crt_batch_device_noalloc: limb_stride below ceil(31K/32)+2");
+        return DR_ERR_ARG;
+    }
+    if (n == 0) return DR_OK;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 64) {
+        set_error("dr_crt_batch_device_noalloc: no current device");
+        return DR_ERR_CUDA;
+    }
+    uint32_t* base = nullptr;
+    {
+        // first call on each device: the array's device address, with that device current
+        std::lock_guard<std::mutex> lk(g_static_mu);
+        if (!g_static_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_crt_static);
+            if (e != cudaSuccess || !p) {
+                set_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+                return DR_ERR_CUDA;
+            }
+            g_static_addr[dev] = p;
+        }
+        base = static_cast<uint32_t*>(g_static_addr[dev]);
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // layout: moduli[K] pinv[K] r2[K] ginv[K] Mlimbs[K*L] Mtotal[L]
+    uint32_t* moduli = base;
+    uint32_t* pinv = base + K;
+    uint32_t* r2 = base + 2 * K;
+    uint32_t* ginv = base + 3 * K;
+    uint32_t* Ml = base + 4 * K;
+    uint32_t* Mt = Ml + (size_t)K * L;
+    // own copy: another thread may grow (and move) the shared table meanwhile
+    const std::vector<uint32_t> tab(prime_table(K).begin(), prime_table(K).begin() + K);
+    e = cudaMemcpyToSymbolAsync(g_crt_static, tab.data(), 4ull * K, 0, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_crt_setup(moduli, K, L, pinv, r2, ginv, Ml, Mt, st);
+    if (e != cudaSuccess) {
+        set_error(std::string("dr_crt_batch_device_noalloc setup: ") + cudaGetErrorString(e));
+        return DR_ERR_CUDA;
+    }
+    CrtTables T{moduli, pinv, r2, ginv, Ml, Mt, K, L};
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = launch_crt(residues_d, n, T, limbs_d, limb_stride, sign_d, nullptr, nullptr, sms, st);
+    if (e != cudaSuccess) {
+        set_error(std::string("dr_crt_batch_device_noalloc: ") + cudaGetErrorString(e));
+        return DR_ERR_CUDA;
+    }
+    return DR_OK;
+}

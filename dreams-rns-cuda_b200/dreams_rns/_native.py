@@ -121,6 +121,7 @@ _SIGNATURES = {
     "dr_batch_read_pipeline": (ctypes.c_int, [_I32, _P, _P, _P, _P, _P, _I32]),
     "dr_crt_batch": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P]),
     "dr_crt_batch_device": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P]),
+    "dr_crt_batch_device_noalloc": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _P, _P]),
     "dr_delta_batch": (ctypes.c_int, [_P, _P, _P, _P, _I32, _I32, _P, _P, _P, _I32, _I32, _P]),
     "dr_topk": (ctypes.c_int, [_P, _I32, _I32, _P, _P]),
     "dr_serve_open": (ctypes.c_int, [_P, _P]),

@@ -177,6 +177,22 @@ int dr_crt_batch_device(const uint32_t *residues_d, int32_t K, int32_t n,
                         const uint32_t *moduli_d, uint32_t *limbs_d, int32_t limb_stride,
                         int32_t *sign_d, int32_t *nlimbs_d, void *stream);
 
+/* Allocation-free variant of dr_crt_batch_device for callers that cannot call
+ * cudaMalloc (code running under an allocator that owns all device memory, or
+ * that must avoid the device-wide synchronisation cudaFree implies).  It has
+ * no counterpart in the reference.  Moduli are the first K primes of
+ * dr_prime_table; outputs are the centred limbs and signs of dr_crt_batch.
+ * It allocates nothing: its tables live in a static device array sized for
+ * K <= 128 (larger K returns DR_ERR_UNSUPPORTED), which every GPU that loads
+ * the library holds until exit.  Every call rebuilds the tables there, so
+ * calls that overlap on the GPU race; order them on one stream.  The first
+ * call on each device looks up the array's device address (cudaGetSymbolAddress
+ * with that device current), so make that first call before any stream
+ * capture.  Needs no dr_init.                                                */
+int dr_crt_batch_device_noalloc(const uint32_t *residues_d, int32_t K, int32_t n,
+                                uint32_t *limbs_d, int32_t limb_stride, int32_t *sign_d,
+                                void *stream);
+
 /* ---- delta (reference runner.py:151-173 compute_dreams_delta_exact) -----
  * delta = -(1 + ln|p/q - L| / ln|q|), q = 0 -> -inf, p/q == L -> +inf,
  * |q| <= 1 -> -inf.  p, q: sign + magnitude limbs as produced by dr_crt_batch
