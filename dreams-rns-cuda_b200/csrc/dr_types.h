@@ -58,17 +58,26 @@ struct DevTile {
     uint64_t s0, s1;       // step range [s0, s1)
 };
 
-// Combine group: the chunks of one (walk, prime block).
+// Combine group: the chunks of one (walk, prime block) in one launch.  With a
+// resident state slot (serving) the chunks are one segment of a longer walk:
+// the running product and denominator are read from the slot (unless this is
+// the first segment), multiplied by the chunk products, and written back (or
+// emitted on the final segment).
+constexpr uint32_t kNoState = 0xffffffffu;
+constexpr uint32_t GROUP_FIRST = 1u, GROUP_FINAL = 2u;
 struct DevGroup {
     uint32_t walk, prime0, nprimes, n_chunks;
     uint32_t slot0;        // first chunk-product slot
     uint32_t cp_chunks;    // chunks covering [0, checkpoint) (0 = no checkpoint)
+    uint32_t state;        // resident state slot or kNoState
+    uint32_t flags;        // GROUP_FIRST | GROUP_FINAL
 };
 
-// Shadow work item: a warp-group of up to 32 walks (integer differences) or
-// one walk (interpreted).
-struct DevShadowItem {
-    uint32_t walk0, n_walks;           // walks are listed in shadow_walks[walk0..]
+// Shadow work item: steps [s0, s1) of one walk; state is a resident slot
+// (serving segments) or kNoState (the walk runs from step 0 to its depth).
+struct DevShadowSeg {
+    uint32_t walk, state;
+    uint64_t s0, s1;
 };
 
 enum ShadowMode : uint32_t { SHADOW_NONE = 0, SHADOW_INTERP = 1, SHADOW_INTFD = 2 };

@@ -299,6 +299,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             g.n_chunks = (uint32_t)ranges.size();
             g.cp_chunks = cp_chunks;
             g.slot0 = g.n_chunks > 1 ? slots : 0;
+            g.state = kNoState;
+            g.flags = 0;
             if (g.n_chunks > 1) slots += g.n_chunks;
             const uint32_t gi = (uint32_t)groups.size();
             groups.push_back(g);
@@ -360,7 +362,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         else
             shadow_sets[LaunchKey{1, 0, G.m, 0}].push_back(w);
     }
-    std::vector<uint32_t> shadow_list;
+    std::vector<DevShadowSeg> shadow_list;
     for (auto& kv : shadow_sets) {
         auto& v = kv.second;
         std::stable_sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) {
@@ -383,7 +385,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         const uint32_t ns = L.kind == 2 ? (uint32_t)streams_for(L.cls, L.m) : 0;
         L.rows_per_warp = L.kind == 1 ? rr + kMaxAxes + L.m * L.m
                                       : rr + kMaxAxes + (L.D + 1) * ns + ns;
-        shadow_list.insert(shadow_list.end(), v.begin(), v.end());
+        for (uint32_t w : v) shadow_list.push_back(DevShadowSeg{w, kNoState, 0, dwalks[w].depth});
         B->launches.push_back(L);
     }
 
@@ -559,6 +561,9 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
     sa.shadow = B.shadow.as<double>();
     sa.n_walks = B.n_walks;
     sa.status = wa.status;
+    sa.state = nullptr;
+    wa.state_P = nullptr;
+    wa.state_sig = nullptr;
     DR_CUDA(cudaEventRecord(B.fork, st));
     const size_t np = C.pool.size();
     size_t used = 0;
@@ -579,7 +584,7 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
                 wa.rows_per_warp = L.rows_per_warp;
                 e = walk_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, wa, nullptr);
             } else {
-                sa.list = B.shadow_list.as<uint32_t>() + L.off;
+                sa.segs = B.shadow_list.as<DevShadowSeg>() + L.off;
                 sa.n_items = L.items;
                 sa.n_list = L.count;
                 sa.queue = B.queues.as<uint32_t>() + L.queue;

@@ -1,0 +1,647 @@
+// Serving: continuous batching of walk requests (dr_serve_*).
+//
+// A scheduler thread owns the device side.  Submitted requests wait in a FIFO
+// until their device state fits under the memory cap (running product and
+// denominator per 32-prime block, FP64 shadow state, outputs); admitted
+// requests are cut into segments.  Every wave takes the next walk segment and
+// the next shadow segment of each admitted request that is not already in
+// flight, builds the tiles (depth chunks x prime blocks), and launches the
+// same persistent kernels as batches do, with combine groups that resume from
+// and write back to resident state slots.  Up to max_inflight waves run at
+// once on separate streams, so requests that arrive while others are on the
+// GPU join the next wave and their work overlaps with what is running.
+// Completion is observed with cudaEventQuery from the host thread; the
+// device never waits on anything.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "../../include/dreams_b200.h"
+#include "engine.h"
+#include "host_common.h"
+#include "launch.h"
+#include "shadow_impl.cuh"
+#include "walk_impl.cuh"
+
+namespace dr {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+constexpr int kServeMaxM = 4;
+constexpr uint32_t kServeStride = kServeMaxM * kServeMaxM * 32;   // words per state slot
+
+struct Req {
+    int64_t id = 0;
+    std::shared_ptr<Plan> plan;
+    std::string blob;
+    dr_walk_desc d{};
+    std::vector<int64_t> axis;
+    uint32_t shadow_mode = SHADOW_NONE;
+    int tdeg = 0;                 // kernel difference depth
+    uint64_t walk_next = 0, shadow_next = 0;
+    bool walk_done = false, shadow_done = false;
+    bool inflight = false, admitted = false, done = false, cancelled = false;
+    std::vector<uint32_t> slots;  // resident product slots, one per prime block
+    int shadow_slot = -1;
+    uint64_t need = 0;
+    Clock::time_point t_submit, t_done;
+    std::vector<uint32_t> p, q;
+    double sh[3] = {0, 0, 0};
+    uint32_t status = 0;
+};
+
+struct Wave {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool busy = false;
+    std::vector<int64_t> reqs;            // requests with a segment in this wave
+    std::vector<uint8_t> walk_final;      // per request: walk part finishes here
+    std::vector<uint8_t> shadow_final;    // per request: shadow finishes here
+    std::vector<uint64_t> walk_end, shadow_end;
+    std::vector<uint64_t> res_off;        // output offsets of finishing walks
+    std::vector<uint32_t> widx;           // walk-table index per request
+    DevBuf progs, code, consts, walks, axis, tiles, groups, done_ctr, chunkP, chunkSig, segs,
+        queues, res, shadow, status;
+    uint32_t* h_res = nullptr;            // pinned outputs
+    double* h_sh = nullptr;
+    uint32_t* h_st = nullptr;
+    size_t h_res_cap = 0, h_walk_cap = 0;
+    uint64_t n_res = 0;
+    uint32_t n_walks = 0;
+    uint64_t prime_steps = 0;
+};
+
+struct Server {
+    dr_serve_config cfg{};
+    uint64_t cap = 0, admitted = 0;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::thread thr;
+    bool stop = false;
+    std::deque<int64_t> pending;
+    std::vector<int64_t> active;
+    std::unordered_map<int64_t, std::unique_ptr<Req>> reqs;
+    int64_t next_id = 1;
+    DevBuf stP, stSig, stShadow;
+    std::vector<uint32_t> free_slots, free_shadow;
+    std::deque<Wave> waves;               // deque: elements never move
+    uint64_t completed = 0, prime_steps = 0;
+    std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, size_t>, int> occ_cache;
+    int error = DR_OK;
+    std::string error_msg;
+};
+
+std::mutex g_srv_mu;
+std::map<int32_t, std::unique_ptr<Server>> g_servers;
+int32_t g_next_srv = 1;
+
+Server* find_server(int32_t h) {
+    std::lock_guard<std::mutex> lk(g_srv_mu);
+    auto it = g_servers.find(h);
+    return it == g_servers.end() ? nullptr : it->second.get();
+}
+
+uint64_t request_bytes(const Req& r) {
+    const uint64_t nb = (r.d.K + 31) / 32;
+    return nb * (kServeStride + 32) * 4 + (r.shadow_mode ? kShadowStateStride * 8 : 0) + 8ull * r.d.K;
+}
+
+template <class T>
+cudaError_t put(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
+    cudaError_t e = b.alloc(sizeof(T) * std::max<size_t>(v.size(), 1));
+    if (e != cudaSuccess || v.empty()) return e;
+    return cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st);
+}
+
+int occupancy(Server& S, int kind, uint32_t cls, uint32_t m, uint32_t D, int block, size_t smem) {
+    auto key = std::make_tuple(kind, cls, m, D, smem);
+    auto it = S.occ_cache.find(key);
+    if (it != S.occ_cache.end()) return it->second;
+    int occ = 0;
+    WalkArgs wa{};
+    ShadowArgs sa{};
+    cudaError_t e;
+    if (kind == 0) e = walk_dispatch(cls, m, D, 0, block, smem, nullptr, wa, &occ);
+    else if (kind == 1) e = shadow_interp_dispatch(m, 0, block, smem, nullptr, sa, &occ);
+    else e = shadow_fd_dispatch(cls, m, D, 0, block, smem, nullptr, sa, &occ);
+    if (e != cudaSuccess) occ = 0;
+    S.occ_cache[key] = occ;
+    return occ;
+}
+
+// Build and launch one wave from the admitted requests (called with S.mu held
+// only for the selection; the device work is issued without the lock).
+int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
+    Context& C = *ctx();
+    const uint32_t chunk = S.cfg.chunk_steps ? S.cfg.chunk_steps : 4096;
+    const uint64_t seg_walk = (uint64_t)chunk * 16;
+    const uint64_t seg_shadow = 8192;
+    std::map<std::string, int> pidx;
+    std::vector<DevProgram> progs;
+    std::vector<uint4> code;
+    std::vector<int64_t> consts, axis;
+    std::vector<DevWalk> walks;
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t>, std::vector<DevTile>> tsets;
+    std::vector<DevGroup> groups;
+    std::map<std::tuple<int, uint32_t, uint32_t, uint32_t>, std::vector<DevShadowSeg>> ssets;
+    uint32_t slots = 0;
+    uint64_t nres = 0, ps = 0;
+    W.reqs.clear();
+    W.walk_final.clear();
+    W.shadow_final.clear();
+    W.walk_end.clear();
+    W.shadow_end.clear();
+    W.res_off.clear();
+    W.widx.clear();
+    for (Req* r : sel) {
+        const Plan& P = *r->plan;
+        auto it = pidx.find(r->blob);
+        int pi;
+        if (it == pidx.end()) {
+            DevProgram d{};
+            d.m = P.m; d.dim = P.dim; d.cls = P.cls; d.degree = P.degree;
+            d.op_off = (uint32_t)code.size(); d.n_ops = (uint32_t)P.ops.size();
+            for (const Insn& in : P.ops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
+            d.n_regs = P.n_regs;
+            d.dop_off = (uint32_t)code.size(); d.dn_ops = (uint32_t)P.dops.size();
+            for (const Insn& in : P.dops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
+            d.dn_regs = P.dn_regs;
+            d.c_off = (uint32_t)consts.size(); d.n_consts = (uint32_t)P.consts.size();
+            consts.insert(consts.end(), P.consts.begin(), P.consts.end());
+            d.n_streams = P.n_streams; d.zero_reg = P.zero_reg;
+            pi = (int)progs.size();
+            progs.push_back(d);
+            pidx.emplace(r->blob, pi);
+        } else {
+            pi = it->second;
+        }
+        const uint32_t wi = (uint32_t)walks.size();
+        DevWalk w{};
+        w.prog = (uint32_t)pi; w.K = r->d.K; w.flags = r->d.flags; w.q_row = r->d.q_row;
+        w.a0 = r->d.a0; w.depth = r->d.depth; w.checkpoint = 0;
+        w.axis_off = axis.size();
+        axis.insert(axis.end(), r->axis.begin(), r->axis.end());
+        w.shadow_mode = r->shadow_mode;
+        const uint64_t we = std::min<uint64_t>(r->d.depth, r->walk_next + seg_walk);
+        const bool wfinal = !r->walk_done && we >= r->d.depth;
+        w.res_off = wfinal ? nres : 0;
+        if (wfinal) nres += r->d.K;
+        walks.push_back(w);
+        W.reqs.push_back(r->id);
+        W.widx.push_back(wi);
+        W.walk_final.push_back(wfinal);
+        W.walk_end.push_back(we);
+        W.res_off.push_back(w.res_off);
+        // walk tiles for [walk_next, we)
+        if (!r->walk_done) {
+            const uint64_t a = r->walk_next, b = we;
+            std::vector<std::pair<uint64_t, uint64_t>> ranges;
+            if (b == a) ranges.emplace_back(a, a);
+            for (uint64_t s0 = a; s0 < b; s0 += chunk) ranges.emplace_back(s0, std::min<uint64_t>(b, s0 + chunk));
+            const uint32_t cls = P.cls;
+            const uint32_t D = cls == CLS_INTERP ? 0u : (uint32_t)r->tdeg;
+            auto& tv = tsets[std::make_tuple(cls, P.m, D)];
+            for (uint32_t blk = 0, p0 = 0; p0 < r->d.K; p0 += 32, ++blk) {
+                DevGroup g{};
+                g.walk = wi; g.prime0 = p0; g.nprimes = std::min<uint32_t>(32, r->d.K - p0);
+                g.n_chunks = (uint32_t)ranges.size(); g.slot0 = slots; slots += g.n_chunks;
+                g.cp_chunks = 0; g.state = r->slots[blk];
+                g.flags = (a == 0 ? GROUP_FIRST : 0u) | (wfinal ? GROUP_FINAL : 0u);
+                const uint32_t gi = (uint32_t)groups.size();
+                groups.push_back(g);
+                for (uint32_t c = 0; c < g.n_chunks; ++c) {
+                    DevTile t{};
+                    t.walk = wi; t.group = gi; t.prime0 = p0; t.nprimes = g.nprimes; t.chunk = c;
+                    t.slot = g.slot0 + c; t.s0 = ranges[c].first; t.s1 = ranges[c].second;
+                    tv.push_back(t);
+                }
+            }
+            ps += (uint64_t)r->d.K * (b - a);
+        }
+        // shadow segment
+        uint64_t se = r->shadow_next;
+        bool sfinal = false;
+        if (r->shadow_mode != SHADOW_NONE && !r->shadow_done) {
+            se = std::min<uint64_t>(r->d.depth, r->shadow_next + seg_shadow);
+            sfinal = se >= r->d.depth;
+            DevShadowSeg g{wi, (uint32_t)r->shadow_slot, r->shadow_next, se};
+            if (r->shadow_mode == SHADOW_INTFD)
+                ssets[std::make_tuple(2, (uint32_t)P.cls, P.m, (uint32_t)r->tdeg)].push_back(g);
+            else
+                ssets[std::make_tuple(1, 0u, P.m, 0u)].push_back(g);
+        }
+        W.shadow_end.push_back(se);
+        W.shadow_final.push_back(sfinal);
+    }
+    W.n_res = std::max<uint64_t>(nres, 1);
+    W.n_walks = (uint32_t)walks.size();
+    W.prime_steps = ps;
+
+    // launches
+    std::vector<LaunchSpec> L;
+    std::vector<DevTile> tiles;
+    std::vector<DevShadowSeg> segs;
+    const int wpb = 4;
+    for (auto& kv : tsets) {
+        auto& v = kv.second;
+        std::stable_sort(v.begin(), v.end(), [](const DevTile& x, const DevTile& y) { return (x.s1 - x.s0) > (y.s1 - y.s0); });
+        LaunchSpec s{};
+        s.kind = 0;
+        std::tie(s.cls, s.m, s.D) = kv.first;
+        s.off = (uint32_t)tiles.size(); s.count = (uint32_t)v.size(); s.items = s.count;
+        uint32_t rr = 1, rc = 1;
+        for (auto& t : v) {
+            const DevProgram& G = progs[walks[t.walk].prog];
+            rr = std::max(rr, std::max(G.n_regs, G.dn_regs));
+            rc = std::max(rc, G.n_consts);
+        }
+        const uint32_t ns = (uint32_t)std::max(streams_for(s.cls, s.m), 0);
+        s.rows_regs = rr; s.rows_consts = rc; s.rows_stage = std::max(s.m * s.m, (s.D + 1) * ns);
+        s.rows_per_warp = s.rows_regs + s.rows_consts + 3 * kMaxAxes + s.rows_stage;
+        tiles.insert(tiles.end(), v.begin(), v.end());
+        L.push_back(s);
+    }
+    for (auto& kv : ssets) {
+        auto& v = kv.second;
+        LaunchSpec s{};
+        int kind;
+        std::tie(kind, s.cls, s.m, s.D) = kv.first;
+        s.kind = kind;
+        s.off = (uint32_t)segs.size(); s.count = (uint32_t)v.size();
+        s.items = kind == 1 ? s.count : (s.count + 31) / 32;
+        uint32_t rr = 1;
+        for (auto& g : v) {
+            const DevProgram& G = progs[walks[g.walk].prog];
+            rr = std::max(rr, kind == 1 ? G.n_regs : G.dn_regs);
+        }
+        const uint32_t ns = kind == 2 ? (uint32_t)streams_for(s.cls, s.m) : 0;
+        s.rows_regs = rr;
+        s.rows_per_warp = kind == 1 ? rr + kMaxAxes + s.m * s.m : rr + kMaxAxes + (s.D + 1) * ns + ns;
+        segs.insert(segs.end(), v.begin(), v.end());
+        L.push_back(s);
+    }
+    uint32_t q = 0;
+    for (auto& s : L) {
+        s.queue = q++;
+        s.block = 32 * wpb;
+        s.smem = (size_t)s.rows_per_warp * 32 * (s.kind == 0 ? 4 : 8) * wpb;
+        const int occ = occupancy(S, s.kind, s.cls, s.m, s.D, s.block, s.smem);
+        if (occ < 1) { set_error("serving: kernel cannot be resident"); return DR_ERR_UNSUPPORTED; }
+        s.grid = std::max(1, std::min((int)((s.items + wpb - 1) / wpb), occ * C.sms));
+    }
+    cudaStream_t st = W.st;
+    cudaError_t e = cudaSuccess;
+#define SV(x) do { e = (x); if (e != cudaSuccess) return cuda_fail(e, #x); } while (0)
+    SV(put(W.progs, progs, st));
+    SV(put(W.code, code, st));
+    SV(put(W.consts, consts, st));
+    SV(put(W.walks, walks, st));
+    SV(put(W.axis, axis, st));
+    SV(put(W.tiles, tiles, st));
+    SV(put(W.groups, groups, st));
+    SV(put(W.segs, segs, st));
+    SV(W.done_ctr.alloc(4ull * std::max<size_t>(groups.size(), 1)));
+    SV(cudaMemsetAsync(W.done_ctr.p, 0, 4ull * std::max<size_t>(groups.size(), 1), st));
+    SV(W.chunkP.alloc(4ull * std::max<uint32_t>(slots, 1) * kServeStride));
+    SV(W.chunkSig.alloc(4ull * std::max<uint32_t>(slots, 1) * 32));
+    SV(W.queues.alloc(4ull * std::max<uint32_t>(q, 1)));
+    SV(cudaMemsetAsync(W.queues.p, 0, 4ull * std::max<uint32_t>(q, 1), st));
+    SV(W.res.alloc(8ull * W.n_res));
+    SV(W.shadow.alloc(8ull * 6 * std::max<uint32_t>(W.n_walks, 1)));
+    SV(W.status.alloc(4ull * std::max<uint32_t>(W.n_walks, 1)));
+    SV(cudaMemsetAsync(W.status.p, 0, 4ull * std::max<uint32_t>(W.n_walks, 1), st));
+    WalkArgs wa{};
+    wa.progs = W.progs.as<DevProgram>(); wa.code = W.code.as<uint4>(); wa.consts = W.consts.as<int64_t>();
+    wa.walks = W.walks.as<DevWalk>(); wa.axis = W.axis.as<int64_t>(); wa.groups = W.groups.as<DevGroup>();
+    wa.group_done = W.done_ctr.as<uint32_t>(); wa.chunk_P = W.chunkP.as<uint32_t>();
+    wa.chunk_stride = kServeStride; wa.chunk_sig = W.chunkSig.as<uint32_t>();
+    wa.state_P = S.stP.as<uint32_t>(); wa.state_sig = S.stSig.as<uint32_t>();
+    wa.primes = C.primes.as<uint32_t>(); wa.pinv = C.pinv.as<uint32_t>(); wa.r2 = C.r2.as<uint32_t>();
+    wa.p_res = W.res.as<uint32_t>(); wa.q_res = W.res.as<uint32_t>() + W.n_res; wa.status = W.status.as<uint32_t>();
+    ShadowArgs sa{};
+    sa.progs = wa.progs; sa.code = wa.code; sa.consts = wa.consts; sa.walks = wa.walks; sa.axis = wa.axis;
+    sa.shadow = W.shadow.as<double>(); sa.n_walks = W.n_walks; sa.status = wa.status;
+    sa.state = S.stShadow.as<double>();
+    for (auto& s : L) {
+        if (s.items == 0) continue;
+        if (s.kind == 0) {
+            wa.tiles = W.tiles.as<DevTile>() + s.off; wa.n_tiles = s.count;
+            wa.queue = W.queues.as<uint32_t>() + s.queue;
+            wa.rows_regs = s.rows_regs; wa.rows_consts = s.rows_consts; wa.rows_stage = s.rows_stage;
+            wa.rows_per_warp = s.rows_per_warp;
+            SV(walk_dispatch(s.cls, s.m, s.D, s.grid, s.block, s.smem, st, wa, nullptr));
+        } else {
+            sa.segs = W.segs.as<DevShadowSeg>() + s.off; sa.n_items = s.items; sa.n_list = s.count;
+            sa.queue = W.queues.as<uint32_t>() + s.queue; sa.rows_regs = s.rows_regs;
+            sa.rows_per_warp = s.rows_per_warp;
+            if (s.kind == 1) SV(shadow_interp_dispatch(s.m, s.grid, s.block, s.smem, st, sa, nullptr));
+            else SV(shadow_fd_dispatch(s.cls, s.m, s.D, s.grid, s.block, s.smem, st, sa, nullptr));
+        }
+    }
+    // outputs back to pinned host memory
+    if (W.h_res_cap < 2 * W.n_res) {
+        if (W.h_res) cudaFreeHost(W.h_res);
+        W.h_res_cap = 2 * W.n_res + 1024;
+        SV(cudaMallocHost(&W.h_res, 4 * W.h_res_cap));
+    }
+    if (W.h_walk_cap < W.n_walks) {
+        if (W.h_sh) cudaFreeHost(W.h_sh);
+        if (W.h_st) cudaFreeHost(W.h_st);
+        W.h_walk_cap = W.n_walks + 256;
+        SV(cudaMallocHost(&W.h_sh, 8 * 6 * W.h_walk_cap));
+        SV(cudaMallocHost(&W.h_st, 4 * W.h_walk_cap));
+    }
+    SV(cudaMemcpyAsync(W.h_res, W.res.p, 8ull * W.n_res, cudaMemcpyDeviceToHost, st));
+    SV(cudaMemcpyAsync(W.h_sh, W.shadow.p, 8ull * 3 * W.n_walks, cudaMemcpyDeviceToHost, st));
+    SV(cudaMemcpyAsync(W.h_st, W.status.p, 4ull * W.n_walks, cudaMemcpyDeviceToHost, st));
+    SV(cudaEventRecord(W.ev, st));
+#undef SV
+    W.busy = true;
+    return DR_OK;
+}
+
+void release(Server& S, Req& r) {
+    for (uint32_t s : r.slots) S.free_slots.push_back(s);
+    r.slots.clear();
+    if (r.shadow_slot >= 0) S.free_shadow.push_back((uint32_t)r.shadow_slot);
+    r.shadow_slot = -1;
+    if (r.admitted) S.admitted -= r.need;
+    r.admitted = false;
+}
+
+void harvest(Server& S, Wave& W) {
+    for (size_t i = 0; i < W.reqs.size(); ++i) {
+        auto it = S.reqs.find(W.reqs[i]);
+        if (it == S.reqs.end()) continue;
+        Req& r = *it->second;
+        r.inflight = false;
+        if (r.cancelled) {
+            release(S, r);
+            auto a = std::find(S.active.begin(), S.active.end(), r.id);
+            if (a != S.active.end()) S.active.erase(a);
+            S.reqs.erase(it);
+            continue;
+        }
+        if (!r.walk_done) {
+            S.prime_steps += (uint64_t)r.d.K * (W.walk_end[i] - r.walk_next);
+            r.walk_next = W.walk_end[i];
+            if (W.walk_final[i]) {
+                r.walk_done = true;
+                r.p.assign(W.h_res + W.res_off[i], W.h_res + W.res_off[i] + r.d.K);
+                r.q.assign(W.h_res + W.n_res + W.res_off[i], W.h_res + W.n_res + W.res_off[i] + r.d.K);
+            }
+        }
+        r.status |= W.h_st[W.widx[i]];
+        if (r.shadow_mode != SHADOW_NONE && !r.shadow_done) {
+            r.shadow_next = W.shadow_end[i];
+            if (W.shadow_final[i]) {
+                r.shadow_done = true;
+                std::memcpy(r.sh, W.h_sh + 3 * W.widx[i], sizeof(r.sh));
+            }
+        }
+        if (r.walk_done && r.shadow_done && !r.done) {
+            r.done = true;
+            r.t_done = Clock::now();
+            ++S.completed;
+            release(S, r);
+            S.active.erase(std::find(S.active.begin(), S.active.end(), r.id));
+        }
+    }
+    W.busy = false;
+}
+
+void admit(Server& S) {
+    for (auto it = S.pending.begin(); it != S.pending.end();) {
+        Req& r = *S.reqs[*it];
+        if (r.cancelled) { it = S.pending.erase(it); continue; }
+        const uint64_t nb = (r.d.K + 31) / 32;
+        const bool fits = S.admitted + r.need <= S.cap && S.free_slots.size() >= nb &&
+                          (r.shadow_mode == SHADOW_NONE || !S.free_shadow.empty());
+        if (!fits) { ++it; continue; }   // smaller later requests may still fit
+        for (uint64_t b = 0; b < nb; ++b) { r.slots.push_back(S.free_slots.back()); S.free_slots.pop_back(); }
+        if (r.shadow_mode != SHADOW_NONE) { r.shadow_slot = (int)S.free_shadow.back(); S.free_shadow.pop_back(); }
+        S.admitted += r.need;
+        r.admitted = true;
+        S.active.push_back(r.id);
+        it = S.pending.erase(it);
+    }
+}
+
+void loop(Server* Sp) {
+    Server& S = *Sp;
+    cudaSetDevice(ctx()->device);
+    const uint32_t max_tiles = S.cfg.max_wave_tiles ? S.cfg.max_wave_tiles : 65536;
+    for (;;) {
+        std::vector<Req*> sel;
+        Wave* free_wave = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(S.mu);
+            for (Wave& W : S.waves)
+                if (W.busy && cudaEventQuery(W.ev) == cudaSuccess) harvest(S, W);
+            S.cv.notify_all();
+            if (S.stop) break;
+            admit(S);
+            for (Wave& W : S.waves)
+                if (!W.busy) { free_wave = &W; break; }
+            if (free_wave) {
+                uint64_t tiles = 0;
+                for (int64_t id : S.active) {
+                    Req& r = *S.reqs[id];
+                    if (r.inflight || r.done) continue;
+                    if (r.cancelled) continue;
+                    const uint64_t nb = (r.d.K + 31) / 32;
+                    const uint64_t span = std::min<uint64_t>(r.d.depth - r.walk_next,
+                                                             (uint64_t)(S.cfg.chunk_steps ? S.cfg.chunk_steps : 4096) * 16);
+                    const uint64_t t = r.walk_done ? 0 : nb * std::max<uint64_t>(1, (span + 4095) / 4096);
+                    if (!sel.empty() && tiles + t > max_tiles) break;
+                    tiles += t;
+                    r.inflight = true;
+                    sel.push_back(&r);
+                }
+            }
+            if (sel.empty()) {
+                S.cv.wait_for(lk, std::chrono::microseconds(200));
+                continue;
+            }
+        }
+        int rc = launch_wave(S, *free_wave, sel);
+        if (rc != DR_OK) {
+            std::lock_guard<std::mutex> lk(S.mu);
+            S.error = rc;
+            S.error_msg = last_error();
+            for (Req* r : sel) r->inflight = false;
+        }
+        if (rc != DR_OK) std::this_thread::sleep_for(std::chrono::milliseconds(1));
+    }
+}
+
+}  // namespace
+}  // namespace dr
+
+using namespace dr;
+
+extern "C" {
+
+int dr_serve_open(const dr_serve_config* cfg, int32_t* server_out) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    if (!server_out) return DR_ERR_ARG;
+    auto S = std::make_unique<Server>();
+    if (cfg) S->cfg = *cfg;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    S->cap = S->cfg.mem_cap_bytes ? S->cfg.mem_cap_bytes : std::min<uint64_t>(fr / 2, 1ull << 30);
+    const uint64_t per = (kServeStride + 32) * 4ull;
+    uint64_t n_slots = std::min<uint64_t>(S->cap / per + 1, 1u << 20);
+    uint64_t n_shadow = std::min<uint64_t>(S->cap / (kShadowStateStride * 8) + 1, 1u << 18);
+    {
+        cudaError_t e = S->stP.alloc(4ull * kServeStride * n_slots);
+        if (e == cudaSuccess) e = S->stSig.alloc(4ull * 32 * n_slots);
+        if (e == cudaSuccess) e = S->stShadow.alloc(8ull * kShadowStateStride * n_shadow);
+        if (e != cudaSuccess) return cuda_fail(e, "dr_serve_open");
+    }
+    for (uint64_t i = n_slots; i-- > 0;) S->free_slots.push_back((uint32_t)i);
+    for (uint64_t i = n_shadow; i-- > 0;) S->free_shadow.push_back((uint32_t)i);
+    const uint32_t nw = S->cfg.max_inflight ? S->cfg.max_inflight : 2;
+    S->waves.resize(nw);
+    for (Wave& W : S->waves) {
+        cudaError_t e = cudaStreamCreateWithFlags(&W.st, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&W.ev, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(e, "dr_serve_open");
+    }
+    Server* raw = S.get();
+    S->thr = std::thread(loop, raw);
+    std::lock_guard<std::mutex> lk(g_srv_mu);
+    const int32_t h = g_next_srv++;
+    g_servers[h] = std::move(S);
+    *server_out = h;
+    return DR_OK;
+}
+
+int dr_serve_submit(int32_t server, const dr_walk_desc* walk, const uint8_t* blob, uint64_t blob_size,
+                    const int64_t* axis_params, int64_t* request_out) {
+    Server* S = find_server(server);
+    if (!S) return DR_ERR_HANDLE;
+    if (!walk || !blob || !request_out) return DR_ERR_ARG;
+    auto r = std::make_unique<Req>();
+    std::string err;
+    int rc = get_plan(blob, blob_size, &r->plan, &err);
+    if (rc) { set_error(err); return rc; }
+    const Plan& P = *r->plan;
+    if (P.m > (uint32_t)kServeMaxM) { set_error("serving supports m <= 4"); return DR_ERR_UNSUPPORTED; }
+    if (walk->K < 1 || walk->K > DR_MAX_K) return DR_ERR_UNSUPPORTED;
+    if (walk->q_row >= P.m) return DR_ERR_ARG;
+    if (walk->checkpoint) { set_error("serving walks take no checkpoint"); return DR_ERR_ARG; }
+    if ((walk->flags & DR_WALK_INIT_PCF) && P.m < 2) return DR_ERR_ARG;
+    if (P.dim && !axis_params) return DR_ERR_ARG;
+    r->d = *walk;
+    r->blob.assign(reinterpret_cast<const char*>(blob), (size_t)blob_size);
+    r->axis.assign(axis_params, axis_params + 4 * P.dim);
+    for (uint32_t a = 0; a < P.dim; ++a)
+        if (r->axis[4 * a + 1] == 0 || r->axis[4 * a + 3] == 0) { set_error("zero denominator"); return DR_ERR_ARG; }
+    r->tdeg = P.cls == CLS_INTERP ? 0 : template_degree(P.cls, P.m, P.degree);
+    if (walk->flags & DR_WALK_SHADOW) {
+        r->shadow_mode = SHADOW_INTERP;
+        if (!P.has_inv && (P.cls == CLS_COMPANION || P.cls == CLS_DENSE) && r->tdeg > 0) {
+            const double b = float_bound_log2(P, r->axis.data(), walk->depth + 1);
+            if (b < 53.0 && b + r->tdeg < 61.0) r->shadow_mode = SHADOW_INTFD;
+        }
+    } else {
+        r->shadow_done = true;
+    }
+    r->need = request_bytes(*r);
+    r->t_submit = Clock::now();
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (r->need > S->cap) { set_error("request larger than the admission cap"); return DR_ERR_NOMEM; }
+    r->id = S->next_id++;
+    *request_out = r->id;
+    S->pending.push_back(r->id);
+    S->reqs[r->id] = std::move(r);
+    S->cv.notify_all();
+    return DR_OK;
+}
+
+int dr_serve_poll(int32_t server, int64_t request, uint32_t* p_res, uint32_t* q_res, double* shadow,
+                  uint32_t* status, double* latency_s) {
+    Server* S = find_server(server);
+    if (!S) return DR_ERR_HANDLE;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->error) { set_error(S->error_msg); return S->error; }
+    auto it = S->reqs.find(request);
+    if (it == S->reqs.end()) return DR_ERR_HANDLE;
+    Req& r = *it->second;
+    if (r.cancelled) return DR_ERR_HANDLE;
+    if (!r.done) return DR_ERR_BUSY;
+    if (p_res) std::memcpy(p_res, r.p.data(), 4ull * r.d.K);
+    if (q_res) std::memcpy(q_res, r.q.data(), 4ull * r.d.K);
+    if (shadow) std::memcpy(shadow, r.sh, sizeof(r.sh));
+    if (status) *status = r.status;
+    if (latency_s) *latency_s = std::chrono::duration<double>(r.t_done - r.t_submit).count();
+    S->reqs.erase(it);
+    return DR_OK;
+}
+
+int dr_serve_cancel(int32_t server, int64_t request) {
+    Server* S = find_server(server);
+    if (!S) return DR_ERR_HANDLE;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(request);
+    if (it == S->reqs.end()) return DR_ERR_HANDLE;
+    Req& r = *it->second;
+    if (r.inflight) { r.cancelled = true; return DR_OK; }   // dropped when its wave retires
+    r.cancelled = true;
+    if (r.admitted) {
+        release(*S, r);
+        auto a = std::find(S->active.begin(), S->active.end(), r.id);
+        if (a != S->active.end()) S->active.erase(a);
+    }
+    return DR_OK;
+}
+
+int dr_serve_stats(int32_t server, uint64_t* completed, uint64_t* prime_steps, uint64_t* admitted_bytes,
+                   uint32_t* queue_depth) {
+    Server* S = find_server(server);
+    if (!S) return DR_ERR_HANDLE;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (completed) *completed = S->completed;
+    if (prime_steps) *prime_steps = S->prime_steps;
+    if (admitted_bytes) *admitted_bytes = S->admitted;
+    if (queue_depth) *queue_depth = (uint32_t)(S->pending.size() + S->active.size());
+    return DR_OK;
+}
+
+int dr_serve_close(int32_t server) {
+    std::unique_ptr<Server> S;
+    {
+        std::lock_guard<std::mutex> lk(g_srv_mu);
+        auto it = g_servers.find(server);
+        if (it == g_servers.end()) return DR_ERR_HANDLE;
+        S = std::move(it->second);
+        g_servers.erase(it);
+    }
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv.notify_all();
+    }
+    if (S->thr.joinable()) S->thr.join();
+    for (Wave& W : S->waves) {
+        if (W.st) cudaStreamSynchronize(W.st);
+        if (W.ev) cudaEventDestroy(W.ev);
+        if (W.st) cudaStreamDestroy(W.st);
+        if (W.h_res) cudaFreeHost(W.h_res);
+        if (W.h_sh) cudaFreeHost(W.h_sh);
+        if (W.h_st) cudaFreeHost(W.h_st);
+    }
+    return DR_OK;
+}
+
+}  // extern "C"

@@ -30,16 +30,19 @@ struct ShadowArgs {
     const int64_t* consts;
     const DevWalk* walks;
     const int64_t* axis;
-    const uint32_t* list;       // walk indices of this launch
-    uint32_t n_items;           // interpreted: walks; integer: groups of 32 walks
-    uint32_t n_list;
+    const DevShadowSeg* segs;   // segments of this launch
+    uint32_t n_items;           // interpreted: segments; integer: groups of 32 segments
+    uint32_t n_list;            // segments
     uint32_t* queue;
     double* shadow;             // [3*w] final, [3*(n_walks + w)] checkpoint
     uint32_t n_walks;
     uint32_t* status;
+    double* state;              // resident chain state [slot][kShadowStateStride]
     uint32_t rows_regs;         // per-warp smem: doubles, 32 per row
     uint32_t rows_per_warp;
 };
+
+constexpr int kShadowStateStride = 72;   // m*m <= 64 entries, then mantissa, exponent, nan flag
 
 // log_scale = sum of ln(max) over the rescale points.  The logarithm is taken
 // once at the end: the product of the maxima is carried as mantissa * 2^exp
@@ -132,6 +135,39 @@ struct FChain {
         }
         nan_seen |= has_nan;
     }
+    __device__ __forceinline__ void load(const double* st) {
+#pragma unroll
+        for (int i = 0; i < M_; ++i)
+#pragma unroll
+            for (int j = 0; j < M_; ++j) P[i][j] = st[i * M_ + j];
+        sc_m = st[64];
+        sc_e = (int)st[65];
+        nan_seen = st[66] != 0.0;
+    }
+    __device__ __forceinline__ void store(double* st) const {
+#pragma unroll
+        for (int i = 0; i < M_; ++i)
+#pragma unroll
+            for (int j = 0; j < M_; ++j) st[i * M_ + j] = P[i][j];
+        st[64] = sc_m;
+        st[65] = (double)sc_e;
+        st[66] = nan_seen ? 1.0 : 0.0;
+    }
+    // start of a segment: the walk's initial matrix at step 0, else the state
+    __device__ __forceinline__ void begin(const DevWalk& W, const DevShadowSeg& g, const double* state) {
+        if (g.s0 == 0 || g.state == kNoState) init(W);
+        else load(state + (size_t)g.state * kShadowStateStride);
+    }
+    // end of a segment: final outputs, or the state for the next segment
+    __device__ __forceinline__ void end(const DevWalk& W, const DevShadowSeg& g, double* state,
+                                        double* shadow, uint32_t* status, uint32_t w) const {
+        if (g.s1 >= W.depth || g.state == kNoState) {
+            write(shadow + 3 * (size_t)w, W);
+            if (nan_seen || !isfinite(P[0][M_ - 1])) atomicOr(status + w, DR_STATUS_SHADOW_NAN);
+        } else {
+            store(state + (size_t)g.state * kShadowStateStride);
+        }
+    }
     __device__ __forceinline__ void write(double* out, const DevWalk& W) const {
         double q = P[0][M_ - 1];
 #pragma unroll
@@ -164,21 +200,22 @@ __global__ void __launch_bounds__(128) k_shadow_interp(const ShadowArgs A) {
         if (lane == 0) it = atomicAdd(A.queue, 1u);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= A.n_items) break;
-        const uint32_t w = A.list[it];
+        const DevShadowSeg g = A.segs[it];
+        const uint32_t w = g.walk;
         const DevWalk W = A.walks[w];
         const DevProgram G = A.progs[W.prog];
         FChain<M_> ch;
-        ch.init(W);
+        ch.begin(W, g, A.state);
         const int64_t* ax = A.axis + W.axis_off;
         if (G.zero_reg != 0xffffffffu) rf[G.zero_reg * 32 + lane] = 0.0;
-        for (uint64_t s0 = 0; s0 < W.depth; s0 += 32) {
+        for (uint64_t s0 = g.s0; s0 < g.s1; s0 += 32) {
             const int64_t s = (int64_t)(s0 + lane);
             for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = axis_f64(ax + 4 * a, s);
             for (int e = 0; e < M_ * M_; ++e) mf[e * 32 + lane] = 0.0;
             __syncwarp();
             interp_f64(A.code + G.op_off, G.n_ops, rf, A.consts + G.c_off, axv, (double)s, mf, lane);
             __syncwarp();
-            const uint32_t n = (uint32_t)min((uint64_t)32, W.depth - s0);
+            const uint32_t n = (uint32_t)min((uint64_t)32, g.s1 - s0);
             for (uint32_t j = 0; j < n; ++j) {
                 double X[M_][M_];
 #pragma unroll
@@ -189,10 +226,8 @@ __global__ void __launch_bounds__(128) k_shadow_interp(const ShadowArgs A) {
             }
             __syncwarp();
         }
-        if (lane == 0) {
-            ch.write(A.shadow + 3 * (size_t)w, W);
-            if (ch.nan_seen || !isfinite(ch.P[0][M_ - 1])) atomicOr(A.status + w, DR_STATUS_SHADOW_NAN);
-        }
+        if (lane == 0) ch.end(W, g, A.state, A.shadow, A.status, w);
+        __syncwarp();
     }
 }
 
@@ -215,12 +250,13 @@ __global__ void __launch_bounds__(128) k_shadow_intfd(const ShadowArgs A) {
         if (it >= A.n_items) break;
         const uint32_t first = it * 32;
         const uint32_t count = min(32u, A.n_list - first);
-        // difference tables: lane j evaluates walk w at step j
+        // difference tables: lane j evaluates segment w's walk at step s0 + j
         for (uint32_t w = 0; w < count; ++w) {
-            const DevWalk W = A.walks[A.list[first + w]];
+            const DevShadowSeg g = A.segs[first + w];
+            const DevWalk W = A.walks[g.walk];
             const DevProgram G = A.progs[W.prog];
             const int64_t* ax = A.axis + W.axis_off;
-            const int64_t s = lane;
+            const int64_t s = (int64_t)g.s0 + lane;
             for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = ax[0 + 4 * a] + s * ax[2 + 4 * a];
             __syncwarp();
             interp_i64(A.code + G.dop_off, G.dn_ops, rf, A.consts + G.c_off, axv, s, outv, lane);
@@ -232,7 +268,8 @@ __global__ void __launch_bounds__(128) k_shadow_intfd(const ShadowArgs A) {
             __syncwarp();
         }
         const bool active = (uint32_t)lane < count;
-        const uint32_t wi = active ? A.list[first + lane] : A.list[first];
+        const DevShadowSeg g = A.segs[first + (active ? lane : 0)];
+        const uint32_t wi = g.walk;
         const DevWalk W = A.walks[wi];
         const DevProgram G = A.progs[W.prog];
         int64_t fd[NS][D + 1];
@@ -248,9 +285,9 @@ __global__ void __launch_bounds__(128) k_shadow_intfd(const ShadowArgs A) {
 #pragma unroll
                     for (int i = 0; i < NS; ++i) fd[i][j] -= fd[i][j - 1];
         FChain<M_> ch;
-        ch.init(W);
-        const uint64_t depth = active ? W.depth : 0;
-        for (uint64_t s = 0; s < depth; ++s) {
+        ch.begin(W, g, A.state);
+        const uint64_t s_end = active ? g.s1 : g.s0;
+        for (uint64_t s = g.s0; s < s_end; ++s) {
             if (CLS == CLS_COMPANION) {
                 double c[M_];
 #pragma unroll
@@ -268,10 +305,7 @@ __global__ void __launch_bounds__(128) k_shadow_intfd(const ShadowArgs A) {
                 for (int j = 0; j < D; ++j) fd[i][j] += fd[i][j + 1];
             if (W.checkpoint && s + 1 == W.checkpoint) ch.write(A.shadow + 3 * ((size_t)A.n_walks + wi), W);
         }
-        if (active) {
-            ch.write(A.shadow + 3 * (size_t)wi, W);
-            if (ch.nan_seen || !isfinite(ch.P[0][M_ - 1])) atomicOr(A.status + wi, DR_STATUS_SHADOW_NAN);
-        }
+        if (active) ch.end(W, g, A.state, A.shadow, A.status, wi);
         __syncwarp();
     }
 }

@@ -39,6 +39,8 @@ struct WalkArgs {
     uint32_t* chunk_P;          // [slot][m*m][32], slots chunk_stride words apart
     uint32_t chunk_stride;      // words per slot: max m*m of the batch times 32
     uint32_t* chunk_sig;        // [slot][32]
+    uint32_t* state_P;          // resident running products [state][chunk_stride words]
+    uint32_t* state_sig;        // resident denominators [state][32]
     const uint32_t* primes;     // prime table and Montgomery constants
     const uint32_t* pinv;
     const uint32_t* r2;
@@ -188,7 +190,8 @@ __device__ __forceinline__ void finish_tile(const WalkArgs& A, const DevTile& T,
                                             const uint32_t (&P)[M_][M_], uint32_t sig, bool scaled,
                                             const Mont& M, int lane) {
     const DevGroup Gr = A.groups[T.group];
-    if (Gr.n_chunks == 1) {
+    const bool resident = Gr.state != kNoState;
+    if (Gr.n_chunks == 1 && !resident) {
         emit<M_>(A, T, W, W.res_off, P, sig, scaled, M, lane);
         return;
     }
@@ -203,11 +206,20 @@ __device__ __forceinline__ void finish_tile(const WalkArgs& A, const DevTile& T,
     old = __shfl_sync(kFull, old, 0);
     if (old != Gr.n_chunks - 1) return;
     __threadfence();
+    // running product: the resident state of earlier segments, else I (the
+    // walk's first chunk already started from its initial matrix)
     uint32_t Q[M_][M_];
     uint32_t acc = M.one;
+    const bool from_state = resident && !(Gr.flags & GROUP_FIRST);
+    if (from_state) {
+        const uint32_t* sp = A.state_P + (size_t)Gr.state * A.chunk_stride;
+#pragma unroll
+        for (int e = 0; e < M_ * M_; ++e) Q[e / M_][e % M_] = __ldcg(sp + e * 32 + lane);
+        acc = __ldcg(A.state_sig + (size_t)Gr.state * 32 + lane);
+    }
     for (uint32_t c = 0; c < Gr.n_chunks; ++c) {
         const uint32_t* src = A.chunk_P + (size_t)(Gr.slot0 + c) * A.chunk_stride;
-        if (c == 0) {
+        if (c == 0 && !from_state) {
 #pragma unroll
             for (int e = 0; e < M_ * M_; ++e) Q[e / M_][e % M_] = __ldcg(src + e * 32 + lane);
         } else {
@@ -219,7 +231,14 @@ __device__ __forceinline__ void finish_tile(const WalkArgs& A, const DevTile& T,
         if (scaled) acc = mmul(acc, __ldcg(A.chunk_sig + (size_t)(Gr.slot0 + c) * 32 + lane), M);
         if (c + 1 == Gr.cp_chunks) emit<M_>(A, T, W, W.cp_res_off, Q, acc, scaled, M, lane);
     }
-    emit<M_>(A, T, W, W.res_off, Q, acc, scaled, M, lane);
+    if (!resident || (Gr.flags & GROUP_FINAL)) {
+        emit<M_>(A, T, W, W.res_off, Q, acc, scaled, M, lane);
+    } else {
+        uint32_t* sp = A.state_P + (size_t)Gr.state * A.chunk_stride;
+#pragma unroll
+        for (int e = 0; e < M_ * M_; ++e) __stcg(sp + e * 32 + lane, Q[e / M_][e % M_]);
+        __stcg(A.state_sig + (size_t)Gr.state * 32 + lane, acc);
+    }
     if (lane == 0) A.group_done[T.group] = 0u;  // re-armed for the next run of this batch
 }
 
@@ -272,7 +291,7 @@ __device__ __forceinline__ void tile_companion(const WalkArgs& A, const DevTile&
     uint32_t fd[M_][D + 1];
     bool inv0 = fd_init<M_, D>(fd, A, G, wm, T.s0, M, lane);
     uint32_t P[M_][M_];
-    init_P<M_>(P, W, T.chunk == 0, M);
+    init_P<M_>(P, W, T.s0 == 0, M);
     const uint32_t n = (uint32_t)(T.s1 - T.s0);
 #pragma unroll 2
     for (uint32_t t = 0; t < n; ++t) {
@@ -303,7 +322,7 @@ __device__ __forceinline__ void tile_rational(const WalkArgs& A, const DevTile& 
     uint32_t fd[M_ + 1][D + 1];
     bool inv0 = fd_init<M_ + 1, D>(fd, A, G, wm, T.s0, M, lane);
     uint32_t P[M_][M_];
-    init_P<M_>(P, W, T.chunk == 0, M);
+    init_P<M_>(P, W, T.s0 == 0, M);
     uint32_t sig = M.one;
     const uint32_t n = (uint32_t)(T.s1 - T.s0);
 #pragma unroll 1
@@ -345,7 +364,7 @@ __device__ __forceinline__ void tile_dense(const WalkArgs& A, const DevTile& T, 
     uint32_t fd[M_ * M_][D + 1];
     bool inv0 = fd_init<M_ * M_, D>(fd, A, G, wm, T.s0, M, lane);
     uint32_t P[M_][M_];
-    init_P<M_>(P, W, T.chunk == 0, M);
+    init_P<M_>(P, W, T.s0 == 0, M);
     const uint32_t n = (uint32_t)(T.s1 - T.s0);
 #pragma unroll 1
     for (uint32_t t = 0; t < n; ++t) {
@@ -367,7 +386,7 @@ __device__ __forceinline__ void tile_interp(const WalkArgs& A, const DevTile& T,
                                             const DevProgram& G, const WarpMem& wm, int lane) {
     const Mont M = tile_setup(A, T, W, G, wm, lane);
     uint32_t P[M_][M_];
-    init_P<M_>(P, W, T.chunk == 0, M);
+    init_P<M_>(P, W, T.s0 == 0, M);
     bool inv0 = false;
     // axis values advance by dx per step; the step counter by one
     uint32_t s_m = to_mont_u64(T.s0, M);
@@ -387,7 +406,7 @@ __device__ __forceinline__ void tile_interp(const WalkArgs& A, const DevTile& T,
     }
     if (__any_sync(kFull, inv0 && (uint32_t)lane < T.nprimes) && lane == 0)
         atomicOr(A.status + T.walk, DR_STATUS_INV0 | DR_STATUS_FALLBACK);
-    else if (lane == 0 && T.chunk == 0)
+    else if (lane == 0 && T.s0 == 0)
         atomicOr(A.status + T.walk, DR_STATUS_FALLBACK);
     finish_tile<M_>(A, T, W, P, M.one, false, M, lane);
 }

@@ -1,0 +1,90 @@
+"""Serving: results are identical alone and in the mix; admission, resume
+from device state, cancellation."""
+
+import random
+import time
+
+import numpy as np
+import pytest
+
+import dreams_rns as dr
+from dreams_rns import _native as N
+from dreams_rns.engine import cmf_request, pcf_request, run_walks
+from dreams_rns.serving import WalkServer
+
+pytestmark = pytest.mark.gpu
+
+
+def _mix(seed, n=40):
+    rng = random.Random(seed)
+    reqs = []
+    ws = dr.synth.uniform_pcfs(n // 2, seed=seed, depth=10, limit_depth=10)
+    for w in ws:
+        reqs.append(pcf_request(dr.compile_pcf(w.a, w.b), w.a0, rng.randrange(0, 3000),
+                                rng.choice([16, 32, 64])))
+    for w in dr.synth.rational_pcfs(n // 4, seed=seed + 1, depth_range=(100, 2000)):
+        reqs.append(pcf_request(dr.compile_pcf(w.a, w.b), w.a0, w.depth, w.K))
+    c = dr.synth.cmf3_sweep(n // 4, n_cmfs=2, seed=seed + 2, depth=700, K=40)
+    for w in c:
+        prog = dr.compile_cmf_from_dict(w.matrix, m=3, dim=3, axis_names=["x", "y", "z"])
+        reqs.append(cmf_request(prog, w.depth, w.K, w.shifts, w.trajectory))
+    # a long walk that needs several segments (walk and shadow)
+    reqs.append(pcf_request(dr.compile_pcf("2*n+1", "-n**2 + 3"), 1, 150_000, 96))
+    return reqs
+
+
+def _same(a, b):
+    assert list(a["p_residues"]) == list(b["p_residues"])
+    assert list(a["q_residues"]) == list(b["q_residues"])
+    for k in ("p_float", "q_float", "log_scale"):
+        assert a[k] == b[k] or (np.isnan(a[k]) and np.isnan(b[k])), k
+
+
+def test_alone_and_in_the_mix():
+    reqs = _mix(5)
+    batch = run_walks(reqs)
+    with WalkServer(max_inflight=3, chunk_steps=2048) as srv:
+        # each request alone
+        alone = {}
+        for i in (0, 7, len(reqs) - 1):
+            rid = srv.submit(reqs[i])
+            alone[i] = srv.wait([rid])[rid]
+        # all of them, arriving in waves while earlier ones run
+        ids = []
+        for i, r in enumerate(reqs):
+            ids.append(srv.submit(r))
+            if i % 9 == 0:
+                time.sleep(0.002)
+        got = srv.wait(ids, timeout=120)
+        st = srv.stats()
+    for i, rid in enumerate(ids):
+        _same(got[rid], batch[i])
+    for i, r in alone.items():
+        _same(r, batch[i])
+    assert st["completed"] == len(reqs) + len(alone)
+    assert st["queue_depth"] == 0 and st["admitted_bytes"] == 0
+
+
+def test_admission_cap_queues_requests():
+    reqs = _mix(8, n=16)[:-1]
+    batch = run_walks(reqs)
+    # cap small enough that only a couple of walks fit at once
+    with WalkServer(mem_cap_bytes=12_000, max_inflight=2) as srv:
+        ids = [srv.submit(r) for r in reqs]
+        got = srv.wait(ids, timeout=120)
+    for i, rid in enumerate(ids):
+        _same(got[rid], batch[i])
+
+
+def test_oversize_and_cancel():
+    big = pcf_request(dr.compile_pcf("1", "n"), 1, 1000, 2048)
+    with WalkServer(mem_cap_bytes=20_000) as srv:
+        with pytest.raises(MemoryError):
+            srv.submit(big)
+        long = pcf_request(dr.compile_pcf("n", "n**2"), 0, 400_000, 64)
+        rid = srv.submit(long)
+        srv.cancel(rid)
+        r2 = srv.submit(pcf_request(dr.compile_pcf("2", "n**2"), 2, 2000, 32))
+        res = srv.wait([r2])[r2]
+    g = run_walks([pcf_request(dr.compile_pcf("2", "n**2"), 2, 2000, 32)])[0]
+    _same(res, g)
