@@ -157,6 +157,142 @@ def algorithmic_int_ops(info, K_, depth):
     return per * K_ * depth
 
 
+# ---- further workloads (single-GPU runs) ------------------------------------
+
+def _compile_cmf(mat):
+    import dreams_rns as dr
+    return dr.compile_cmf_from_dict(mat, m=3, dim=3, axis_names=["x", "y", "z"]).serialize()
+
+
+def _time_batch(batch, stream, torch, reps=3):
+    batch.run(stream.cuda_stream)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        batch.run(stream.cuda_stream)
+        e1.record(stream)
+        ts.append((e0, e1))
+    torch.cuda.synchronize()
+    return statistics.median(a.elapsed_time(b) for a, b in ts)
+
+
+def bench_rational(stream, torch):
+    """Uneven batch: 8192 rational PCFs (INV every step), depth log-uniform in
+    [200, 50000], K in {16,32,64,128}, bytecode 10..200 ops, one graph-captured
+    persistent launch set with device top-256 by delta against pi."""
+    import mpmath as mp_
+    import dreams_rns as dr
+    from dreams_rns.engine import WalkBatch, pcf_request
+    cand = dr.synth.rational_pcfs(10000, seed=3)
+    blobs = compile_all(cand)
+    n_ops = lambda b: int.from_bytes(b[8:12], "little")  # noqa: E731  (blob header: m, dim, n_ops, n_consts)
+    keep = [(b, w) for b, w in zip(blobs, cand) if 10 <= n_ops(b) <= 200][:8192]
+    reqs = [pcf_request(b, w.a0, w.depth, w.K) for b, w in keep]
+    batch = WalkBatch(reqs)
+    mp_.mp.dps = 200
+    batch.set_pipeline(delta="fixed", target=dr.runner.target_ratio(mp_.pi), topk=256)
+    ms = _time_batch(batch, stream, torch)
+    st = batch.stats()
+    pl = batch.read_pipeline()
+    batch.close()
+    return {"walks": len(reqs), "prime_steps": st["prime_steps"], "ms": ms,
+            "prime_steps_per_s": st["prime_steps"] / (ms * 1e-3), "launches": st["launches"],
+            "top1_delta": float(pl["topk_val"][0]) if len(pl["topk_val"]) else None}
+
+
+def bench_cmf3(stream, torch, n_walks=16384):
+    """3x3 CMF sweep: 16384 (shift, direction) pairs over 64 cubic CMFs, depth
+    5000, K=64, top-100 by delta against zeta(3); plus the plain path (one walk
+    per launch, per-step interpreter) on a few walks for comparison."""
+    import mpmath as mp_
+    import dreams_rns as dr
+    from dreams_rns import _native as N
+    from dreams_rns.engine import WalkBatch, cmf_request
+    ws = dr.synth.cmf3_sweep(n_walks, n_cmfs=64, seed=4)
+    keys = {}
+    for w in ws:
+        keys.setdefault(w.program_key, w.matrix)
+    with mp.get_context("spawn").Pool(min(os.cpu_count() or 4, 16)) as pool:
+        kb = dict(zip(keys, pool.map(_compile_cmf, list(keys.values()))))
+    reqs = [cmf_request(kb[w.program_key], w.depth, w.K, w.shifts, w.trajectory) for w in ws]
+    batch = WalkBatch(reqs)
+    mp_.mp.dps = 200
+    batch.set_pipeline(delta="fixed", target=dr.runner.target_ratio(mp_.zeta(3)), topk=100)
+    ms = _time_batch(batch, stream, torch)
+    st = batch.stats()
+    batch.close()
+    rate = st["prime_steps"] / (ms * 1e-3)
+    plain_ms = []
+    for w in ws[:3]:
+        b = WalkBatch([cmf_request(kb[w.program_key], w.depth, w.K, w.shifts, w.trajectory)],
+                      engine=N.DR_ENGINE_PLAIN)
+        plain_ms.append(_time_batch(b, stream, torch, reps=1))
+        b.close()
+    plain_rate = 5000 * 64 / (statistics.median(plain_ms) * 1e-3)
+    return {"walks": len(reqs), "prime_steps": st["prime_steps"], "ms": ms, "prime_steps_per_s": rate,
+            "plain_one_walk_per_launch_prime_steps_per_s": plain_rate,
+            "batched_over_plain": rate / plain_rate}
+
+
+def bench_serving(seconds=3.0, rate=1000.0):
+    """Serving stream: Poisson arrivals drawn from the single-PCF, uniform-PCF
+    and rational-PCF generators, plus 1% deep walks (deg-1 a, b, depth 10^6,
+    K=512); p50/p99 request latency and prime-steps/s."""
+    import random
+    import numpy as np
+    import dreams_rns as dr
+    from dreams_rns.engine import pcf_request
+    from dreams_rns.serving import WalkServer
+    rng = random.Random(11)
+    nrng = np.random.default_rng(12)
+    uni = dr.synth.uniform_pcfs(96, seed=21, depth=2000, limit_depth=2000)
+    rat = dr.synth.rational_pcfs(96, seed=22)
+    deep = [dr.synth.deep_pcf(nrng) for _ in range(6)]
+    ub = compile_all(uni)
+    rb = compile_all(rat)
+    db = compile_all(deep)
+    single = dr.compile_pcf("2", "n**2").serialize()
+    pool = ([("single", pcf_request(single, 2, 2000, 32))] +
+            [("uniform", pcf_request(b, w.a0, 2000, 32)) for b, w in zip(ub, uni)] +
+            [("rational", pcf_request(b, w.a0, w.depth, w.K)) for b, w in zip(rb, rat)])
+    deep_reqs = [pcf_request(b, w.a0, w.depth, w.K) for b, w in zip(db, deep)]
+    arrivals = []
+    t = 0.0
+    while t < seconds:
+        t += rng.expovariate(rate)
+        if rng.random() < 0.01:
+            arrivals.append((t, "deep", rng.choice(deep_reqs)))
+        else:
+            kind, req = rng.choice(pool)
+            arrivals.append((t, kind, req))
+    lat = {}
+    kinds = {}
+    with WalkServer(max_inflight=3) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for at, kind, req in arrivals:
+            while time.perf_counter() - t0 < at:
+                pass
+            rid = srv.submit(req)
+            ids.append(rid)
+            kinds[rid] = kind
+        res = srv.wait(ids, timeout=600)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    for rid, r in res.items():
+        lat.setdefault(kinds[rid], []).append(r["latency_s"])
+    allv = sorted(v for vs in lat.values() for v in vs)
+    pct = lambda v, q: v[min(len(v) - 1, int(q * len(v)))] * 1e3  # noqa: E731
+    return {"requests": len(ids), "arrival_rate_per_s": rate, "seconds": seconds,
+            "p50_ms": pct(allv, 0.50), "p99_ms": pct(allv, 0.99),
+            "p50_ms_by_kind": {k: pct(sorted(v), 0.5) for k, v in lat.items()},
+            "p99_ms_by_kind": {k: pct(sorted(v), 0.99) for k, v in lat.items()},
+            "prime_steps": st["prime_steps"], "prime_steps_per_s": st["prime_steps"] / wall,
+            "wall_s": wall}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -164,6 +300,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the rational, CMF-sweep and serving measurements")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -326,6 +464,18 @@ def main():
             "gpu_launches": n_launch,
             "roofline": roofline,
             "top1_delta": float(pipe["topk_val"][0]) if len(pipe["topk_val"]) else None}
+    if dist:
+        from dreams_rns.distributed import global_topk
+        base = rank * N_WALKS
+        local = [(float(v), base + int(i)) for i, v in zip(pipe["topk_idx"], pipe["topk_val"])]
+        g = global_topk(local, TOPK)
+        line["global_top1_delta"] = g[0][0] if g else None
+    if world == 1 and not args.no_extras:
+        line["rational_pcf_batch"] = bench_rational(stream, torch)
+        line["cmf3_sweep"] = bench_cmf3(stream, torch)
+        line["serving"] = bench_serving()
+        line["p50_ms"] = line["serving"]["p50_ms"]
+        line["p99_ms"] = line["serving"]["p99_ms"]
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(blobs, ws)
     batch.close()

@@ -528,14 +528,9 @@ static int enqueue_pipeline(Batch& B, cudaStream_t st) {
     return DR_OK;
 }
 
-// One run of a batch: zero the work counters and status words, then every
-// launch group (shadow kernels first, they have the longest serial chains)
-// on its own stream of the pool, forked from and joined back into st.
-static int enqueue_batch(Batch& B, cudaStream_t st) {
+static void batch_args(Batch& B, WalkArgs& wa, ShadowArgs& sa) {
     Context& C = *g_ctx;
-    DR_CUDA(cudaMemsetAsync(B.queues.p, 0, B.queues.bytes, st));
-    DR_CUDA(cudaMemsetAsync(B.status.p, 0, B.status.bytes, st));
-    WalkArgs wa{};
+    wa = WalkArgs{};
     wa.progs = B.progs.as<DevProgram>();
     wa.code = B.code.as<uint4>();
     wa.consts = B.consts.as<int64_t>();
@@ -546,13 +541,15 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
     wa.chunk_P = B.chunkP.as<uint32_t>();
     wa.chunk_stride = B.chunk_stride;
     wa.chunk_sig = B.chunkSig.as<uint32_t>();
+    wa.state_P = nullptr;
+    wa.state_sig = nullptr;
     wa.primes = C.primes.as<uint32_t>();
     wa.pinv = C.pinv.as<uint32_t>();
     wa.r2 = C.r2.as<uint32_t>();
     wa.p_res = B.res.as<uint32_t>();
     wa.q_res = B.res.as<uint32_t>() + std::max<uint64_t>(B.n_res, 1);
     wa.status = B.status.as<uint32_t>();
-    ShadowArgs sa{};
+    sa = ShadowArgs{};
     sa.progs = wa.progs;
     sa.code = wa.code;
     sa.consts = wa.consts;
@@ -562,8 +559,39 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
     sa.n_walks = B.n_walks;
     sa.status = wa.status;
     sa.state = nullptr;
-    wa.state_P = nullptr;
-    wa.state_sig = nullptr;
+}
+
+static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, ShadowArgs& sa, cudaStream_t s) {
+    if (L.kind == 0) {
+        wa.tiles = B.tiles.as<DevTile>() + L.off;
+        wa.n_tiles = L.count;
+        wa.queue = B.queues.as<uint32_t>() + L.queue;
+        wa.rows_regs = L.rows_regs;
+        wa.rows_consts = L.rows_consts;
+        wa.rows_stage = L.rows_stage;
+        wa.rows_per_warp = L.rows_per_warp;
+        return walk_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, wa, nullptr);
+    }
+    sa.segs = B.shadow_list.as<DevShadowSeg>() + L.off;
+    sa.n_items = L.items;
+    sa.n_list = L.count;
+    sa.queue = B.queues.as<uint32_t>() + L.queue;
+    sa.rows_regs = L.rows_regs;
+    sa.rows_per_warp = L.rows_per_warp;
+    return L.kind == 1 ? shadow_interp_dispatch(L.m, L.grid, L.block, L.smem, s, sa, nullptr)
+                       : shadow_fd_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, sa, nullptr);
+}
+
+// One run of a batch: zero the work counters and status words, then every
+// launch group (shadow kernels first, they have the longest serial chains)
+// on its own stream of the pool, forked from and joined back into st.
+static int enqueue_batch(Batch& B, cudaStream_t st) {
+    Context& C = *g_ctx;
+    DR_CUDA(cudaMemsetAsync(B.queues.p, 0, B.queues.bytes, st));
+    DR_CUDA(cudaMemsetAsync(B.status.p, 0, B.status.bytes, st));
+    WalkArgs wa;
+    ShadowArgs sa;
+    batch_args(B, wa, sa);
     DR_CUDA(cudaEventRecord(B.fork, st));
     const size_t np = C.pool.size();
     size_t used = 0;
@@ -573,26 +601,7 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
             cudaStream_t s = C.pool[used % np];
             if (used < np) DR_CUDA(cudaStreamWaitEvent(s, B.fork, 0));
             ++used;
-            cudaError_t e;
-            if (L.kind == 0) {
-                wa.tiles = B.tiles.as<DevTile>() + L.off;
-                wa.n_tiles = L.count;
-                wa.queue = B.queues.as<uint32_t>() + L.queue;
-                wa.rows_regs = L.rows_regs;
-                wa.rows_consts = L.rows_consts;
-                wa.rows_stage = L.rows_stage;
-                wa.rows_per_warp = L.rows_per_warp;
-                e = walk_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, wa, nullptr);
-            } else {
-                sa.segs = B.shadow_list.as<DevShadowSeg>() + L.off;
-                sa.n_items = L.items;
-                sa.n_list = L.count;
-                sa.queue = B.queues.as<uint32_t>() + L.queue;
-                sa.rows_regs = L.rows_regs;
-                sa.rows_per_warp = L.rows_per_warp;
-                e = L.kind == 1 ? shadow_interp_dispatch(L.m, L.grid, L.block, L.smem, s, sa, nullptr)
-                                : shadow_fd_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, sa, nullptr);
-            }
+            cudaError_t e = launch_one(B, L, wa, sa, s);
             if (e != cudaSuccess) {
                 // rejoin what was forked so a capture can end cleanly
                 for (size_t i = 0; i < std::min(used, np); ++i) {
@@ -608,6 +617,33 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
         DR_CUDA(cudaStreamWaitEvent(st, B.joins[i], 0));
     }
     if (B.pipe_on) return enqueue_pipeline(B, st);
+    return DR_OK;
+}
+
+// Every launch group alone, one after another on one stream, timed with
+// events: where a batch's time goes (used by the autotuner and diagnostics).
+int batch_profile(Batch& B, std::vector<float>* ms) {
+    Context& C = *g_ctx;
+    cudaStream_t st = C.stream;
+    WalkArgs wa;
+    ShadowArgs sa;
+    batch_args(B, wa, sa);
+    DR_CUDA(cudaMemsetAsync(B.queues.p, 0, B.queues.bytes, st));
+    DR_CUDA(cudaMemsetAsync(B.status.p, 0, B.status.bytes, st));
+    std::vector<cudaEvent_t> ev(B.launches.size() + 1);
+    for (auto& e : ev) DR_CUDA(cudaEventCreate(&e));
+    DR_CUDA(cudaEventRecord(ev[0], st));
+    for (size_t i = 0; i < B.launches.size(); ++i) {
+        if (B.launches[i].items) {
+            cudaError_t e = launch_one(B, B.launches[i], wa, sa, st);
+            if (e != cudaSuccess) return cuda_fail(e, "profile launch");
+        }
+        DR_CUDA(cudaEventRecord(ev[i + 1], st));
+    }
+    DR_CUDA(cudaStreamSynchronize(st));
+    ms->assign(B.launches.size(), 0.f);
+    for (size_t i = 0; i < B.launches.size(); ++i) cudaEventElapsedTime(&(*ms)[i], ev[i], ev[i + 1]);
+    for (auto& e : ev) cudaEventDestroy(e);
     return DR_OK;
 }
 
@@ -728,7 +764,7 @@ int dr_init(int device) {
     DR_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
     DR_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     DR_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
-    c->pool.resize(8);
+    c->pool.resize(24);   // more than the launch groups of any batch, so none queue behind another
     for (auto& s : c->pool) DR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     const auto& tab = prime_table(DR_MAX_K);
     std::vector<uint32_t> pinv(DR_MAX_K), r2(DR_MAX_K);
@@ -947,6 +983,29 @@ int dr_batch_read_pipeline(int32_t batch, double* delta, int32_t* topk_idx, doub
         }
     }
     if (signs) DR_CUDA(cudaMemcpy(signs, B->signs.p, 4ull * 4 * n, cudaMemcpyDeviceToHost));
+    return DR_OK;
+}
+
+int dr_batch_profile(int32_t batch, int32_t max_launches, int32_t* n_launches, int32_t* kind,
+                     int32_t* cls, int32_t* m, int32_t* degree, uint32_t* items, float* ms) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    std::vector<float> t;
+    rc = batch_profile(*B, &t);
+    if (rc) return rc;
+    const int n = (int)B->launches.size();
+    if (n_launches) *n_launches = n;
+    for (int i = 0; i < n && i < max_launches; ++i) {
+        const LaunchSpec& L = B->launches[i];
+        if (kind) kind[i] = L.kind;
+        if (cls) cls[i] = (int32_t)L.cls;
+        if (m) m[i] = (int32_t)L.m;
+        if (degree) degree[i] = (int32_t)L.D;
+        if (items) items[i] = L.items;
+        if (ms) ms[i] = t[i];
+    }
     return DR_OK;
 }
 

@@ -70,8 +70,11 @@ __device__ __forceinline__ uint32_t negm(uint32_t a, uint32_t p) { return subm(0
 
 // Montgomery form of a signed 64-bit integer
 __device__ __forceinline__ uint32_t to_mont_i64(int64_t v, const Mont& M) {
-    int64_t r = v % (int64_t)M.p;
-    if (r < 0) r += M.p;
+    const int64_t p = (int64_t)M.p;
+    int64_t r;
+    if (v >= 0 && v < p) r = v;                 // small constants: no 64-bit division
+    else if (v < 0 && v > -p) r = v + p;
+    else { r = v % p; if (r < 0) r += p; }
     return mmul((uint32_t)r, M.r2, M);
 }
 

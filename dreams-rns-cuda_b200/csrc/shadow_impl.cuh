@@ -50,6 +50,35 @@ constexpr int kShadowStateStride = 72;   // m*m <= 64 entries, then mantissa, ex
 // transcendental off the per-step dependency chain.  The result equals the
 // reference's running sum to within its own per-term rounding (~1e-15
 // relative).
+// x / b rounded to nearest for b > 1e10 finite, given y = RN(1/b): Markstein's
+// correction (q0 = RN(x*y), r = x - b*q0 exactly by FMA, q = RN(q0 + r*y) is
+// the correctly rounded quotient when it is a normal number; P. Markstein,
+// IBM J. Res. Dev. 34(1), 1990).  Zero keeps its sign; subnormal quotients
+// take the IEEE division.  One reciprocal serves every entry of a rescale.
+__device__ __forceinline__ double div_by(double x, double b, double y) {
+    if (x == 0.0) return x;
+    const double q0 = __dmul_rn(x, y);
+    const double r = __fma_rn(-q0, b, x);
+    const double q = __fma_rn(r, y, q0);
+    return fabs(q) >= 2.2250738585072014e-308 ? q : __ddiv_rn(x, b);
+}
+
+template <int M_>
+__device__ __forceinline__ void rescale(double (&P)[M_][M_], double mx) {
+    if (isinf(mx)) {
+#pragma unroll
+        for (int i = 0; i < M_; ++i)
+#pragma unroll
+            for (int j = 0; j < M_; ++j) P[i][j] = __ddiv_rn(P[i][j], mx);
+        return;
+    }
+    const double y = __drcp_rn(mx);
+#pragma unroll
+    for (int i = 0; i < M_; ++i)
+#pragma unroll
+        for (int j = 0; j < M_; ++j) P[i][j] = div_by(P[i][j], mx, y);
+}
+
 template <int M_>
 struct FChain {
     double P[M_][M_];
@@ -89,10 +118,7 @@ struct FChain {
 #pragma unroll
             for (int j = 0; j < M_; ++j) P[i][j] = C[i][j];
         if (!has_nan && mx > 1e10) {
-#pragma unroll
-            for (int i = 0; i < M_; ++i)
-#pragma unroll
-                for (int j = 0; j < M_; ++j) P[i][j] = __ddiv_rn(P[i][j], mx);
+            rescale<M_>(P, mx);
             int e;
             sc_m = frexp(__dmul_rn(sc_m, mx), &e);
             sc_e += e;
@@ -103,8 +129,18 @@ struct FChain {
     // the dense product with exact 0/1 entries for finite P)
     __device__ __forceinline__ void step_companion(const double (&c)[M_]) {
         double last[M_];
+        // the shifted columns are known before the new one: their max and NaN
+        // test stay off the dependency chain
         double mx = 0.0;
         bool has_nan = false;
+#pragma unroll
+        for (int i = 0; i < M_; ++i)
+#pragma unroll
+            for (int j = 1; j < M_; ++j) {
+                const double a = fabs(P[i][j]);
+                has_nan |= (a != a);
+                mx = fmax(mx, a);
+            }
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
             double v = __dmul_rn(P[i][0], c[0]);
@@ -112,23 +148,19 @@ struct FChain {
             for (int k = 1; k < M_; ++k) v = __fma_rn(P[i][k], c[k], v);
             last[i] = v;
         }
+        double mn = 0.0;
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
 #pragma unroll
             for (int j = 0; j + 1 < M_; ++j) P[i][j] = P[i][j + 1];
             P[i][M_ - 1] = last[i];
-#pragma unroll
-            for (int j = 0; j < M_; ++j) {
-                const double a = fabs(P[i][j]);
-                has_nan |= (a != a);
-                mx = fmax(mx, a);
-            }
+            const double a = fabs(last[i]);
+            has_nan |= (a != a);
+            mn = fmax(mn, a);
         }
+        mx = fmax(mx, mn);
         if (!has_nan && mx > 1e10) {
-#pragma unroll
-            for (int i = 0; i < M_; ++i)
-#pragma unroll
-                for (int j = 0; j < M_; ++j) P[i][j] = __ddiv_rn(P[i][j], mx);
+            rescale<M_>(P, mx);
             int e;
             sc_m = frexp(__dmul_rn(sc_m, mx), &e);
             sc_e += e;

@@ -87,7 +87,8 @@ __device__ __forceinline__ Mont tile_setup(const WalkArgs& A, const DevTile& T, 
         const int64_t* ax = A.axis + W.axis_off + 4 * a;
         const uint32_t sn = to_mont_i64(__ldg(ax + 0), M), sd = to_mont_i64(__ldg(ax + 1), M);
         const uint32_t tn = to_mont_i64(__ldg(ax + 2), M), td = to_mont_i64(__ldg(ax + 3), M);
-        const uint32_t icd = minv(mmul(sd, td, M), M);
+        // inv(sd*td); the reference skips the inverse when sd*td == 1
+        const uint32_t icd = (__ldg(ax + 1) == 1 && __ldg(ax + 3) == 1) ? M.one : minv(mmul(sd, td, M), M);
         wm.x0[a * 32 + lane] = mmul(mmul(sn, td, M), icd, M);
         wm.dx[a * 32 + lane] = mmul(mmul(tn, sd, M), icd, M);
     }

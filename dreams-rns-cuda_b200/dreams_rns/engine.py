@@ -297,6 +297,20 @@ class WalkBatch:
         return {"prime_steps": ps.value, "tiles": nt.value, "launches": nl.value,
                 "last_ms": ms.value}
 
+    def profile(self) -> List[dict]:
+        """Each launch group run alone and timed (kind 0 walk, 1 interpreted
+        shadow, 2 integer-difference shadow)."""
+        cap = 64
+        n = ctypes.c_int32()
+        arrs = [np.zeros(cap, dtype=np.int32) for _ in range(4)]
+        items = np.zeros(cap, dtype=np.uint32)
+        ms = np.zeros(cap, dtype=np.float32)
+        N.check(N.lib().dr_batch_profile(self.handle, cap, ctypes.byref(n), *[N.ptr(a) for a in arrs],
+                                         N.ptr(items), N.ptr(ms)), "dr_batch_profile")
+        return [{"kind": int(arrs[0][i]), "class": int(arrs[1][i]), "m": int(arrs[2][i]),
+                 "degree": int(arrs[3][i]), "items": int(items[i]), "ms": float(ms[i])}
+                for i in range(min(n.value, cap))]
+
     def close(self) -> None:
         if self.handle:
             N.lib().dr_batch_destroy(self.handle)

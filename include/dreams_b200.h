@@ -162,6 +162,13 @@ int dr_batch_read_pipeline(int32_t batch, double *delta, int32_t *topk_idx, doub
                            uint32_t *limbs, int32_t *signs, int32_t limb_stride);
 int dr_batch_destroy(int32_t batch);
 
+/* Where a batch's time goes: runs every launch group of the batch alone, one
+ * after another, timing each with CUDA events (walk kernels: kind 0; FP64
+ * shadow: kind 1 interpreted, kind 2 integer differences).  No reference
+ * counterpart (the reference has no profiling hooks); used by the autotuner. */
+int dr_batch_profile(int32_t batch, int32_t max_launches, int32_t *n_launches, int32_t *kind,
+                     int32_t *cls, int32_t *m, int32_t *degree, uint32_t *items, float *ms);
+
 /* ---- CRT (reference runner.py:105-129 crt_reconstruct + centered) --------
  * residues[i*K + k] mod moduli[k] for n values.  Outputs the centred value
  * x - M if x > M/2 else x, where x in [0, M) is the reference's CRT result,
