@@ -33,7 +33,7 @@ struct DevProgram {
     uint32_t n_streams;                // derived outputs
     uint32_t zero_reg;                 // compacted register that always holds 0
     uint32_t shadow_fd;                // 1: float shadow may use integer differences
-    uint32_t pad;
+    uint32_t fcomp;                    // 1: float step matrix has the companion shape
 };
 
 // Per-walk record in device memory.
@@ -74,11 +74,26 @@ struct DevGroup {
 };
 
 // Shadow work item: steps [s0, s1) of one walk; state is a resident slot
-// (serving segments) or kNoState (the walk runs from step 0 to its depth).
+// (segments of a longer walk) or kNoState (the walk runs from step 0 to its
+// depth).  Interpreted segments also own a range of the step-matrix buffer
+// (mf_off, in doubles: (s1 - s0) steps of ne entries) and the evaluation
+// items item0 .. item0 + ceil((s1 - s0) / kEvalSteps) - 1.
 struct DevShadowSeg {
     uint32_t walk, state;
     uint64_t s0, s1;
+    uint64_t mf_off;
+    uint32_t item0, pad;
 };
+
+// Steps per evaluation work item of the interpreted shadow.
+constexpr int kEvalSteps = 128;
+
+// Entries of the float step matrix the chain reads per step: the last column
+// when the reference's float evaluation yields exactly the companion shape
+// (sub-diagonal 1.0, other non-last columns 0.0), else all m*m.
+inline uint32_t shadow_entries(uint32_t m, bool float_companion) {
+    return float_companion ? m : m * m;
+}
 
 enum ShadowMode : uint32_t { SHADOW_NONE = 0, SHADOW_INTERP = 1, SHADOW_INTFD = 2 };
 

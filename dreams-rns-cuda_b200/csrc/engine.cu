@@ -199,6 +199,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         d.n_streams = P.n_streams;
         d.zero_reg = P.zero_reg;
         d.shadow_fd = (!P.has_inv && (P.cls == CLS_COMPANION || P.cls == CLS_DENSE)) ? 1u : 0u;
+        d.fcomp = float_companion_shape(P) ? 1u : 0u;
         dprogs[i] = d;
     }
 
@@ -360,32 +361,56 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         if (W.shadow_mode == SHADOW_INTFD)
             shadow_sets[LaunchKey{2, P.cls, P.m, (uint32_t)template_degree(P.cls, P.m, P.degree)}].push_back(w);
         else
-            shadow_sets[LaunchKey{1, 0, G.m, 0}].push_back(w);
+            shadow_sets[LaunchKey{1, G.fcomp, G.m, 0}].push_back(w);
     }
     std::vector<DevShadowSeg> shadow_list;
+    std::vector<uint32_t> eval_items;
+    uint64_t mf_doubles = 0;
+    uint32_t state_slots = 0;
+    const uint64_t cap_doubles =
+        (uint64_t)((tune && tune->shadow_buffer_mb) ? tune->shadow_buffer_mb : 2048) << 17;
+    uint32_t max_dim = 1;
+    for (auto& d : dprogs) max_dim = std::max(max_dim, d.dim);
     for (auto& kv : shadow_sets) {
         auto& v = kv.second;
         std::stable_sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) {
             return dwalks[a].depth > dwalks[b].depth;
         });
+        uint32_t rr = 1;
+        for (uint32_t w : v) {
+            const DevProgram& G = dprogs[dwalks[w].prog];
+            rr = std::max(rr, kv.first.kind == 1 ? G.n_regs : G.dn_regs);
+        }
+        if (kv.first.kind == 1) {
+            // interpreted: the step-matrix buffer holds every step of every
+            // walk when it fits under the cap, else the walks run in rounds
+            const uint32_t ne = shadow_entries(kv.first.m, kv.first.cls != 0);
+            uint64_t need = 0;
+            for (uint32_t w : v) need += dwalks[w].depth * ne;
+            uint64_t round = UINT64_MAX;
+            if (need > cap_doubles) {
+                round = cap_doubles / ((uint64_t)v.size() * ne);
+                round = std::max<uint64_t>(kEvalSteps, round / kEvalSteps * kEvalSteps);
+            }
+            std::vector<DevShadowSeg> segs;
+            for (uint32_t w : v) segs.push_back(DevShadowSeg{w, kNoState, 0, dwalks[w].depth, 0, 0, 0});
+            mf_doubles += shadow_interp_plan(B->launches, shadow_list, eval_items, segs, kv.first.m,
+                                             kv.first.cls != 0, rr, mf_doubles, round, state_slots);
+            if (round != UINT64_MAX) state_slots += (uint32_t)v.size();
+            continue;
+        }
         LaunchSpec L{};
-        L.kind = kv.first.kind;
+        L.kind = 2;
         L.cls = kv.first.cls;
         L.m = kv.first.m;
         L.D = kv.first.D;
         L.off = (uint32_t)shadow_list.size();
         L.count = (uint32_t)v.size();
-        L.items = L.kind == 1 ? L.count : (L.count + 31) / 32;
-        uint32_t rr = 1;
-        for (uint32_t w : v) {
-            const DevProgram& G = dprogs[dwalks[w].prog];
-            rr = std::max(rr, L.kind == 1 ? G.n_regs : G.dn_regs);
-        }
+        L.items = (L.count + 31) / 32;
         L.rows_regs = rr;
-        const uint32_t ns = L.kind == 2 ? (uint32_t)streams_for(L.cls, L.m) : 0;
-        L.rows_per_warp = L.kind == 1 ? rr + kMaxAxes + L.m * L.m
-                                      : rr + kMaxAxes + (L.D + 1) * ns + ns;
-        for (uint32_t w : v) shadow_list.push_back(DevShadowSeg{w, kNoState, 0, dwalks[w].depth});
+        const uint32_t ns = (uint32_t)streams_for(L.cls, L.m);
+        L.rows_per_warp = rr + kMaxAxes + (L.D + 1) * ns + ns;
+        for (uint32_t w : v) shadow_list.push_back(DevShadowSeg{w, kNoState, 0, dwalks[w].depth, 0, 0, 0});
         B->launches.push_back(L);
     }
 
@@ -394,6 +419,11 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     uint32_t q = 0;
     for (LaunchSpec& L : B->launches) {
         L.queue = q++;
+        if (L.kind == 1) {
+            L.queue2 = q++;
+            if ((rc = shadow_interp_geometry(L, max_dim, C.sms))) return rc;
+            continue;
+        }
         L.block = 32 * wpb;
         const size_t word = L.kind == 0 ? 4 : 8;
         L.smem = (size_t)L.rows_per_warp * 32 * word * wpb;
@@ -406,7 +436,6 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         WalkArgs wa{};
         ShadowArgs sa{};
         if (L.kind == 0) e = walk_dispatch(L.cls, L.m, L.D, 0, L.block, L.smem, nullptr, wa, &occ);
-        else if (L.kind == 1) e = shadow_interp_dispatch(L.m, 0, L.block, L.smem, nullptr, sa, &occ);
         else e = shadow_fd_dispatch(L.cls, L.m, L.D, 0, L.block, L.smem, nullptr, sa, &occ);
         if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
         if (occ < 1) {
@@ -430,6 +459,9 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     if ((rc = upload(B->tiles, tiles, st))) return rc;
     if ((rc = upload(B->groups, groups, st))) return rc;
     if ((rc = upload(B->shadow_list, shadow_list, st))) return rc;
+    if ((rc = upload(B->eval_items, eval_items, st))) return rc;
+    DR_CUDA(B->mf.alloc(8ull * std::max<uint64_t>(mf_doubles, 1)));
+    DR_CUDA(B->shadow_state.alloc(8ull * kShadowStateStride * std::max<uint32_t>(state_slots, 1)));
     DR_CUDA(B->group_done.alloc(4ull * std::max<uint32_t>(B->n_groups, 1)));
     DR_CUDA(cudaMemsetAsync(B->group_done.p, 0, B->group_done.bytes, st));
     uint32_t max_m = 1;
@@ -460,6 +492,105 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     DR_CUDA(cudaStreamSynchronize(st));
     *out = std::move(B);
     return DR_OK;
+}
+
+uint64_t shadow_interp_plan(std::vector<LaunchSpec>& launches, std::vector<DevShadowSeg>& list,
+                            std::vector<uint32_t>& eval_items, const std::vector<DevShadowSeg>& segs,
+                            uint32_t m, bool comp, uint32_t rows_regs, uint64_t mf_base,
+                            uint64_t round_steps, uint32_t slot_base) {
+    const uint32_t ne = shadow_entries(m, comp);
+    const bool rounds = round_steps != UINT64_MAX;
+    uint64_t region = 0;
+    for (uint64_t r = 0;; ++r) {
+        LaunchSpec L{};
+        L.kind = 1;
+        L.cls = comp ? 1u : 0u;
+        L.m = m;
+        L.follow = r > 0;
+        L.off = (uint32_t)list.size();
+        L.eoff = (uint32_t)eval_items.size();
+        L.rows_regs = rows_regs;
+        uint64_t off = mf_base;
+        uint32_t idx = 0;
+        for (size_t i = 0; i < segs.size(); ++i) {
+            const DevShadowSeg& g = segs[i];
+            const uint64_t a = rounds ? g.s0 + r * round_steps : g.s0;
+            if (a >= g.s1 && !(r == 0 && g.s0 == g.s1)) continue;
+            const uint64_t b = rounds ? std::min(g.s1, a + round_steps) : g.s1;
+            DevShadowSeg n = g;
+            n.s0 = a;
+            n.s1 = b;
+            n.mf_off = off;
+            n.item0 = (uint32_t)(eval_items.size() - L.eoff);
+            if (rounds) n.state = slot_base + (uint32_t)i;
+            const uint64_t nit = (b - a + kEvalSteps - 1) / kEvalSteps;
+            for (uint64_t k = 0; k < nit; ++k) eval_items.push_back(idx);
+            list.push_back(n);
+            ++idx;
+            off += (b - a) * ne;
+        }
+        if (idx == 0) break;
+        L.count = idx;
+        L.items = (uint32_t)(eval_items.size() - L.eoff);
+        L.items2 = (idx + 31) / 32;
+        launches.push_back(L);
+        region = std::max(region, off - mf_base);
+        if (!rounds) break;
+    }
+    return region;
+}
+
+int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms) {
+    const uint32_t base = L.rows_regs + max_dim + L.m * L.m;
+    uint32_t U = 1;
+    for (uint32_t u : {4u, 2u})
+        if ((size_t)u * base * 32 * 8 <= 16 * 1024) { U = u; break; }
+    L.U = U;
+    L.rows_axes = max_dim;
+    L.rows_per_warp = U * base;
+    const size_t per_warp = (size_t)L.rows_per_warp * 32 * 8;
+    int wpb = 4;
+    while (wpb > 1 && per_warp * wpb > 227 * 1024) wpb /= 2;
+    if (per_warp * wpb > 227 * 1024) {
+        set_error("program needs more shared memory per warp than a block offers");
+        return DR_ERR_UNSUPPORTED;
+    }
+    L.block = 32 * wpb;
+    L.smem = per_warp * wpb;
+    ShadowArgs sa{};
+    int occ = 0;
+    cudaError_t e = shadow_eval_dispatch(U, 0, L.block, L.smem, nullptr, sa, &occ);
+    if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+    if (occ < 1) {
+        set_error("kernel cannot be resident with this shared memory size");
+        return DR_ERR_UNSUPPORTED;
+    }
+    L.grid = std::max(1, std::min((int)((L.items + wpb - 1) / wpb), occ * sms));
+    L.block2 = 32;
+    L.smem2 = shadow_chain_smem(L.m, L.cls != 0);
+    e = shadow_chain_dispatch(L.m, L.cls != 0, 0, L.block2, L.smem2, nullptr, sa, &occ);
+    if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+    if (occ < 1) {
+        set_error("kernel cannot be resident with this shared memory size");
+        return DR_ERR_UNSUPPORTED;
+    }
+    L.grid2 = std::max(1, std::min((int)L.items2, occ * sms));
+    return DR_OK;
+}
+
+cudaError_t launch_shadow_interp(const LaunchSpec& L, ShadowArgs sa, uint32_t* queues,
+                                 const uint32_t* eval_items, cudaStream_t s) {
+    sa.eval_items = eval_items + L.eoff;
+    sa.n_items = L.items;
+    sa.queue = queues + L.queue;
+    sa.rows_axes = L.rows_axes;
+    if (L.items) {
+        cudaError_t e = shadow_eval_dispatch(L.U, L.grid, L.block, L.smem, s, sa, nullptr);
+        if (e != cudaSuccess) return e;
+    }
+    sa.n_items = L.items2;
+    sa.queue = queues + L.queue2;
+    return shadow_chain_dispatch(L.m, L.cls != 0, L.grid2, L.block2, L.smem2, s, sa, nullptr);
 }
 
 static CrtTables tables_of(const CrtSet& S);
@@ -558,7 +689,8 @@ static void batch_args(Batch& B, WalkArgs& wa, ShadowArgs& sa) {
     sa.shadow = B.shadow.as<double>();
     sa.n_walks = B.n_walks;
     sa.status = wa.status;
-    sa.state = nullptr;
+    sa.state = B.shadow_state.as<double>();
+    sa.mf = B.mf.as<double>();
 }
 
 static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, ShadowArgs& sa, cudaStream_t s) {
@@ -573,13 +705,15 @@ static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, Shado
         return walk_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, wa, nullptr);
     }
     sa.segs = B.shadow_list.as<DevShadowSeg>() + L.off;
-    sa.n_items = L.items;
     sa.n_list = L.count;
-    sa.queue = B.queues.as<uint32_t>() + L.queue;
     sa.rows_regs = L.rows_regs;
     sa.rows_per_warp = L.rows_per_warp;
-    return L.kind == 1 ? shadow_interp_dispatch(L.m, L.grid, L.block, L.smem, s, sa, nullptr)
-                       : shadow_fd_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, sa, nullptr);
+    if (L.kind == 2) {
+        sa.n_items = L.items;
+        sa.queue = B.queues.as<uint32_t>() + L.queue;
+        return shadow_fd_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, sa, nullptr);
+    }
+    return launch_shadow_interp(L, sa, B.queues.as<uint32_t>(), B.eval_items.as<uint32_t>(), s);
 }
 
 // One run of a batch: zero the work counters and status words, then every
@@ -595,12 +729,17 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
     DR_CUDA(cudaEventRecord(B.fork, st));
     const size_t np = C.pool.size();
     size_t used = 0;
+    cudaStream_t prev = nullptr;
     for (int pass = 0; pass < 2; ++pass) {
         for (const LaunchSpec& L : B.launches) {
-            if (L.items == 0 || (pass == 0) != (L.kind != 0)) continue;
-            cudaStream_t s = C.pool[used % np];
-            if (used < np) DR_CUDA(cudaStreamWaitEvent(s, B.fork, 0));
-            ++used;
+            if ((L.items == 0 && L.items2 == 0) || (pass == 0) != (L.kind != 0)) continue;
+            cudaStream_t s = prev;
+            if (!L.follow || !prev) {
+                s = C.pool[used % np];
+                if (used < np) DR_CUDA(cudaStreamWaitEvent(s, B.fork, 0));
+                ++used;
+            }
+            prev = s;
             cudaError_t e = launch_one(B, L, wa, sa, s);
             if (e != cudaSuccess) {
                 // rejoin what was forked so a capture can end cleanly
@@ -622,7 +761,7 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
 
 // Every launch group alone, one after another on one stream, timed with
 // events: where a batch's time goes (used by the autotuner and diagnostics).
-int batch_profile(Batch& B, std::vector<float>* ms) {
+int batch_profile(Batch& B, std::vector<float>* ms, std::vector<float>* ms2) {
     Context& C = *g_ctx;
     cudaStream_t st = C.stream;
     WalkArgs wa;
@@ -630,19 +769,46 @@ int batch_profile(Batch& B, std::vector<float>* ms) {
     batch_args(B, wa, sa);
     DR_CUDA(cudaMemsetAsync(B.queues.p, 0, B.queues.bytes, st));
     DR_CUDA(cudaMemsetAsync(B.status.p, 0, B.status.bytes, st));
-    std::vector<cudaEvent_t> ev(B.launches.size() + 1);
+    const size_t n = B.launches.size();
+    std::vector<cudaEvent_t> ev(2 * n + 1);
     for (auto& e : ev) DR_CUDA(cudaEventCreate(&e));
     DR_CUDA(cudaEventRecord(ev[0], st));
-    for (size_t i = 0; i < B.launches.size(); ++i) {
-        if (B.launches[i].items) {
-            cudaError_t e = launch_one(B, B.launches[i], wa, sa, st);
-            if (e != cudaSuccess) return cuda_fail(e, "profile launch");
+    for (size_t i = 0; i < n; ++i) {
+        const LaunchSpec& L = B.launches[i];
+        cudaError_t e = cudaSuccess;
+        if (L.kind == 1) {
+            // the evaluation and the chain timed apart
+            sa.segs = B.shadow_list.as<DevShadowSeg>() + L.off;
+            sa.n_list = L.count;
+            sa.rows_regs = L.rows_regs;
+            sa.rows_per_warp = L.rows_per_warp;
+            sa.rows_axes = L.rows_axes;
+            sa.eval_items = B.eval_items.as<uint32_t>() + L.eoff;
+            if (L.items) {
+                sa.n_items = L.items;
+                sa.queue = B.queues.as<uint32_t>() + L.queue;
+                e = shadow_eval_dispatch(L.U, L.grid, L.block, L.smem, st, sa, nullptr);
+            }
+            if (e == cudaSuccess) e = cudaEventRecord(ev[2 * i + 1], st);
+            if (e == cudaSuccess) {
+                sa.n_items = L.items2;
+                sa.queue = B.queues.as<uint32_t>() + L.queue2;
+                e = shadow_chain_dispatch(L.m, L.cls != 0, L.grid2, L.block2, L.smem2, st, sa, nullptr);
+            }
+        } else {
+            if (L.items) e = launch_one(B, L, wa, sa, st);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[2 * i + 1], st);
         }
-        DR_CUDA(cudaEventRecord(ev[i + 1], st));
+        if (e != cudaSuccess) return cuda_fail(e, "profile launch");
+        DR_CUDA(cudaEventRecord(ev[2 * i + 2], st));
     }
     DR_CUDA(cudaStreamSynchronize(st));
-    ms->assign(B.launches.size(), 0.f);
-    for (size_t i = 0; i < B.launches.size(); ++i) cudaEventElapsedTime(&(*ms)[i], ev[i], ev[i + 1]);
+    ms->assign(n, 0.f);
+    ms2->assign(n, 0.f);
+    for (size_t i = 0; i < n; ++i) {
+        cudaEventElapsedTime(&(*ms)[i], ev[2 * i], ev[2 * i + 1]);
+        cudaEventElapsedTime(&(*ms2)[i], ev[2 * i + 1], ev[2 * i + 2]);
+    }
     for (auto& e : ev) cudaEventDestroy(e);
     return DR_OK;
 }
@@ -851,7 +1017,7 @@ int dr_batch_stats(int32_t batch, uint64_t* prime_steps, uint32_t* n_tiles, uint
     if (n_tiles) *n_tiles = B->n_tiles;
     if (n_launches) {
         uint32_t k = 0;
-        for (auto& L : B->launches) k += L.items > 0;
+        for (auto& L : B->launches) k += (L.items > 0) + (L.kind == 1 && L.items2 > 0);
         *n_launches = k;
     }
     if (last_ms) {
@@ -987,13 +1153,14 @@ int dr_batch_read_pipeline(int32_t batch, double* delta, int32_t* topk_idx, doub
 }
 
 int dr_batch_profile(int32_t batch, int32_t max_launches, int32_t* n_launches, int32_t* kind,
-                     int32_t* cls, int32_t* m, int32_t* degree, uint32_t* items, float* ms) {
+                     int32_t* cls, int32_t* m, int32_t* degree, uint32_t* items, float* ms,
+                     float* ms2) {
     int rc = ensure_ctx();
     if (rc) return rc;
     Batch* B = find_batch(batch);
     if (!B) return DR_ERR_HANDLE;
-    std::vector<float> t;
-    rc = batch_profile(*B, &t);
+    std::vector<float> t, t2;
+    rc = batch_profile(*B, &t, &t2);
     if (rc) return rc;
     const int n = (int)B->launches.size();
     if (n_launches) *n_launches = n;
@@ -1005,6 +1172,7 @@ int dr_batch_profile(int32_t batch, int32_t max_launches, int32_t* n_launches, i
         if (degree) degree[i] = (int32_t)L.D;
         if (items) items[i] = L.items;
         if (ms) ms[i] = t[i];
+        if (ms2) ms2[i] = t2[i];
     }
     return DR_OK;
 }

@@ -68,14 +68,36 @@ int crt_limbs_for(int K);  // L: limbs of prod(moduli) + 1
 
 struct LaunchSpec {
     int kind;                  // 0 walk, 1 shadow (interpreted), 2 shadow (integer differences)
-    uint32_t cls, m, D;
+    uint32_t cls, m, D;        // kind 1: cls = 1 when the float matrix has the companion shape
     uint32_t off, count;       // tiles / list entries of this launch
-    uint32_t items;            // work items (tiles, walks or 32-walk groups)
+    uint32_t items;            // work items (tiles, evaluation items or 32-walk groups)
     uint32_t queue;            // queue counter index
     uint32_t rows_regs, rows_consts, rows_stage, rows_per_warp;
     size_t smem;
     int grid, block;
+    // kind 1: the evaluation launch above is followed by the chain launch
+    uint32_t U = 1, rows_axes = 0, eoff = 0;   // sub-blocks, axis rows, first evaluation item
+    uint32_t items2 = 0, queue2 = 0;
+    size_t smem2 = 0;
+    int grid2 = 0, block2 = 0;
+    bool follow = false;       // runs on the stream of the previous launch (shadow rounds)
 };
+
+// Interpreted-shadow launch geometry shared by batches and serving waves:
+// picks U and the per-warp rows of the evaluation kernel, the chain kernel's
+// shared memory, and both grids.  Returns DR_OK or an error status.
+int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms);
+
+// Builds the interpreted-shadow launches of one (m, companion-shape) group:
+// segs (sorted longest first) become one launch, or several rounds of at most
+// `round_steps` steps with resident state slots from slot_base (round_steps =
+// UINT64_MAX: one launch, the segments' own state slots).  Appends to list and
+// eval_items and returns the doubles of step-matrix buffer the group needs
+// (its segments' mf_off start at mf_base).
+uint64_t shadow_interp_plan(std::vector<LaunchSpec>& launches, std::vector<DevShadowSeg>& list,
+                            std::vector<uint32_t>& eval_items, const std::vector<DevShadowSeg>& segs,
+                            uint32_t m, bool comp, uint32_t rows_regs, uint64_t mf_base,
+                            uint64_t round_steps, uint32_t slot_base);
 
 struct Batch {
     int32_t id = 0;
@@ -87,6 +109,7 @@ struct Batch {
     uint32_t chunk_stride = 0;   // words per chunk-product slot
     DevBuf progs, code, consts, walks, axis, tiles, groups, group_done, chunkP, chunkSig;
     DevBuf shadow_list, queues, res, shadow, status;   // res: p residues then q residues
+    DevBuf mf, eval_items, shadow_state;               // interpreted shadow
     // device pipeline (CRT -> delta -> top-k)
     dr_pipeline pipe{};
     bool pipe_on = false;
@@ -117,5 +140,11 @@ int batch_read(Batch& B, uint32_t* p_res, uint32_t* q_res, uint64_t n_res, doubl
                uint32_t* status);
 
 int cuda_fail(cudaError_t e, const char* where);
+
+struct ShadowArgs;
+// Evaluation then chain launch of one interpreted-shadow launch group on s;
+// sa carries the batch-wide pointers and this launch's segs / rows.
+cudaError_t launch_shadow_interp(const LaunchSpec& L, ShadowArgs sa, uint32_t* queues,
+                                 const uint32_t* eval_items, cudaStream_t s);
 
 }  // namespace dr

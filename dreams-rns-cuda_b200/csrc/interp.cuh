@@ -70,39 +70,82 @@ __device__ __forceinline__ double cube_rn(double x) {
     return __dadd_rn(p1, __fma_rn(e, x, e1));
 }
 
-// Float64 interpreter (reference runner.py:311-364, cmf_walk.py:261-313).
-// rf is a [register][32] double array; axv holds the axis values of each
-// lane's step.  No contraction: every operation is an explicit IEEE op.
+// Float64 interpreter (reference runner.py:311-364, cmf_walk.py:261-313),
+// U sub-blocks of 32 steps at once: every decoded instruction is applied to
+// U independent values per lane, so the shared-memory round trips of one
+// sub-block overlap those of the others.  Register r of sub-block u for this
+// lane lives at rf[(r*U + u)*32 + lane]; axv and out use the same layout.
+// The next instruction is fetched while the current one executes.  No
+// contraction: every operation is an explicit IEEE op.
+template <int U>
 __device__ __forceinline__ void interp_f64(const uint4* __restrict__ code, uint32_t n,
                                            double* __restrict__ rf,
                                            const int64_t* __restrict__ consts,
-                                           const double* __restrict__ axv, double step,
+                                           const double* __restrict__ axv, int64_t s_lane,
                                            double* __restrict__ out, int lane) {
+    if (n == 0) return;
+    uint4 nx = __ldg(code);
 #pragma unroll 1
     for (uint32_t pc = 0; pc < n; ++pc) {
-        const uint4 in = __ldg(code + pc);
+        const uint4 in = nx;
+        if (pc + 1 < n) nx = __ldg(code + pc + 1);
+#define R_(r, u) rf[((r) * U + (u)) * 32 + lane]
         switch (in.x) {
-            case OP_LOAD_X: rf[in.z * 32 + lane] = axv[in.y * 32 + lane]; break;
-            case OP_LOAD_C: rf[in.z * 32 + lane] = __ll2double_rn(__ldg(consts + in.y)); break;
-            case OP_LOAD_N: rf[in.y * 32 + lane] = step; break;
-            case OP_ADD: rf[in.w * 32 + lane] = __dadd_rn(rf[in.y * 32 + lane], rf[in.z * 32 + lane]); break;
-            case OP_SUB: rf[in.w * 32 + lane] = __dsub_rn(rf[in.y * 32 + lane], rf[in.z * 32 + lane]); break;
-            case OP_MUL: rf[in.w * 32 + lane] = __dmul_rn(rf[in.y * 32 + lane], rf[in.z * 32 + lane]); break;
-            case OP_NEG: rf[in.z * 32 + lane] = -rf[in.y * 32 + lane]; break;
-            case OP_POW2: {
-                const double v = rf[in.y * 32 + lane];
-                rf[in.z * 32 + lane] = __dmul_rn(v, v);
+            case OP_LOAD_X:
+#pragma unroll
+                for (int u = 0; u < U; ++u) R_(in.z, u) = axv[(in.y * U + u) * 32 + lane];
+                break;
+            case OP_LOAD_C: {
+                const double c = __ll2double_rn(__ldg(consts + in.y));
+#pragma unroll
+                for (int u = 0; u < U; ++u) R_(in.z, u) = c;
                 break;
             }
-            case OP_POW3: rf[in.z * 32 + lane] = cube_rn(rf[in.y * 32 + lane]); break;
-            case OP_INV: {
-                const double v = rf[in.y * 32 + lane];
-                rf[in.z * 32 + lane] = fabs(v) > 1e-300 ? __ddiv_rn(1.0, v) : 0.0;
+            case OP_LOAD_N:
+#pragma unroll
+                for (int u = 0; u < U; ++u) R_(in.y, u) = __ll2double_rn(s_lane + 32 * u);
                 break;
-            }
-            case OP_STORE: out[in.z * 32 + lane] = rf[in.y * 32 + lane]; break;
+            case OP_ADD:
+#pragma unroll
+                for (int u = 0; u < U; ++u) R_(in.w, u) = __dadd_rn(R_(in.y, u), R_(in.z, u));
+                break;
+            case OP_SUB:
+#pragma unroll
+                for (int u = 0; u < U; ++u) R_(in.w, u) = __dsub_rn(R_(in.y, u), R_(in.z, u));
+                break;
+            case OP_MUL:
+#pragma unroll
+                for (int u = 0; u < U; ++u) R_(in.w, u) = __dmul_rn(R_(in.y, u), R_(in.z, u));
+                break;
+            case OP_NEG:
+#pragma unroll
+                for (int u = 0; u < U; ++u) R_(in.z, u) = -R_(in.y, u);
+                break;
+            case OP_POW2:
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double v = R_(in.y, u);
+                    R_(in.z, u) = __dmul_rn(v, v);
+                }
+                break;
+            case OP_POW3:
+#pragma unroll
+                for (int u = 0; u < U; ++u) R_(in.z, u) = cube_rn(R_(in.y, u));
+                break;
+            case OP_INV:
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double v = R_(in.y, u);
+                    R_(in.z, u) = fabs(v) > 1e-300 ? __ddiv_rn(1.0, v) : 0.0;
+                }
+                break;
+            case OP_STORE:
+#pragma unroll
+                for (int u = 0; u < U; ++u) out[(in.z * U + u) * 32 + lane] = R_(in.y, u);
+                break;
             default: break;
         }
+#undef R_
     }
 }
 

@@ -51,8 +51,12 @@ int topk_tile_size();
 // occ != nullptr: only report resident blocks per SM for (block, smem).
 cudaError_t walk_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block, size_t smem,
                           cudaStream_t st, const WalkArgs& a, int* occ);
-cudaError_t shadow_interp_dispatch(uint32_t m, int grid, int block, size_t smem, cudaStream_t st,
-                                   const ShadowArgs& a, int* occ);
+// interpreted shadow: evaluation (U sub-blocks per pass) and chain kernels
+cudaError_t shadow_eval_dispatch(uint32_t U, int grid, int block, size_t smem, cudaStream_t st,
+                                 const ShadowArgs& a, int* occ);
+cudaError_t shadow_chain_dispatch(uint32_t m, bool comp, int grid, int block, size_t smem,
+                                  cudaStream_t st, const ShadowArgs& a, int* occ);
+size_t shadow_chain_smem(uint32_t m, bool comp);
 cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block,
                                size_t smem, cudaStream_t st, const ShadowArgs& a, int* occ);
 

@@ -563,4 +563,40 @@ double float_bound_log2(const Plan& plan, const int64_t* axis, uint64_t depth) {
     return worst > 0 ? std::log2(worst) : -1.0;
 }
 
+bool float_companion_shape(const Plan& p) {
+    const uint32_t m = p.m;
+    if (m < 2) return false;
+    // per register: holds a LOAD_C constant (value), or anything else
+    std::vector<uint8_t> is_c(p.n_regs + 1, 0);
+    std::vector<int64_t> cv(p.n_regs + 1, 0);
+    if (p.zero_reg != 0xffffffffu && p.zero_reg < is_c.size()) is_c[p.zero_reg] = 1;
+    std::vector<uint8_t> e_c(m * m, 1);      // never stored: 0.0
+    std::vector<int64_t> e_v(m * m, 0);
+    auto set = [&](uint32_t r, bool c, int64_t v) {
+        if (r < is_c.size()) { is_c[r] = c; cv[r] = v; }
+    };
+    for (const Insn& in : p.ops) {
+        switch (in.op) {
+            case OP_LOAD_C: set(in.b, in.a < p.consts.size(), in.a < p.consts.size() ? p.consts[in.a] : 0); break;
+            case OP_LOAD_N: set(in.a, false, 0); break;
+            case OP_LOAD_X: case OP_NEG: case OP_POW2: case OP_POW3: case OP_INV: set(in.b, false, 0); break;
+            case OP_ADD: case OP_SUB: case OP_MUL: set(in.c, false, 0); break;
+            case OP_STORE:
+                if (in.b < m * m) {
+                    const bool c = in.a < is_c.size() && is_c[in.a];
+                    e_c[in.b] = c;
+                    e_v[in.b] = c ? cv[in.a] : 0;
+                }
+                break;
+            default: break;
+        }
+    }
+    for (uint32_t i = 0; i < m; ++i)
+        for (uint32_t j = 0; j + 1 < m; ++j) {
+            const uint32_t k = i * m + j;
+            if (!e_c[k] || e_v[k] != (i == j + 1 ? 1 : 0)) return false;
+        }
+    return true;
+}
+
 }  // namespace dr

@@ -42,6 +42,12 @@ struct Plan {
 int parse_blob(const uint8_t* blob, uint64_t size, RawProgram* out, std::string* err);
 int plan_program(const RawProgram& raw, Plan* out, std::string* err);
 
+// True when the reference's float evaluation of the (compacted) program gives
+// every non-last-column entry as an exact constant of the companion shape
+// (1.0 on the sub-diagonal, 0.0 elsewhere): the entries are stored straight
+// from LOAD_C of that constant (or never stored, which leaves 0.0).
+bool float_companion_shape(const Plan& plan);
+
 // log2 of a bound on |value| of every register the reference float evaluator
 // produces for steps [0, depth) with integer axes (sd = td = 1); +inf when the
 // program has INV or the bound is not finite.

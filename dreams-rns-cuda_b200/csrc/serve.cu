@@ -69,7 +69,7 @@ struct Wave {
     std::vector<uint64_t> res_off;        // output offsets of finishing walks
     std::vector<uint32_t> widx;           // walk-table index per request
     DevBuf progs, code, consts, walks, axis, tiles, groups, done_ctr, chunkP, chunkSig, segs,
-        queues, res, shadow, status;
+        queues, res, shadow, status, mf, eval_items;
     uint32_t* h_res = nullptr;            // pinned outputs
     double* h_sh = nullptr;
     uint32_t* h_st = nullptr;
@@ -130,7 +130,6 @@ int occupancy(Server& S, int kind, uint32_t cls, uint32_t m, uint32_t D, int blo
     ShadowArgs sa{};
     cudaError_t e;
     if (kind == 0) e = walk_dispatch(cls, m, D, 0, block, smem, nullptr, wa, &occ);
-    else if (kind == 1) e = shadow_interp_dispatch(m, 0, block, smem, nullptr, sa, &occ);
     else e = shadow_fd_dispatch(cls, m, D, 0, block, smem, nullptr, sa, &occ);
     if (e != cudaSuccess) occ = 0;
     S.occ_cache[key] = occ;
@@ -143,7 +142,20 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     Context& C = *ctx();
     const uint32_t chunk = S.cfg.chunk_steps ? S.cfg.chunk_steps : 4096;
     const uint64_t seg_walk = (uint64_t)chunk * 16;
-    const uint64_t seg_shadow = 8192;
+    // interpreted shadow segments: at most 8192 steps, fewer when the wave's
+    // step-matrix buffer would pass 1 GiB
+    uint64_t n_interp = 0, ne_max = 1;
+    for (Req* r : sel)
+        if (r->shadow_mode == SHADOW_INTERP && !r->shadow_done) {
+            ++n_interp;
+            ne_max = std::max<uint64_t>(ne_max, shadow_entries(r->plan->m, float_companion_shape(*r->plan)));
+        }
+    uint64_t seg_shadow = 8192;
+    if (n_interp) {
+        const uint64_t cap = (1ull << 30) / 8;
+        seg_shadow = std::min<uint64_t>(
+            8192, std::max<uint64_t>(kEvalSteps, cap / (n_interp * ne_max) / kEvalSteps * kEvalSteps));
+    }
     std::map<std::string, int> pidx;
     std::vector<DevProgram> progs;
     std::vector<uint4> code;
@@ -177,6 +189,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
             d.c_off = (uint32_t)consts.size(); d.n_consts = (uint32_t)P.consts.size();
             consts.insert(consts.end(), P.consts.begin(), P.consts.end());
             d.n_streams = P.n_streams; d.zero_reg = P.zero_reg;
+            d.fcomp = float_companion_shape(P) ? 1u : 0u;
             pi = (int)progs.size();
             progs.push_back(d);
             pidx.emplace(r->blob, pi);
@@ -232,11 +245,11 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
         if (r->shadow_mode != SHADOW_NONE && !r->shadow_done) {
             se = std::min<uint64_t>(r->d.depth, r->shadow_next + seg_shadow);
             sfinal = se >= r->d.depth;
-            DevShadowSeg g{wi, (uint32_t)r->shadow_slot, r->shadow_next, se};
+            DevShadowSeg g{wi, (uint32_t)r->shadow_slot, r->shadow_next, se, 0, 0, 0};
             if (r->shadow_mode == SHADOW_INTFD)
                 ssets[std::make_tuple(2, (uint32_t)P.cls, P.m, (uint32_t)r->tdeg)].push_back(g);
             else
-                ssets[std::make_tuple(1, 0u, P.m, 0u)].push_back(g);
+                ssets[std::make_tuple(1, progs[pi].fcomp, P.m, 0u)].push_back(g);
         }
         W.shadow_end.push_back(se);
         W.shadow_final.push_back(sfinal);
@@ -269,28 +282,48 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
         tiles.insert(tiles.end(), v.begin(), v.end());
         L.push_back(s);
     }
+    std::vector<uint32_t> eval_items;
+    uint64_t mf_doubles = 0;
+    uint32_t max_dim = 1;
+    for (auto& d : progs) max_dim = std::max(max_dim, d.dim);
     for (auto& kv : ssets) {
         auto& v = kv.second;
-        LaunchSpec s{};
         int kind;
-        std::tie(kind, s.cls, s.m, s.D) = kv.first;
-        s.kind = kind;
-        s.off = (uint32_t)segs.size(); s.count = (uint32_t)v.size();
-        s.items = kind == 1 ? s.count : (s.count + 31) / 32;
+        uint32_t cls, m, D;
+        std::tie(kind, cls, m, D) = kv.first;
         uint32_t rr = 1;
         for (auto& g : v) {
             const DevProgram& G = progs[walks[g.walk].prog];
             rr = std::max(rr, kind == 1 ? G.n_regs : G.dn_regs);
         }
-        const uint32_t ns = kind == 2 ? (uint32_t)streams_for(s.cls, s.m) : 0;
+        if (kind == 1) {
+            std::stable_sort(v.begin(), v.end(), [](const DevShadowSeg& x, const DevShadowSeg& y) {
+                return (x.s1 - x.s0) > (y.s1 - y.s0);
+            });
+            mf_doubles += shadow_interp_plan(L, segs, eval_items, v, m, cls != 0, rr, mf_doubles,
+                                             UINT64_MAX, 0);
+            continue;
+        }
+        LaunchSpec s{};
+        s.kind = kind;
+        s.cls = cls; s.m = m; s.D = D;
+        s.off = (uint32_t)segs.size(); s.count = (uint32_t)v.size();
+        s.items = (s.count + 31) / 32;
+        const uint32_t ns = (uint32_t)streams_for(s.cls, s.m);
         s.rows_regs = rr;
-        s.rows_per_warp = kind == 1 ? rr + kMaxAxes + s.m * s.m : rr + kMaxAxes + (s.D + 1) * ns + ns;
+        s.rows_per_warp = rr + kMaxAxes + (s.D + 1) * ns + ns;
         segs.insert(segs.end(), v.begin(), v.end());
         L.push_back(s);
     }
     uint32_t q = 0;
     for (auto& s : L) {
         s.queue = q++;
+        if (s.kind == 1) {
+            s.queue2 = q++;
+            const int rc = shadow_interp_geometry(s, max_dim, C.sms);
+            if (rc) return rc;
+            continue;
+        }
         s.block = 32 * wpb;
         s.smem = (size_t)s.rows_per_warp * 32 * (s.kind == 0 ? 4 : 8) * wpb;
         const int occ = occupancy(S, s.kind, s.cls, s.m, s.D, s.block, s.smem);
@@ -308,6 +341,8 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     SV(put(W.tiles, tiles, st));
     SV(put(W.groups, groups, st));
     SV(put(W.segs, segs, st));
+    SV(put(W.eval_items, eval_items, st));
+    SV(W.mf.alloc(8ull * std::max<uint64_t>(mf_doubles, 1)));
     SV(W.done_ctr.alloc(4ull * std::max<size_t>(groups.size(), 1)));
     SV(cudaMemsetAsync(W.done_ctr.p, 0, 4ull * std::max<size_t>(groups.size(), 1), st));
     SV(W.chunkP.alloc(4ull * std::max<uint32_t>(slots, 1) * kServeStride));
@@ -330,8 +365,9 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     sa.progs = wa.progs; sa.code = wa.code; sa.consts = wa.consts; sa.walks = wa.walks; sa.axis = wa.axis;
     sa.shadow = W.shadow.as<double>(); sa.n_walks = W.n_walks; sa.status = wa.status;
     sa.state = S.stShadow.as<double>();
+    sa.mf = W.mf.as<double>();
     for (auto& s : L) {
-        if (s.items == 0) continue;
+        if (s.items == 0 && s.items2 == 0) continue;
         if (s.kind == 0) {
             wa.tiles = W.tiles.as<DevTile>() + s.off; wa.n_tiles = s.count;
             wa.queue = W.queues.as<uint32_t>() + s.queue;
@@ -342,7 +378,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
             sa.segs = W.segs.as<DevShadowSeg>() + s.off; sa.n_items = s.items; sa.n_list = s.count;
             sa.queue = W.queues.as<uint32_t>() + s.queue; sa.rows_regs = s.rows_regs;
             sa.rows_per_warp = s.rows_per_warp;
-            if (s.kind == 1) SV(shadow_interp_dispatch(s.m, s.grid, s.block, s.smem, st, sa, nullptr));
+            if (s.kind == 1) SV(launch_shadow_interp(s, sa, W.queues.as<uint32_t>(), W.eval_items.as<uint32_t>(), st));
             else SV(shadow_fd_dispatch(s.cls, s.m, s.D, s.grid, s.block, s.smem, st, sa, nullptr));
         }
     }

@@ -5,15 +5,31 @@
 
 namespace dr {
 
-cudaError_t shadow_interp_dispatch(uint32_t m, int grid, int block, size_t smem, cudaStream_t st,
-                                   const ShadowArgs& a, int* occ) {
-    switch (m) {
+cudaError_t shadow_eval_dispatch(uint32_t U, int grid, int block, size_t smem, cudaStream_t st,
+                                 const ShadowArgs& a, int* occ) {
+    switch (U) {
+        case 1: return run_kernel(k_shadow_eval<1>, grid, block, smem, st, a, occ);
+        case 2: return run_kernel(k_shadow_eval<2>, grid, block, smem, st, a, occ);
+        case 4: return run_kernel(k_shadow_eval<4>, grid, block, smem, st, a, occ);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t shadow_chain_dispatch(uint32_t m, bool comp, int grid, int block, size_t smem,
+                                  cudaStream_t st, const ShadowArgs& a, int* occ) {
+    switch (m * 2 + (comp ? 1 : 0)) {
 #define DR_X(M_, D_) \
-    case M_: return run_kernel(k_shadow_interp<M_>, grid, block, smem, st, a, occ);
+    case M_ * 2: return run_kernel(k_shadow_chain<M_, false>, grid, block, smem, st, a, occ); \
+    case M_ * 2 + 1: return run_kernel(k_shadow_chain<M_, true>, grid, block, smem, st, a, occ);
         DR_INTERP_INSTANCES(DR_X)
 #undef DR_X
         default: return cudaErrorInvalidValue;
     }
+}
+
+size_t shadow_chain_smem(uint32_t m, bool comp) {
+    const int ne = (int)shadow_entries(m, comp);
+    return 2ull * chain_chunk_steps(ne) * ne * 32 * sizeof(double);
 }
 
 cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block,
@@ -40,3 +56,34 @@ cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, i
 }
 
 }  // namespace dr
+
+namespace dr {
+
+// Test hook: the shadow's rescale division, one quotient per thread.
+__global__ void k_debug_rescale(const double* x, const double* b, int n, double* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double P[1][1] = {{x[i]}};
+    rescale<1>(P, b[i]);
+    out[i] = P[0][0];
+}
+
+}  // namespace dr
+
+extern "C" int dr_debug_rescale(const double* x, const double* b, int32_t n, double* out) {
+    using namespace dr;
+    if (n < 0 || (n > 0 && (!x || !b || !out))) return DR_ERR_ARG;
+    if (n == 0) return DR_OK;
+    double* d = nullptr;
+    const size_t bytes = 8ull * n;
+    if (cudaMalloc(&d, 3 * bytes) != cudaSuccess) return DR_ERR_NOMEM;
+    cudaError_t e = cudaMemcpy(d, x, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d + n, b, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_debug_rescale<<<(n + 255) / 256, 256>>>(d, d + n, n, d + 2 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 2 * n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? DR_OK : DR_ERR_CUDA;
+}

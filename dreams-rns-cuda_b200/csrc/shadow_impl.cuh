@@ -7,14 +7,25 @@
 // and is reproduced with explicit IEEE intrinsics (no contraction).
 //
 // Two modes:
-//   interpreted  one warp per walk; lane j evaluates M_f(s0 + j) for 32 steps
-//                with the float interpreter, then all lanes run the 32-step
-//                chain (redundantly, so nothing diverges).
+//   interpreted  two kernels.  k_shadow_eval evaluates M_f(s) for every step of
+//                every segment in parallel (work items of kEvalSteps steps,
+//                lane = step, the float interpreter on U sub-blocks at once)
+//                and stores the entries the chain needs (the last column when
+//                the float matrix has the companion shape, else all m*m) in a
+//                step-matrix buffer.  k_shadow_chain then runs the sequential
+//                recurrence with lane = segment, 32 segments per warp, streaming
+//                its steps' entries through shared memory with cp.async double
+//                buffering, so the serial chain never waits on the interpreter.
 //   integer      lane = walk, 32 walks per warp: when the host has bounded every
 //                intermediate of the reference's float evaluation below 2^53
 //                (no INV, integer axes) all those floats are exact integers, so
 //                M_f(s) equals the exact integer entries, which advance by
 //                int64 forward differences.  Bit-identical to the reference.
+//
+// Per step the chain's critical path is the product, the max-abs test and,
+// when it fires, one correctly rounded reciprocal plus a three-operation
+// correction per entry; the max / NaN / threshold tests run on the integer
+// pipe so the FP64 pipe only carries the arithmetic.
 #pragma once
 #include <stdint.h>
 
@@ -31,8 +42,11 @@ struct ShadowArgs {
     const DevWalk* walks;
     const int64_t* axis;
     const DevShadowSeg* segs;   // segments of this launch
-    uint32_t n_items;           // interpreted: segments; integer: groups of 32 segments
+    uint32_t n_items;           // evaluation items, or groups of 32 segments (chain, integer)
     uint32_t n_list;            // segments
+    double* mf;                 // step-matrix buffer of the interpreted mode
+    const uint32_t* eval_items; // segment (index into segs) of every evaluation item
+    uint32_t rows_axes;         // evaluation: axis rows per sub-block
     uint32_t* queue;
     double* shadow;             // [3*w] final, [3*(n_walks + w)] checkpoint
     uint32_t n_walks;
@@ -46,37 +60,80 @@ constexpr int kShadowStateStride = 72;   // m*m <= 64 entries, then mantissa, ex
 
 // log_scale = sum of ln(max) over the rescale points.  The logarithm is taken
 // once at the end: the product of the maxima is carried as mantissa * 2^exp
-// (frexp after every rescale, so it cannot overflow), which keeps the
+// (renormalised by its exponent bits after every rescale, so it cannot overflow), which keeps the
 // transcendental off the per-step dependency chain.  The result equals the
 // reference's running sum to within its own per-term rounding (~1e-15
 // relative).
-// x / b rounded to nearest for b > 1e10 finite, given y = RN(1/b): Markstein's
-// correction (q0 = RN(x*y), r = x - b*q0 exactly by FMA, q = RN(q0 + r*y) is
-// the correctly rounded quotient when it is a normal number; P. Markstein,
-// IBM J. Res. Dev. 34(1), 1990).  Zero keeps its sign; subnormal quotients
-// take the IEEE division.  One reciprocal serves every entry of a rescale.
-__device__ __forceinline__ double div_by(double x, double b, double y) {
-    if (x == 0.0) return x;
-    const double q0 = __dmul_rn(x, y);
-    const double r = __fma_rn(-q0, b, x);
-    const double q = __fma_rn(r, y, q0);
-    return fabs(q) >= 2.2250738585072014e-308 ? q : __ddiv_rn(x, b);
-}
+// IEEE division for the rare entries outside the Markstein domain; not
+// inlined so that the common path never pays for it.
+static __device__ __noinline__ double div_slow(double x, double b) { return __ddiv_rn(x, b); }
 
+// |x| as an unsigned bit pattern: for non-NaN doubles these order exactly as
+// the magnitudes do (+inf = 0x7ff0...0 is the largest), and every NaN lies
+// above +inf.  With M the largest |bits| of the matrix, the reference's
+// max(|P|) is NaN iff M > kInfBits, and max(|P|) > 1e10 iff M > kBigBits.
+constexpr unsigned long long kInfBits = 0x7ff0000000000000ULL;
+constexpr unsigned long long kBigBits = 0x4202a05f20000000ULL;   // 1e10
+__device__ __forceinline__ unsigned long long absbits(double x) {
+    return (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffULL;
+}
+__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) {
+    return a > b ? a : b;
+}
+__device__ __forceinline__ bool is_zero(double x) {
+    return ((__double2hiint(x) & 0x7fffffff) | __double2loint(x)) == 0;
+}
+// Biased exponent field of x (0 for zeros and subnormals).
+__device__ __forceinline__ int bexp(double x) { return (__double2hiint(x) >> 20) & 0x7ff; }
+
+// P /= mx entrywise, each quotient rounded to nearest.  The Markstein path
+// (y = RN(1/mx); q0 = RN(x*y); r = x - mx*q0 by FMA; q = RN(q0 + r*y);
+// P. Markstein, IBM J. Res. Dev. 34(1), 1990) is exact when y, q and the
+// residual r are normal numbers: r is exact when |x| >= 2^-969 (biased
+// exponent >= 54, so |r| ~ 2^-52 |x| stays normal), q is normal when
+// ex - em >= -1021 (|x/mx| > 2^(ex - em - 1)), y is normal when mx < 2^1022.
+// Entries outside these ranges (and an infinite mx) take the IEEE division.
+// A zero keeps its sign.  The test depends only on the inputs, so its
+// branch resolves while the reciprocal is in flight.
 template <int M_>
 __device__ __forceinline__ void rescale(double (&P)[M_][M_], double mx) {
-    if (isinf(mx)) {
+    const int em = bexp(mx);
+    bool slow = em >= 2045;
+#pragma unroll
+    for (int i = 0; i < M_; ++i)
+#pragma unroll
+        for (int j = 0; j < M_; ++j) {
+            const int ex = bexp(P[i][j]);
+            slow |= !is_zero(P[i][j]) & ((ex < 60) | (ex - em < -1020));
+        }
+    if (__builtin_expect(slow, 0)) {
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
-            for (int j = 0; j < M_; ++j) P[i][j] = __ddiv_rn(P[i][j], mx);
+            for (int j = 0; j < M_; ++j) P[i][j] = div_slow(P[i][j], mx);
         return;
     }
     const double y = __drcp_rn(mx);
 #pragma unroll
     for (int i = 0; i < M_; ++i)
 #pragma unroll
-        for (int j = 0; j < M_; ++j) P[i][j] = div_by(P[i][j], mx, y);
+        for (int j = 0; j < M_; ++j) {
+            const double x = P[i][j];
+            const double q0 = __dmul_rn(x, y);
+            const double r = __fma_rn(-q0, mx, x);
+            const double q = __fma_rn(r, y, q0);
+            P[i][j] = is_zero(x) ? x : q;
+        }
+}
+
+// sc_m * 2^sc_e *= mx with sc_m kept in [0.5, 1) (frexp by exponent bits: the
+// product of sc_m >= 0.5 and mx > 1e10 is a normal number or infinite).
+__device__ __forceinline__ void scale_acc(double& sc_m, int& sc_e, double mx) {
+    const double p = __dmul_rn(sc_m, mx);
+    const int hi = __double2hiint(p);
+    const bool inf = (hi & 0x7ff00000) == 0x7ff00000;
+    sc_e += inf ? 0 : ((hi >> 20) & 0x7ff) - 1022;
+    sc_m = inf ? p : __hiloint2double((hi & 0x800fffff) | 0x3fe00000, __double2loint(p));
 }
 
 template <int M_>
@@ -99,8 +156,7 @@ struct FChain {
     // P <- P @ X with numpy's rounding, then the max-abs rescale
     __device__ __forceinline__ void step(const double (&X)[M_][M_]) {
         double C[M_][M_];
-        double mx = 0.0;
-        bool has_nan = false;
+        unsigned long long mb = 0;
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
@@ -109,38 +165,40 @@ struct FChain {
 #pragma unroll
                 for (int k = 1; k < M_; ++k) c = __fma_rn(P[i][k], X[k][j], c);
                 C[i][j] = c;
-                const double a = fabs(c);
-                has_nan |= (a != a);
-                mx = fmax(mx, a);
+                mb = umax64(mb, absbits(c));
             }
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
             for (int j = 0; j < M_; ++j) P[i][j] = C[i][j];
-        if (!has_nan && mx > 1e10) {
+        const bool has_nan = mb > kInfBits;
+        if (!has_nan && mb > kBigBits) {
+            const double mx = __longlong_as_double((long long)mb);
             rescale<M_>(P, mx);
-            int e;
-            sc_m = frexp(__dmul_rn(sc_m, mx), &e);
-            sc_e += e;
+            scale_acc(sc_m, sc_e, mx);
         }
         nan_seen |= has_nan;
     }
-    // companion step: columns shift left, last column = P @ c (same rounding as
-    // the dense product with exact 0/1 entries for finite P)
+    // companion step: columns shift left, last column = P @ c.  The dense
+    // product with exact 0/1 entries gives the shifted entry itself when it is
+    // nonzero, and for a zero the sum of the signed zeros P[i][k]*0, which is
+    // -0 only when every P[i][k] has its sign bit set; the last column is the
+    // dense product's own FMA chain.
     __device__ __forceinline__ void step_companion(const double (&c)[M_]) {
         double last[M_];
-        // the shifted columns are known before the new one: their max and NaN
-        // test stay off the dependency chain
-        double mx = 0.0;
-        bool has_nan = false;
+        // the shifted columns are known before the new one: their max and
+        // signed-zero fix stay off the dependency chain
+        unsigned long long ms = 0;
+        bool allneg[M_];
 #pragma unroll
-        for (int i = 0; i < M_; ++i)
+        for (int i = 0; i < M_; ++i) {
+            bool neg = true;
 #pragma unroll
-            for (int j = 1; j < M_; ++j) {
-                const double a = fabs(P[i][j]);
-                has_nan |= (a != a);
-                mx = fmax(mx, a);
-            }
+            for (int k = 0; k < M_; ++k) neg &= (__double2hiint(P[i][k]) < 0);
+            allneg[i] = neg;
+#pragma unroll
+            for (int j = 1; j < M_; ++j) ms = umax64(ms, absbits(P[i][j]));
+        }
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
             double v = __dmul_rn(P[i][0], c[0]);
@@ -148,22 +206,22 @@ struct FChain {
             for (int k = 1; k < M_; ++k) v = __fma_rn(P[i][k], c[k], v);
             last[i] = v;
         }
-        double mn = 0.0;
+        unsigned long long mb = ms;
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
 #pragma unroll
-            for (int j = 0; j + 1 < M_; ++j) P[i][j] = P[i][j + 1];
+            for (int j = 0; j + 1 < M_; ++j) {
+                const double v = P[i][j + 1];
+                P[i][j] = is_zero(v) ? (allneg[i] ? -0.0 : 0.0) : v;
+            }
             P[i][M_ - 1] = last[i];
-            const double a = fabs(last[i]);
-            has_nan |= (a != a);
-            mn = fmax(mn, a);
+            mb = umax64(mb, absbits(last[i]));
         }
-        mx = fmax(mx, mn);
-        if (!has_nan && mx > 1e10) {
+        const bool has_nan = mb > kInfBits;
+        if (!has_nan && mb > kBigBits) {
+            const double mx = __longlong_as_double((long long)mb);
             rescale<M_>(P, mx);
-            int e;
-            sc_m = frexp(__dmul_rn(sc_m, mx), &e);
-            sc_e += e;
+            scale_acc(sc_m, sc_e, mx);
         }
         nan_seen |= has_nan;
     }
@@ -215,51 +273,181 @@ struct FChain {
 // the host guarantees these integers fit in int64 for the whole walk.
 __device__ __forceinline__ double axis_f64(const int64_t* ax, int64_t s) {
     const int64_t k = ax[0] * ax[3] + s * ax[2] * ax[1];
-    return __ddiv_rn(__ll2double_rn(k), __ll2double_rn(ax[1] * ax[3]));
+    const int64_t d = ax[1] * ax[3];
+    return d == 1 ? __ll2double_rn(k) : __ddiv_rn(__ll2double_rn(k), __ll2double_rn(d));
 }
 
-template <int M_>
-__global__ void __launch_bounds__(128) k_shadow_interp(const ShadowArgs A) {
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Steps per staged chunk of the chain kernel (entries * steps = 64 doubles
+// per lane and buffer, at least two steps).
+__host__ __device__ constexpr int chain_chunk_steps(int ne) { return ne >= 32 ? 2 : 64 / ne; }
+
+// Evaluation: each warp takes items of kEvalSteps steps of one segment and
+// runs the float interpreter on U sub-blocks of 32 steps at a time.  The
+// per-warp shared memory holds the register file, the axis values and the
+// m*m outputs, each as [row][U][32] doubles; every lane touches only its own
+// column, so no warp synchronisation is needed.
+template <int U>
+__global__ void __launch_bounds__(128) k_shadow_eval(const ShadowArgs A) {
     extern __shared__ double dsm[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    double* base = dsm + (size_t)warp * A.rows_per_warp * 32;
-    double* rf = base;
-    double* axv = rf + A.rows_regs * 32;
-    double* mf = axv + kMaxAxes * 32;   // [entry][32 steps]
+    double* rf = dsm + (size_t)warp * A.rows_per_warp * 32;
+    double* axv = rf + (size_t)A.rows_regs * U * 32;
+    double* outv = axv + (size_t)A.rows_axes * U * 32;
     for (;;) {
         uint32_t it = 0;
         if (lane == 0) it = atomicAdd(A.queue, 1u);
         it = __shfl_sync(0xffffffffu, it, 0);
         if (it >= A.n_items) break;
-        const DevShadowSeg g = A.segs[it];
-        const uint32_t w = g.walk;
-        const DevWalk W = A.walks[w];
+        const DevShadowSeg g = A.segs[A.eval_items[it]];
+        const DevWalk W = A.walks[g.walk];
         const DevProgram G = A.progs[W.prog];
+        const int64_t* ax = A.axis + W.axis_off;
+        const uint32_t m = G.m;
+        const bool comp = G.fcomp != 0;
+        const uint32_t ne = comp ? m : m * m;
+        if (G.zero_reg != 0xffffffffu)
+#pragma unroll
+            for (int u = 0; u < U; ++u) rf[(G.zero_reg * U + u) * 32 + lane] = 0.0;
+        for (uint32_t e = 0; e < m * m; ++e)
+#pragma unroll
+            for (int u = 0; u < U; ++u) outv[(e * U + u) * 32 + lane] = 0.0;
+        const uint64_t len = g.s1 - g.s0;
+        const uint64_t t_item = (uint64_t)(it - g.item0) * kEvalSteps;
+        double* dst = A.mf + g.mf_off;
+        for (int pass = 0; pass < kEvalSteps / (32 * U); ++pass) {
+            const uint64_t t0 = t_item + (uint64_t)pass * 32 * U;
+            if (t0 >= len) break;
+            const int64_t s_lane = (int64_t)(g.s0 + t0) + lane;
+            for (uint32_t a = 0; a < G.dim; ++a)
+#pragma unroll
+                for (int u = 0; u < U; ++u) axv[(a * U + u) * 32 + lane] = axis_f64(ax + 4 * a, s_lane + 32 * u);
+            interp_f64<U>(A.code + G.op_off, G.n_ops, rf, A.consts + G.c_off, axv, s_lane, outv, lane);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint64_t t = t0 + 32 * u + lane;
+                if (t < len) {
+                    double* d = dst + t * ne;
+                    for (uint32_t e = 0; e < ne; ++e) {
+                        const uint32_t slot = comp ? e * m + m - 1 : e;
+                        d[e] = outv[(slot * U + u) * 32 + lane];
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int M_, bool COMP>
+__device__ __forceinline__ void chain_step(FChain<M_>& ch, const double (&X)[COMP ? M_ : M_ * M_]) {
+    if (COMP) {
+        double cv[M_];
+#pragma unroll
+        for (int i = 0; i < M_; ++i) cv[i] = X[i];
+        ch.step_companion(cv);
+    } else {
+        double Xm[M_][M_];
+#pragma unroll
+        for (int e = 0; e < M_ * M_; ++e) Xm[e / M_][e % M_] = X[e];
+        ch.step(Xm);
+    }
+}
+
+// Chain: lane = segment, 32 segments per warp (one warp per block).  The
+// warp's entries for the next chunk of steps are copied into shared memory
+// ([buffer][step][entry][lane]) while the current chunk runs; every lane only
+// reads what it copied itself, so the per-thread cp.async group wait is the
+// only synchronisation.
+template <int M_, bool COMP>
+__global__ void __launch_bounds__(32) k_shadow_chain(const ShadowArgs A) {
+    constexpr int NE = COMP ? M_ : M_ * M_;
+    constexpr int CS = chain_chunk_steps(NE);
+    extern __shared__ double dsm[];
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        uint32_t it = 0;
+        if (lane == 0) it = atomicAdd(A.queue, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= A.n_items) break;
+        const uint32_t first = it * 32;
+        const uint32_t count = min(32u, A.n_list - first);
+        const bool active = (uint32_t)lane < count;
+        const DevShadowSeg g = A.segs[first + (active ? lane : 0)];
+        const DevWalk W = A.walks[g.walk];
         FChain<M_> ch;
         ch.begin(W, g, A.state);
-        const int64_t* ax = A.axis + W.axis_off;
-        if (G.zero_reg != 0xffffffffu) rf[G.zero_reg * 32 + lane] = 0.0;
-        for (uint64_t s0 = g.s0; s0 < g.s1; s0 += 32) {
-            const int64_t s = (int64_t)(s0 + lane);
-            for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = axis_f64(ax + 4 * a, s);
-            for (int e = 0; e < M_ * M_; ++e) mf[e * 32 + lane] = 0.0;
-            __syncwarp();
-            interp_f64(A.code + G.op_off, G.n_ops, rf, A.consts + G.c_off, axv, (double)s, mf, lane);
-            __syncwarp();
-            const uint32_t n = (uint32_t)min((uint64_t)32, g.s1 - s0);
-            for (uint32_t j = 0; j < n; ++j) {
-                double X[M_][M_];
+        const uint64_t len = active ? g.s1 - g.s0 : 0;
+        const double* src = A.mf + g.mf_off;
+        unsigned long long mlen = len;
+        // chunks every lane runs in full, and the chunk holding any lane's
+        // checkpoint, are warp-uniform facts: full chunks without a
+        // checkpoint run without per-step tests
+        unsigned long long minlen = active ? len : ~0ull;
 #pragma unroll
-                for (int e = 0; e < M_ * M_; ++e) X[e / M_][e % M_] = mf[e * 32 + j];
-                ch.step(X);
-                if (W.checkpoint && s0 + j + 1 == W.checkpoint && lane == 0)
-                    ch.write(A.shadow + 3 * ((size_t)A.n_walks + w), W);
-            }
-            __syncwarp();
+        for (int o = 16; o > 0; o >>= 1) {
+            mlen = max(mlen, __shfl_xor_sync(0xffffffffu, mlen, o));
+            minlen = min(minlen, __shfl_xor_sync(0xffffffffu, minlen, o));
         }
-        if (lane == 0) ch.end(W, g, A.state, A.shadow, A.status, w);
-        __syncwarp();
+        const uint64_t cp_rel = (active && W.checkpoint > g.s0 && W.checkpoint <= g.s1)
+                                    ? W.checkpoint - g.s0 - 1 : ~0ull;
+        const uint64_t nch = (mlen + CS - 1) / CS;
+        auto issue = [&](uint64_t c) {
+            double* buf = dsm + (size_t)(c & 1) * CS * NE * 32;
+#pragma unroll 1
+            for (int t = 0; t < CS; ++t) {
+                const uint64_t rel = c * CS + t;
+                if (rel < len)
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) cp_async8(buf + (t * NE + e) * 32 + lane, src + rel * NE + e);
+            }
+        };
+        if (nch) issue(0);
+        cp_async_commit();
+        for (uint64_t c = 0; c < nch; ++c) {
+            if (c + 1 < nch) issue(c + 1);
+            cp_async_commit();
+            cp_async_wait<1>();
+            const double* buf = dsm + (size_t)(c & 1) * CS * NE * 32;
+            const uint64_t base = c * CS;
+            const bool cp_here = __any_sync(0xffffffffu, cp_rel >= base && cp_rel < base + CS);
+            if (base + CS <= minlen && !cp_here) {
+                double X[NE];
+#pragma unroll
+                for (int e = 0; e < NE; ++e) X[e] = buf[e * 32 + lane];
+#pragma unroll 2
+                for (int t = 0; t < CS; ++t) {
+                    double Y[NE];
+                    const int tn = t + 1 < CS ? t + 1 : t;
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) Y[e] = buf[(tn * NE + e) * 32 + lane];
+                    chain_step<M_, COMP>(ch, X);
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) X[e] = Y[e];
+                }
+            } else {
+#pragma unroll 1
+                for (int t = 0; t < CS; ++t) {
+                    const uint64_t rel = base + t;
+                    if (rel < len) {
+                        double X[NE];
+#pragma unroll
+                        for (int e = 0; e < NE; ++e) X[e] = buf[(t * NE + e) * 32 + lane];
+                        chain_step<M_, COMP>(ch, X);
+                        if (rel == cp_rel) ch.write(A.shadow + 3 * ((size_t)A.n_walks + g.walk), W);
+                    }
+                }
+            }
+        }
+        cp_async_wait<0>();
+        if (active) ch.end(W, g, A.state, A.shadow, A.status, g.walk);
     }
 }
 

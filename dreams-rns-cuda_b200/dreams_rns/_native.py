@@ -68,7 +68,7 @@ assert WALK_DTYPE.itemsize == ctypes.sizeof(WalkDesc)
 
 class Tune(ctypes.Structure):
     _fields_ = [("chunk_steps", ctypes.c_uint32), ("warps_per_block", ctypes.c_uint32),
-                ("engine", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("engine", ctypes.c_uint32), ("shadow_buffer_mb", ctypes.c_uint32)]
 
 
 class Pipeline(ctypes.Structure):
@@ -118,7 +118,7 @@ _SIGNATURES = {
     "dr_batch_stats": (ctypes.c_int, [_I32, _P, _P, _P, _P]),
     "dr_batch_destroy": (ctypes.c_int, [_I32]),
     "dr_batch_set_pipeline": (ctypes.c_int, [_I32, _P]),
-    "dr_batch_profile": (ctypes.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P]),
+    "dr_batch_profile": (ctypes.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "dr_batch_read_pipeline": (ctypes.c_int, [_I32, _P, _P, _P, _P, _P, _I32]),
     "dr_crt_batch": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P]),
     "dr_crt_batch_device": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P]),
@@ -132,6 +132,7 @@ _SIGNATURES = {
     "dr_serve_stats": (ctypes.c_int, [_I32, _P, _P, _P, _P]),
     "dr_serve_close": (ctypes.c_int, [_I32]),
     "dr_bench_int_peak": (ctypes.c_int, [_I32, _P]),
+    "dr_debug_rescale": (ctypes.c_int, [_P, _P, _I32, _P]),
     "dr_debug_sim_walk": (ctypes.c_int, [ctypes.c_char_p, _U64, _I32, _U64, _U64, _P, _I32, _I64,
                                          _U32, _U64, _I32, _P, _P, _P, _P]),
 }

@@ -150,11 +150,12 @@ class _Packed:
         self.n = n
 
 
-def _tune(chunk_steps=0, engine=N.DR_ENGINE_AUTO, warps_per_block=0):
+def _tune(chunk_steps=0, engine=N.DR_ENGINE_AUTO, warps_per_block=0, shadow_buffer_mb=0):
     t = N.Tune()
     t.chunk_steps = chunk_steps
     t.engine = engine
     t.warps_per_block = warps_per_block
+    t.shadow_buffer_mb = shadow_buffer_mb
     return t
 
 
@@ -180,7 +181,7 @@ def _unpack(pk: _Packed, reqs, p, q, sh, st):
 
 
 def run_walks(reqs: Sequence[WalkRequest], chunk_steps: int = 0,
-              engine: int = N.DR_ENGINE_AUTO) -> List[dict]:
+              engine: int = N.DR_ENGINE_AUTO, shadow_buffer_mb: int = 0) -> List[dict]:
     """Run every request in one engine call; one result dict per request."""
     N.init()
     reqs = list(reqs)
@@ -191,7 +192,7 @@ def run_walks(reqs: Sequence[WalkRequest], chunk_steps: int = 0,
     q = np.zeros(pk.n_res, dtype=np.uint32)
     sh = np.zeros(6 * pk.n, dtype=np.float64)
     st = np.zeros(pk.n, dtype=np.uint32)
-    t = _tune(chunk_steps, engine)
+    t = _tune(chunk_steps, engine, 0, shadow_buffer_mb)
     N.check(N.lib().dr_walk_batch(N.ptr(pk.desc), pk.n, N.ptr(pk.blobs), N.ptr(pk.offsets),
                                   pk.n_programs, N.ptr(pk.axis), pk.n_axis, ctypes.byref(t),
                                   N.ptr(p), N.ptr(q), pk.n_res, N.ptr(sh), N.ptr(st)),
@@ -203,11 +204,11 @@ class WalkBatch:
     """A batch of walks prepared once and resident on the device."""
 
     def __init__(self, reqs: Sequence[WalkRequest], chunk_steps: int = 0,
-                 engine: int = N.DR_ENGINE_AUTO, warps_per_block: int = 0):
+                 engine: int = N.DR_ENGINE_AUTO, warps_per_block: int = 0, shadow_buffer_mb: int = 0):
         N.init()
         self.reqs = list(reqs)
         self.pk = _Packed(self.reqs)
-        t = _tune(chunk_steps, engine, warps_per_block)
+        t = _tune(chunk_steps, engine, warps_per_block, shadow_buffer_mb)
         h = ctypes.c_int32(0)
         N.check(N.lib().dr_batch_create(N.ptr(self.pk.desc), self.pk.n, N.ptr(self.pk.blobs),
                                         N.ptr(self.pk.offsets), self.pk.n_programs,
@@ -305,11 +306,12 @@ class WalkBatch:
         arrs = [np.zeros(cap, dtype=np.int32) for _ in range(4)]
         items = np.zeros(cap, dtype=np.uint32)
         ms = np.zeros(cap, dtype=np.float32)
+        ms2 = np.zeros(cap, dtype=np.float32)
         N.check(N.lib().dr_batch_profile(self.handle, cap, ctypes.byref(n), *[N.ptr(a) for a in arrs],
-                                         N.ptr(items), N.ptr(ms)), "dr_batch_profile")
+                                         N.ptr(items), N.ptr(ms), N.ptr(ms2)), "dr_batch_profile")
         return [{"kind": int(arrs[0][i]), "class": int(arrs[1][i]), "m": int(arrs[2][i]),
-                 "degree": int(arrs[3][i]), "items": int(items[i]), "ms": float(ms[i])}
-                for i in range(min(n.value, cap))]
+                 "degree": int(arrs[3][i]), "items": int(items[i]), "ms": float(ms[i]),
+                 "ms2": float(ms2[i])} for i in range(min(n.value, cap))]
 
     def close(self) -> None:
         if self.handle:

@@ -89,7 +89,10 @@ typedef struct dr_tune {
     uint32_t chunk_steps;     /* depth-chunk length; 0 = autotuned           */
     uint32_t warps_per_block; /* 0 = default                                  */
     uint32_t engine;          /* DR_ENGINE_*                                  */
-    uint32_t reserved;
+    uint32_t shadow_buffer_mb;/* cap of the interpreted shadow's step-matrix
+                                 buffer per launch group; 0 = default
+                                 (2048); walks beyond it run their shadow in
+                                 rounds with resident state                 */
 } dr_tune;
 
 /* ---- context ---------------------------------------------------------- */
@@ -164,10 +167,12 @@ int dr_batch_destroy(int32_t batch);
 
 /* Where a batch's time goes: runs every launch group of the batch alone, one
  * after another, timing each with CUDA events (walk kernels: kind 0; FP64
- * shadow: kind 1 interpreted, kind 2 integer differences).  No reference
- * counterpart (the reference has no profiling hooks); used by the autotuner. */
+ * shadow: kind 1 interpreted, kind 2 integer differences).  ms: the launch
+ * (kind 1: its step-matrix evaluation), ms2: kind 1's chain kernel.  No
+ * reference counterpart (the reference has no profiling hooks). */
 int dr_batch_profile(int32_t batch, int32_t max_launches, int32_t *n_launches, int32_t *kind,
-                     int32_t *cls, int32_t *m, int32_t *degree, uint32_t *items, float *ms);
+                     int32_t *cls, int32_t *m, int32_t *degree, uint32_t *items, float *ms,
+                     float *ms2);
 
 /* ---- CRT (reference runner.py:105-129 crt_reconstruct + centered) --------
  * residues[i*K + k] mod moduli[k] for n values.  Outputs the centred value

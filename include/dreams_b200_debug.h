@@ -31,6 +31,11 @@ int dr_debug_template_degree(int32_t cls, int32_t m, int32_t degree);
  * denominator of the walk kernels' roofline. */
 int dr_bench_int_peak(int32_t kind, double *lane_ops_per_s);
 
+/* The FP64 shadow's rescale division on the device: out[i] = x[i] / b[i]
+ * rounded to nearest through the same code path the shadow kernels use
+ * (Markstein correction, IEEE fallback).  Host buffers; b[i] > 1e10. */
+int dr_debug_rescale(const double *x, const double *b, int32_t n, double *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -183,6 +183,59 @@ def test_shadow_vs_oracle():
         assert _close(r["log_scale"], o["log_scale"], 1e-13)
 
 
+def test_shadow_rounds_match_single_pass():
+    """A small step-matrix buffer splits the interpreted shadow into rounds
+    with resident state; results (checkpoints included) must not change."""
+    rng = random.Random(5)
+    reqs = []
+    for trial in range(40):
+        a = dr.synth.poly_str([rng.randrange(-9, 10) for _ in range(3)])
+        b = dr.synth.poly_str([rng.randrange(-9, 10) for _ in range(5)])
+        if trial % 2:
+            b = f"({b})/({dr.synth.poly_str([rng.randrange(1, 9), rng.randrange(-3, 4)])})"
+        depth = rng.randrange(1, 6000)
+        cp = rng.randrange(1, depth) if depth > 2 and trial % 3 == 0 else 0
+        reqs.append(pcf_request(dr.compile_pcf(a, b), dr.pcf_initial_values(a), depth, 32, checkpoint=cp))
+    one = run_walks(reqs)
+    rounds = run_walks(reqs, shadow_buffer_mb=1)
+    for req, x, y in zip(reqs, one, rounds):
+        for k in ("p_float", "q_float", "log_scale"):
+            assert x[k] == y[k] or (math.isnan(x[k]) and math.isnan(y[k])), k
+        if req.checkpoint:
+            for k in ("p_float", "q_float", "log_scale"):
+                assert x["checkpoint"][k] == y["checkpoint"][k], k
+        o = walk_c.pcf_walk(req.blob, req.a0, req.depth, 32)
+        assert _close(x["p_float"], o["p_float"]) and _close(x["q_float"], o["q_float"])
+
+
+def test_rescale_division_is_correctly_rounded():
+    """The shadow's rescale division (reciprocal + Markstein correction, IEEE
+    fallback outside its domain) must equal IEEE x / b bit for bit."""
+    import ctypes
+    rng = np.random.default_rng(17)
+    n = 1 << 20
+    b = 10.0 ** rng.uniform(10.0, 300.0, n)
+    x = b * rng.uniform(-1.0, 1.0, n)
+    # edges: zeros of both signs, tiny and subnormal numerators, huge and
+    # power-of-two divisors, all-ones mantissas, |x| == b
+    k = 4096
+    x[:k] = np.concatenate([[0.0, -0.0, 5e-324, -5e-324, 2.2250738585072014e-308, 1e-300, 1e-290,
+                             2.0 ** -969, 2.0 ** -970, np.nextafter(2.0 ** -968, 0)],
+                            rng.uniform(-1, 1, k - 10) * 10.0 ** rng.uniform(-320, 0, k - 10)])
+    b[:k] = 10.0 ** rng.uniform(10, 308, k)
+    b[k:2 * k] = 2.0 ** rng.integers(34, 1023, k).astype(np.float64)
+    b[2 * k:3 * k] = np.nextafter(2.0 ** rng.integers(34, 1024, k).astype(np.float64), 0)
+    b[3 * k:3 * k + 16] = [1.7976931348623157e308, 2.0 ** 1022, np.nextafter(2.0 ** 1022, 0),
+                           np.nextafter(2.0 ** 1022, np.inf)] * 4
+    x[3 * k:4 * k] = b[3 * k:4 * k] * rng.choice([-1.0, 1.0], k)
+    out = np.zeros(n)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    N.check(N.lib().dr_debug_rescale(p(x), p(b), n, p(out)), "dr_debug_rescale")
+    want = x / b
+    same = (out.view(np.uint64) == want.view(np.uint64))
+    assert same.all(), (x[~same][:4], b[~same][:4], out[~same][:4], want[~same][:4])
+
+
 def test_prepared_batch_replay():
     ws = dr.synth.uniform_pcfs(64, seed=9, depth=500, limit_depth=1200)
     reqs = [pcf_request(dr.compile_pcf(w.a, w.b), w.a0, w.depth, 32, checkpoint=w.checkpoint)
