@@ -97,6 +97,26 @@ inline uint32_t shadow_entries(uint32_t m, bool float_companion) {
 
 enum ShadowMode : uint32_t { SHADOW_NONE = 0, SHADOW_INTERP = 1, SHADOW_INTFD = 2 };
 
+// Diagnostics: when a launch carries a timestamp pair, the first instruction
+// of every block lowers [0] and the last raises [1] to the global timer (ns),
+// so a concurrent run shows when each kernel actually held the GPU.
+#ifdef __CUDACC__
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void stamp_begin(unsigned long long* ts) {
+    if (ts && threadIdx.x == 0) atomicMin(ts, (unsigned long long)global_ns());
+}
+__device__ __forceinline__ void stamp_end(unsigned long long* ts) {
+    if (ts) {
+        __syncthreads();
+        if (threadIdx.x == 0) atomicMax(ts + 1, (unsigned long long)global_ns());
+    }
+}
+#endif
+
 constexpr int kMaxM = 8;
 constexpr int kMaxAxes = 8;
 constexpr int kMaxDegree = 16;

@@ -421,7 +421,26 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         L.queue = q++;
         if (L.kind == 1) {
             L.queue2 = q++;
-            if ((rc = shadow_interp_geometry(L, max_dim, C.sms))) return rc;
+            if ((rc = shadow_interp_geometry(L, max_dim, C.sms, shadow_list.data() + L.off))) return rc;
+            continue;
+        }
+        if (L.kind == 2) {
+            const size_t per_warp = (size_t)L.rows_per_warp * 32 * 8;
+            L.block = 32 * kChainWarps;
+            L.smem = std::max(per_warp * kChainWarps, chain_hog_smem());
+            if (per_warp * kChainWarps > L.smem) {
+                set_error("program needs more shared memory per warp than a block offers");
+                return DR_ERR_UNSUPPORTED;
+            }
+            int occ = 0;
+            ShadowArgs sa{};
+            cudaError_t e = shadow_fd_dispatch(L.cls, L.m, L.D, 0, L.block, L.smem, nullptr, sa, &occ);
+            if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+            if (occ < 1) {
+                set_error("kernel cannot be resident with this shared memory size");
+                return DR_ERR_UNSUPPORTED;
+            }
+            L.grid = std::min(chain_blocks(shadow_list.data() + L.off, L.count), occ * C.sms);
             continue;
         }
         L.block = 32 * wpb;
@@ -487,7 +506,10 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     DR_CUDA(cudaEventCreate(&B->ev1));
     DR_CUDA(cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming));
     DR_CUDA(cudaEventCreateWithFlags(&B->join, cudaEventDisableTiming));
-    B->joins.resize(C.pool.size());
+    B->joins.resize(C.pool.size() + C.hpool.size());
+    B->evals.assign(B->launches.size(), nullptr);
+    for (size_t i = 0; i < B->launches.size(); ++i)
+        if (B->launches[i].kind == 1) DR_CUDA(cudaEventCreateWithFlags(&B->evals[i], cudaEventDisableTiming));
     for (auto& e : B->joins) DR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     DR_CUDA(cudaStreamSynchronize(st));
     *out = std::move(B);
@@ -540,7 +562,35 @@ uint64_t shadow_interp_plan(std::vector<LaunchSpec>& launches, std::vector<DevSh
     return region;
 }
 
-int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms) {
+size_t chain_hog_smem() {
+    static size_t bytes = 0;
+    if (!bytes) {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || v <= 0)
+            v = 96 * 1024;
+        bytes = (size_t)v;
+    }
+    return bytes;
+}
+
+int chain_blocks(const DevShadowSeg* segs, uint32_t count) {
+    // segments are sorted longest first; a warp takes 32 of them, so item k
+    // lasts as long as segment 32k.  Enough warps that the total chain work
+    // spread over them ends with the longest chain, plus one block of slack.
+    uint64_t total = 0, longest = 0;
+    for (uint32_t k = 0; k < count; k += 32) {
+        const uint64_t len = segs[k].s1 - segs[k].s0;
+        total += std::max<uint64_t>(len, 1);
+        longest = std::max<uint64_t>(longest, std::max<uint64_t>(len, 1));
+    }
+    const uint32_t items = (count + 31) / 32;
+    const uint64_t warps = longest ? (total + longest - 1) / longest : 1;
+    const uint64_t blocks = (warps + kChainWarps - 1) / kChainWarps + 1;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (items + kChainWarps - 1) / kChainWarps));
+}
+
+int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs) {
     const uint32_t base = L.rows_regs + max_dim + L.m * L.m;
     uint32_t U = 1;
     for (uint32_t u : {4u, 2u})
@@ -566,20 +616,20 @@ int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms) {
         return DR_ERR_UNSUPPORTED;
     }
     L.grid = std::max(1, std::min((int)((L.items + wpb - 1) / wpb), occ * sms));
-    L.block2 = 32;
-    L.smem2 = shadow_chain_smem(L.m, L.cls != 0);
+    L.block2 = 32 * kChainWarps;
+    L.smem2 = std::max(shadow_chain_smem(L.m, L.cls != 0) * kChainWarps, chain_hog_smem());
     e = shadow_chain_dispatch(L.m, L.cls != 0, 0, L.block2, L.smem2, nullptr, sa, &occ);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
     if (occ < 1) {
         set_error("kernel cannot be resident with this shared memory size");
         return DR_ERR_UNSUPPORTED;
     }
-    L.grid2 = std::max(1, std::min((int)L.items2, occ * sms));
+    L.grid2 = std::min(chain_blocks(segs, L.count), occ * sms);
     return DR_OK;
 }
 
 cudaError_t launch_shadow_interp(const LaunchSpec& L, ShadowArgs sa, uint32_t* queues,
-                                 const uint32_t* eval_items, cudaStream_t s) {
+                                 const uint32_t* eval_items, cudaStream_t s, cudaEvent_t evaluated) {
     sa.eval_items = eval_items + L.eoff;
     sa.n_items = L.items;
     sa.queue = queues + L.queue;
@@ -588,8 +638,13 @@ cudaError_t launch_shadow_interp(const LaunchSpec& L, ShadowArgs sa, uint32_t* q
         cudaError_t e = shadow_eval_dispatch(L.U, L.grid, L.block, L.smem, s, sa, nullptr);
         if (e != cudaSuccess) return e;
     }
+    if (evaluated) {
+        cudaError_t e = cudaEventRecord(evaluated, s);
+        if (e != cudaSuccess) return e;
+    }
     sa.n_items = L.items2;
     sa.queue = queues + L.queue2;
+    if (sa.tstamp) sa.tstamp += 2;
     return shadow_chain_dispatch(L.m, L.cls != 0, L.grid2, L.block2, L.smem2, s, sa, nullptr);
 }
 
@@ -694,6 +749,9 @@ static void batch_args(Batch& B, WalkArgs& wa, ShadowArgs& sa) {
 }
 
 static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, ShadowArgs& sa, cudaStream_t s) {
+    unsigned long long* ts = B.stamping ? B.tstamps.as<unsigned long long>() + 4 * (&L - B.launches.data()) : nullptr;
+    wa.tstamp = ts;
+    sa.tstamp = ts;
     if (L.kind == 0) {
         wa.tiles = B.tiles.as<DevTile>() + L.off;
         wa.n_tiles = L.count;
@@ -713,13 +771,16 @@ static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, Shado
         sa.queue = B.queues.as<uint32_t>() + L.queue;
         return shadow_fd_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, sa, nullptr);
     }
-    return launch_shadow_interp(L, sa, B.queues.as<uint32_t>(), B.eval_items.as<uint32_t>(), s);
+    const size_t i = &L - B.launches.data();
+    return launch_shadow_interp(L, sa, B.queues.as<uint32_t>(), B.eval_items.as<uint32_t>(), s,
+                                i < B.evals.size() && !L.follow ? B.evals[i] : nullptr);
 }
 
 // One run of a batch: zero the work counters and status words, then every
-// launch group (shadow kernels first, they have the longest serial chains)
-// on its own stream of the pool, forked from and joined back into st.
-static int enqueue_batch(Batch& B, cudaStream_t st) {
+// launch group (shadow kernels first, on high-priority streams: they hold
+// the longest serial chains) on its own stream, forked from and joined back
+// into st.
+static int enqueue_batch(Batch& B, cudaStream_t st, std::vector<cudaEvent_t>* ends = nullptr) {
     Context& C = *g_ctx;
     DR_CUDA(cudaMemsetAsync(B.queues.p, 0, B.queues.bytes, st));
     DR_CUDA(cudaMemsetAsync(B.status.p, 0, B.status.bytes, st));
@@ -727,34 +788,49 @@ static int enqueue_batch(Batch& B, cudaStream_t st) {
     ShadowArgs sa;
     batch_args(B, wa, sa);
     DR_CUDA(cudaEventRecord(B.fork, st));
-    const size_t np = C.pool.size();
-    size_t used = 0;
+    std::vector<cudaStream_t> used;
+    auto take = [&](std::vector<cudaStream_t>& pool, size_t& k) -> cudaStream_t {
+        cudaStream_t s = pool[k % pool.size()];
+        if (k < pool.size()) {
+            used.push_back(s);
+            if (cudaStreamWaitEvent(s, B.fork, 0) != cudaSuccess) return nullptr;
+        }
+        ++k;
+        return s;
+    };
+    size_t k_lo = 0, k_hi = 0;
     cudaStream_t prev = nullptr;
-    for (int pass = 0; pass < 2; ++pass) {
+    int rc = DR_OK;
+    for (int pass = 0; pass < 2 && rc == DR_OK; ++pass) {
         for (const LaunchSpec& L : B.launches) {
             if ((L.items == 0 && L.items2 == 0) || (pass == 0) != (L.kind != 0)) continue;
             cudaStream_t s = prev;
             if (!L.follow || !prev) {
-                s = C.pool[used % np];
-                if (used < np) DR_CUDA(cudaStreamWaitEvent(s, B.fork, 0));
-                ++used;
+                s = pass == 0 ? take(C.hpool, k_hi) : take(C.pool, k_lo);
+                // walks start once the step matrices are evaluated, so the
+                // shadow chains (high priority) are placed before them
+                if (s && pass == 1)
+                    for (size_t j = 0; j < B.launches.size(); ++j)
+                        if (B.launches[j].kind == 1 && !B.launches[j].follow && B.launches[j].items)
+                            if (cudaStreamWaitEvent(s, B.evals[j], 0) != cudaSuccess) s = nullptr;
             }
+            if (!s) { rc = cuda_fail(cudaErrorUnknown, "stream fork"); break; }
             prev = s;
             cudaError_t e = launch_one(B, L, wa, sa, s);
+            if (e == cudaSuccess && ends) e = cudaEventRecord((*ends)[&L - B.launches.data()], s);
             if (e != cudaSuccess) {
-                // rejoin what was forked so a capture can end cleanly
-                for (size_t i = 0; i < std::min(used, np); ++i) {
-                    cudaEventRecord(B.joins[i], C.pool[i]);
-                    cudaStreamWaitEvent(st, B.joins[i], 0);
-                }
-                return cuda_fail(e, L.kind == 0 ? "walk launch" : "shadow launch");
+                rc = cuda_fail(e, L.kind == 0 ? "walk launch" : "shadow launch");
+                break;
             }
         }
     }
-    for (size_t i = 0; i < std::min(used, np); ++i) {
-        DR_CUDA(cudaEventRecord(B.joins[i], C.pool[i]));
-        DR_CUDA(cudaStreamWaitEvent(st, B.joins[i], 0));
+    // rejoin every forked stream (also on errors, so a capture can end cleanly)
+    for (size_t i = 0; i < used.size(); ++i) {
+        cudaEventRecord(B.joins[i], used[i]);
+        cudaStreamWaitEvent(st, B.joins[i], 0);
     }
+    if (rc != DR_OK) return rc;
+    DR_CUDA(cudaGetLastError());
     if (B.pipe_on) return enqueue_pipeline(B, st);
     return DR_OK;
 }
@@ -813,6 +889,38 @@ int batch_profile(Batch& B, std::vector<float>* ms, std::vector<float>* ms2) {
     return DR_OK;
 }
 
+// One eager (uncaptured) run with the launch groups concurrent as in a
+// normal run, the kernels stamping when their first block started and their
+// last block ended: per launch [start, end, start2, end2] in ms after the
+// earliest start (start2/end2: kind 1's chain kernel; -1 = did not run).
+int batch_timeline(Batch& B, std::vector<float>* out) {
+    Context& C = *g_ctx;
+    cudaStream_t st = C.stream;
+    const size_t n = B.launches.size();
+    std::vector<unsigned long long> h(4 * n);
+    for (size_t i = 0; i < n; ++i) {
+        h[4 * i] = h[4 * i + 2] = ~0ull;
+        h[4 * i + 1] = h[4 * i + 3] = 0;
+    }
+    DR_CUDA(B.tstamps.alloc(8 * h.size()));
+    DR_CUDA(cudaMemcpy(B.tstamps.p, h.data(), 8 * h.size(), cudaMemcpyHostToDevice));
+    B.stamping = true;
+    int rc = enqueue_batch(B, st);
+    B.stamping = false;
+    if (rc) return rc;
+    DR_CUDA(cudaStreamSynchronize(st));
+    DR_CUDA(cudaMemcpy(h.data(), B.tstamps.p, 8 * h.size(), cudaMemcpyDeviceToHost));
+    unsigned long long t0 = ~0ull;
+    for (size_t i = 0; i < 2 * n; ++i) t0 = std::min(t0, h[2 * i]);
+    out->assign(4 * n, -1.f);
+    for (size_t i = 0; i < 2 * n; ++i)
+        if (h[2 * i] != ~0ull) {
+            (*out)[2 * i] = (float)((h[2 * i] - t0) * 1e-6);
+            (*out)[2 * i + 1] = (float)((h[2 * i + 1] - t0) * 1e-6);
+        }
+    return DR_OK;
+}
+
 int batch_run(Batch& B, cudaStream_t st) {
     Context& C = *g_ctx;
     if (!st) st = C.stream;
@@ -828,7 +936,8 @@ int batch_run(Batch& B, cudaStream_t st) {
         cudaStreamDestroy(cap);
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
         if (e != cudaSuccess) return cuda_fail(e, "end capture");
-        e = cudaGraphInstantiate(&B.graph, g, 0);
+        // node priorities: the shadow chains are placed before the walk blocks
+        e = cudaGraphInstantiateWithFlags(&B.graph, g, cudaGraphInstantiateFlagUseNodePriority);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) { B.graph = nullptr; return cuda_fail(e, "graph instantiate"); }
     }
@@ -932,6 +1041,10 @@ int dr_init(int device) {
     DR_CUDA(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     c->pool.resize(24);   // more than the launch groups of any batch, so none queue behind another
     for (auto& s : c->pool) DR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int prio_lo = 0, prio_hi = 0;
+    DR_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    c->hpool.resize(8);
+    for (auto& s : c->hpool) DR_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, prio_hi));
     const auto& tab = prime_table(DR_MAX_K);
     std::vector<uint32_t> pinv(DR_MAX_K), r2(DR_MAX_K);
     for (int k = 0; k < DR_MAX_K; ++k) {
@@ -1149,6 +1262,20 @@ int dr_batch_read_pipeline(int32_t batch, double* delta, int32_t* topk_idx, doub
         }
     }
     if (signs) DR_CUDA(cudaMemcpy(signs, B->signs.p, 4ull * 4 * n, cudaMemcpyDeviceToHost));
+    return DR_OK;
+}
+
+int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t* n_launches, float* spans) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    std::vector<float> t;
+    rc = batch_timeline(*B, &t);
+    if (rc) return rc;
+    if (n_launches) *n_launches = (int32_t)(t.size() / 4);
+    for (int i = 0; i < (int)t.size() && i < 4 * max_launches; ++i)
+        if (spans) spans[i] = t[i];
     return DR_OK;
 }
 

@@ -50,6 +50,7 @@ struct Context {
     int sms = 0;
     cudaStream_t stream = nullptr, side = nullptr;
     std::vector<cudaStream_t> pool;   // launch groups of a batch run concurrently on these
+    std::vector<cudaStream_t> hpool;  // high-priority streams for the FP64 shadow launches
     DevBuf primes, pinv, r2;   // DR_MAX_K-entry prime table
     std::mutex mu;
     std::unordered_map<std::string, std::shared_ptr<Plan>> plan_cache;
@@ -86,7 +87,15 @@ struct LaunchSpec {
 // Interpreted-shadow launch geometry shared by batches and serving waves:
 // picks U and the per-warp rows of the evaluation kernel, the chain kernel's
 // shared memory, and both grids.  Returns DR_OK or an error status.
-int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms);
+int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs);
+
+// FP64 chain kernels (interpreted chain, integer-difference shadow) run as
+// blocks of kChainWarps warps that claim a whole SM's shared memory, so no
+// walk block shares their SM's issue slots; the grid is sized so the chains
+// finish with the longest one.
+constexpr int kChainWarps = 4;
+int chain_blocks(const DevShadowSeg* segs, uint32_t count);
+size_t chain_hog_smem();
 
 // Builds the interpreted-shadow launches of one (m, companion-shape) group:
 // segs (sorted longest first) become one launch, or several rounds of at most
@@ -125,6 +134,9 @@ struct Batch {
     cudaGraphExec_t graph = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr, join = nullptr;
     std::vector<cudaEvent_t> joins;
+    std::vector<cudaEvent_t> evals;     // per launch: its step-matrix evaluation is done
+    DevBuf tstamps;                     // diagnostics: 4 timestamps per launch
+    bool stamping = false;
     float last_ms = 0.f;
     bool has_shadow = false;
     ~Batch();
@@ -144,7 +156,9 @@ int cuda_fail(cudaError_t e, const char* where);
 struct ShadowArgs;
 // Evaluation then chain launch of one interpreted-shadow launch group on s;
 // sa carries the batch-wide pointers and this launch's segs / rows.
+// evaluated: recorded on s between the two kernels when not null.
 cudaError_t launch_shadow_interp(const LaunchSpec& L, ShadowArgs sa, uint32_t* queues,
-                                 const uint32_t* eval_items, cudaStream_t s);
+                                 const uint32_t* eval_items, cudaStream_t s,
+                                 cudaEvent_t evaluated = nullptr);
 
 }  // namespace dr

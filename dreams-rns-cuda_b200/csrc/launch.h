@@ -70,6 +70,8 @@ cudaError_t walk_dispatch_dense(uint32_t m, uint32_t D, int grid, int block, siz
 cudaError_t walk_dispatch_interp(uint32_t m, int grid, int block, size_t smem, cudaStream_t st,
                                  const WalkArgs& a, int* occ);
 
+// Launches carry their stream's priority as a launch attribute, so the
+// priority also holds for the kernel nodes of a captured CUDA graph.
 template <typename KernelT, typename ArgT>
 inline cudaError_t run_kernel(KernelT k, int grid, int block, size_t smem, cudaStream_t st,
                               const ArgT& a, int* occ) {
@@ -78,6 +80,20 @@ inline cudaError_t run_kernel(KernelT k, int grid, int block, size_t smem, cudaS
         if (e != cudaSuccess) return e;
     }
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, block, smem);
+    int prio = 0;
+    if (st && cudaStreamGetPriority(st, &prio) == cudaSuccess && prio != 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)grid);
+        cfg.blockDim = dim3((unsigned)block);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributePriority;
+        attr[0].val.priority = prio;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, k, a);
+    }
     k<<<grid, block, smem, st>>>(a);
     return cudaGetLastError();
 }

@@ -47,6 +47,7 @@ struct ShadowArgs {
     double* mf;                 // step-matrix buffer of the interpreted mode
     const uint32_t* eval_items; // segment (index into segs) of every evaluation item
     uint32_t rows_axes;         // evaluation: axis rows per sub-block
+    unsigned long long* tstamp; // diagnostics: [start, end] of this launch, or null
     uint32_t* queue;
     double* shadow;             // [3*w] final, [3*(n_walks + w)] checkpoint
     uint32_t n_walks;
@@ -68,43 +69,31 @@ constexpr int kShadowStateStride = 72;   // m*m <= 64 entries, then mantissa, ex
 // inlined so that the common path never pays for it.
 static __device__ __noinline__ double div_slow(double x, double b) { return __ddiv_rn(x, b); }
 
-// |x| as an unsigned bit pattern: for non-NaN doubles these order exactly as
-// the magnitudes do (+inf = 0x7ff0...0 is the largest), and every NaN lies
-// above +inf.  With M the largest |bits| of the matrix, the reference's
-// max(|P|) is NaN iff M > kInfBits, and max(|P|) > 1e10 iff M > kBigBits.
-constexpr unsigned long long kInfBits = 0x7ff0000000000000ULL;
-constexpr unsigned long long kBigBits = 0x4202a05f20000000ULL;   // 1e10
-__device__ __forceinline__ unsigned long long absbits(double x) {
-    return (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffULL;
-}
-__device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) {
-    return a > b ? a : b;
-}
-__device__ __forceinline__ bool is_zero(double x) {
-    return ((__double2hiint(x) & 0x7fffffff) | __double2loint(x)) == 0;
-}
 // Biased exponent field of x (0 for zeros and subnormals).
 __device__ __forceinline__ int bexp(double x) { return (__double2hiint(x) >> 20) & 0x7ff; }
 
 // P /= mx entrywise, each quotient rounded to nearest.  The Markstein path
 // (y = RN(1/mx); q0 = RN(x*y); r = x - mx*q0 by FMA; q = RN(q0 + r*y);
 // P. Markstein, IBM J. Res. Dev. 34(1), 1990) is exact when y, q and the
-// residual r are normal numbers: r is exact when |x| >= 2^-969 (biased
-// exponent >= 54, so |r| ~ 2^-52 |x| stays normal), q is normal when
-// ex - em >= -1021 (|x/mx| > 2^(ex - em - 1)), y is normal when mx < 2^1022.
-// Entries outside these ranges (and an infinite mx) take the IEEE division.
-// A zero keeps its sign.  The test depends only on the inputs, so its
-// branch resolves while the reciprocal is in flight.
+// residual r are normal numbers: y is normal for mx < 2^1022 (biased exponent
+// em < 2045); r ~ 2^-52 |x| is normal for a biased exponent ex >= 60 of x;
+// q is normal when ex >= em - 1000 (|x/mx| > 2^(ex - em - 1)).  Entries outside
+// these ranges (and an infinite mx) take the IEEE division.  The test reads
+// only exponent bits of the inputs, so it completes on the integer pipe
+// while the reciprocal is in flight.  q takes the sign of x, which keeps the
+// sign of a zero.
 template <int M_>
 __device__ __forceinline__ void rescale(double (&P)[M_][M_], double mx) {
+    const double y = __drcp_rn(mx);
     const int em = bexp(mx);
+    const int t_hi = max(60, em - 1000) << 20;
     bool slow = em >= 2045;
 #pragma unroll
     for (int i = 0; i < M_; ++i)
 #pragma unroll
         for (int j = 0; j < M_; ++j) {
-            const int ex = bexp(P[i][j]);
-            slow |= !is_zero(P[i][j]) & ((ex < 60) | (ex - em < -1020));
+            const int ahi = __double2hiint(P[i][j]) & 0x7fffffff;
+            slow |= (ahi < t_hi) & ((ahi | __double2loint(P[i][j])) != 0);
         }
     if (__builtin_expect(slow, 0)) {
 #pragma unroll
@@ -113,7 +102,6 @@ __device__ __forceinline__ void rescale(double (&P)[M_][M_], double mx) {
             for (int j = 0; j < M_; ++j) P[i][j] = div_slow(P[i][j], mx);
         return;
     }
-    const double y = __drcp_rn(mx);
 #pragma unroll
     for (int i = 0; i < M_; ++i)
 #pragma unroll
@@ -121,8 +109,7 @@ __device__ __forceinline__ void rescale(double (&P)[M_][M_], double mx) {
             const double x = P[i][j];
             const double q0 = __dmul_rn(x, y);
             const double r = __fma_rn(-q0, mx, x);
-            const double q = __fma_rn(r, y, q0);
-            P[i][j] = is_zero(x) ? x : q;
+            P[i][j] = copysign(__fma_rn(r, y, q0), x);
         }
 }
 
@@ -153,10 +140,14 @@ struct FChain {
         sc_e = 0;
         nan_seen = false;
     }
-    // P <- P @ X with numpy's rounding, then the max-abs rescale
+    // P <- P @ X with numpy's rounding, then the max-abs rescale.  A NaN
+    // anywhere in P makes its whole row NaN in the product (NaN * x is NaN
+    // for every x), so the new entries alone decide the reference's
+    // "max(|P|) is NaN" case.
     __device__ __forceinline__ void step(const double (&X)[M_][M_]) {
         double C[M_][M_];
-        unsigned long long mb = 0;
+        double mx = 0.0;
+        bool has_nan = false;
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
@@ -165,40 +156,39 @@ struct FChain {
 #pragma unroll
                 for (int k = 1; k < M_; ++k) c = __fma_rn(P[i][k], X[k][j], c);
                 C[i][j] = c;
-                mb = umax64(mb, absbits(c));
+                has_nan |= c != c;
+                mx = fmax(mx, fabs(c));
             }
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
             for (int j = 0; j < M_; ++j) P[i][j] = C[i][j];
-        const bool has_nan = mb > kInfBits;
-        if (!has_nan && mb > kBigBits) {
-            const double mx = __longlong_as_double((long long)mb);
+        if (!has_nan && mx > 1e10) {
             rescale<M_>(P, mx);
             scale_acc(sc_m, sc_e, mx);
         }
         nan_seen |= has_nan;
     }
-    // companion step: columns shift left, last column = P @ c.  The dense
-    // product with exact 0/1 entries gives the shifted entry itself when it is
-    // nonzero, and for a zero the sum of the signed zeros P[i][k]*0, which is
-    // -0 only when every P[i][k] has its sign bit set; the last column is the
-    // dense product's own FMA chain.
+    // companion step: P @ X with X's first m-1 columns the shifted identity
+    // and its last column c.  The shifted entries use the dense product's
+    // own operations with the exact 0 and 1 (so signed zeros, infinities and
+    // NaNs come out as numpy's); they depend only on the old P and stay off
+    // the dependency chain.  A NaN in row i of P always reaches the new
+    // last[i], so the new column decides the NaN case.
     __device__ __forceinline__ void step_companion(const double (&c)[M_]) {
         double last[M_];
-        // the shifted columns are known before the new one: their max and
-        // signed-zero fix stay off the dependency chain
-        unsigned long long ms = 0;
-        bool allneg[M_];
+        double sh[M_][M_ > 1 ? M_ - 1 : 1];
+        double mxs = 0.0;
 #pragma unroll
-        for (int i = 0; i < M_; ++i) {
-            bool neg = true;
+        for (int i = 0; i < M_; ++i)
 #pragma unroll
-            for (int k = 0; k < M_; ++k) neg &= (__double2hiint(P[i][k]) < 0);
-            allneg[i] = neg;
+            for (int j = 0; j + 1 < M_; ++j) {
+                double v = __dmul_rn(P[i][0], j + 1 == 0 ? 1.0 : 0.0);
 #pragma unroll
-            for (int j = 1; j < M_; ++j) ms = umax64(ms, absbits(P[i][j]));
-        }
+                for (int k = 1; k < M_; ++k) v = __fma_rn(P[i][k], k == j + 1 ? 1.0 : 0.0, v);
+                sh[i][j] = v;
+                mxs = fmax(mxs, fabs(v));
+            }
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
             double v = __dmul_rn(P[i][0], c[0]);
@@ -206,20 +196,17 @@ struct FChain {
             for (int k = 1; k < M_; ++k) v = __fma_rn(P[i][k], c[k], v);
             last[i] = v;
         }
-        unsigned long long mb = ms;
+        bool has_nan = false;
+        double mx = mxs;
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
 #pragma unroll
-            for (int j = 0; j + 1 < M_; ++j) {
-                const double v = P[i][j + 1];
-                P[i][j] = is_zero(v) ? (allneg[i] ? -0.0 : 0.0) : v;
-            }
+            for (int j = 0; j + 1 < M_; ++j) P[i][j] = sh[i][j];
             P[i][M_ - 1] = last[i];
-            mb = umax64(mb, absbits(last[i]));
+            has_nan |= last[i] != last[i];
+            mx = fmax(mx, fabs(last[i]));
         }
-        const bool has_nan = mb > kInfBits;
-        if (!has_nan && mb > kBigBits) {
-            const double mx = __longlong_as_double((long long)mb);
+        if (!has_nan && mx > 1e10) {
             rescale<M_>(P, mx);
             scale_acc(sc_m, sc_e, mx);
         }
@@ -285,9 +272,11 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Steps per staged chunk of the chain kernel (entries * steps = 64 doubles
-// per lane and buffer, at least two steps).
-__host__ __device__ constexpr int chain_chunk_steps(int ne) { return ne >= 32 ? 2 : 64 / ne; }
+// Steps per staged chunk of the chain kernel (entries * steps = 16 doubles
+// per lane and buffer, at least two steps): a chunk of chain steps takes
+// thousands of cycles, far more than the copy of the next one, so small
+// buffers suffice and leave shared memory to the walk kernels running beside.
+__host__ __device__ constexpr int chain_chunk_steps(int ne) { return ne >= 8 ? 2 : 16 / ne; }
 
 // Evaluation: each warp takes items of kEvalSteps steps of one segment and
 // runs the float interpreter on U sub-blocks of 32 steps at a time.  The
@@ -302,6 +291,7 @@ __global__ void __launch_bounds__(128) k_shadow_eval(const ShadowArgs A) {
     double* rf = dsm + (size_t)warp * A.rows_per_warp * 32;
     double* axv = rf + (size_t)A.rows_regs * U * 32;
     double* outv = axv + (size_t)A.rows_axes * U * 32;
+    stamp_begin(A.tstamp);
     for (;;) {
         uint32_t it = 0;
         if (lane == 0) it = atomicAdd(A.queue, 1u);
@@ -344,6 +334,7 @@ __global__ void __launch_bounds__(128) k_shadow_eval(const ShadowArgs A) {
             }
         }
     }
+    stamp_end(A.tstamp);
 }
 
 template <int M_, bool COMP>
@@ -361,17 +352,20 @@ __device__ __forceinline__ void chain_step(FChain<M_>& ch, const double (&X)[COM
     }
 }
 
-// Chain: lane = segment, 32 segments per warp (one warp per block).  The
+// Chain: lane = segment, 32 segments per warp, every warp of the block on
+// its own items.  The
 // warp's entries for the next chunk of steps are copied into shared memory
 // ([buffer][step][entry][lane]) while the current chunk runs; every lane only
 // reads what it copied itself, so the per-thread cp.async group wait is the
 // only synchronisation.
 template <int M_, bool COMP>
-__global__ void __launch_bounds__(32) k_shadow_chain(const ShadowArgs A) {
+__global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
     constexpr int NE = COMP ? M_ : M_ * M_;
     constexpr int CS = chain_chunk_steps(NE);
-    extern __shared__ double dsm[];
+    extern __shared__ double dsm_all[];
     const int lane = threadIdx.x & 31;
+    double* dsm = dsm_all + (size_t)(threadIdx.x >> 5) * 2 * CS * NE * 32;
+    stamp_begin(A.tstamp);
     for (;;) {
         uint32_t it = 0;
         if (lane == 0) it = atomicAdd(A.queue, 1u);
@@ -449,11 +443,12 @@ __global__ void __launch_bounds__(32) k_shadow_chain(const ShadowArgs A) {
         cp_async_wait<0>();
         if (active) ch.end(W, g, A.state, A.shadow, A.status, g.walk);
     }
+    stamp_end(A.tstamp);
 }
 
 // Integer-difference shadow: NS streams of depth D per walk, lane = walk.
 template <int CLS, int M_, int D>
-__global__ void __launch_bounds__(128) k_shadow_intfd(const ShadowArgs A) {
+__global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
     constexpr int NS = (CLS == CLS_COMPANION) ? M_ : M_ * M_;
     extern __shared__ double dsm[];
     const int lane = threadIdx.x & 31;
@@ -463,6 +458,7 @@ __global__ void __launch_bounds__(128) k_shadow_intfd(const ShadowArgs A) {
     int64_t* axv = rf + A.rows_regs * 32;
     int64_t* stage = axv + kMaxAxes * 32;      // [(j*NS + i)][32 walks]
     int64_t* outv = stage + (D + 1) * NS * 32; // [stream][32 steps]
+    stamp_begin(A.tstamp);
     for (;;) {
         uint32_t it = 0;
         if (lane == 0) it = atomicAdd(A.queue, 1u);
@@ -528,6 +524,7 @@ __global__ void __launch_bounds__(128) k_shadow_intfd(const ShadowArgs A) {
         if (active) ch.end(W, g, A.state, A.shadow, A.status, wi);
         __syncwarp();
     }
+    stamp_end(A.tstamp);
 }
 
 }  // namespace dr

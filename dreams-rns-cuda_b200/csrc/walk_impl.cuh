@@ -50,6 +50,7 @@ struct WalkArgs {
     // per-warp shared memory layout, in 32-word rows
     uint32_t rows_regs, rows_consts, rows_stage;
     uint32_t rows_per_warp;
+    unsigned long long* tstamp;   // diagnostics: [start, end] of this launch, or null
 };
 
 struct WarpMem {
@@ -419,6 +420,7 @@ __global__ void __launch_bounds__(128) k_walk(const WalkArgs A) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const WarpMem wm = warp_mem(A, smem, warp);
+    stamp_begin(A.tstamp);
     for (;;) {
         uint32_t t = 0;
         if (lane == 0) t = atomicAdd(A.queue, 1u);
@@ -433,6 +435,7 @@ __global__ void __launch_bounds__(128) k_walk(const WalkArgs A) {
         else tile_interp<M_>(A, T, W, G, wm, lane);
         __syncwarp();
     }
+    stamp_end(A.tstamp);
 }
 
 }  // namespace dr

@@ -31,6 +31,15 @@ int dr_debug_template_degree(int32_t cls, int32_t m, int32_t degree);
  * denominator of the walk kernels' roofline. */
 int dr_bench_int_peak(int32_t kind, double *lane_ops_per_s);
 
+/* One uncaptured run of a prepared batch with its launch groups concurrent
+ * as in dr_batch_run; the kernels stamp the global timer when their first
+ * block starts and their last block ends.  spans: 4 floats per launch group
+ * (dr_batch_profile's order): [start, end, start2, end2] in ms after the
+ * earliest start; start2/end2 belong to the chain kernel of an interpreted
+ * shadow group; -1 where a kernel did not run. */
+int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t *n_launches,
+                            float *spans);
+
 /* The FP64 shadow's rescale division on the device: out[i] = x[i] / b[i]
  * rounded to nearest through the same code path the shadow kernels use
  * (Markstein correction, IEEE fallback).  Host buffers; b[i] > 1e10. */
