@@ -294,6 +294,7 @@ def bench_serving(seconds=3.0, rate=1000.0):
 
 
 def main():
+    global N_WALKS
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
@@ -302,12 +303,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the rational, CMF-sweep and serving measurements")
+    ap.add_argument("--walks", type=int, default=N_WALKS,
+                    help="PCFs per GPU (default 4096, the benchmark workload; smaller values "
+                         "give the same workload shape for profiler captures)")
     args = ap.parse_args()
+    N_WALKS = args.walks
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    config = {"workload": "uniform PCF batch: 4096 seeded PCFs, deg a<=2, deg b<=4, coeffs in "
+    config = {"workload": f"uniform PCF batch: {N_WALKS} seeded PCFs, deg a<=2, deg b<=4, coeffs in "
                           "[-10,10], m=2, depth 8000 with the depth-2000 convergent on the way, "
                           "K=32, delta(2000) vs own depth-8000 convergent, top-100",
               "walks_per_gpu": N_WALKS, "K": K, "depth": DEPTH, "checkpoint": CHECKPOINT,

@@ -1,4 +1,4 @@
-// Garner CRT to exact 32-bit limbs (reference runner.py:105-129).
+// Garner CRT to exact 32-bit limbs (reference runner.py:57-81).
 //
 // The reference's iterative CRT adds one mixed-radix digit per modulus:
 //     t_i = (a_i - x mod p_i) * inv(M_i mod p_i) mod p_i,  x += M_i t_i,
@@ -9,7 +9,7 @@
 //      own moduli j > i -- K sequential steps, K/32 mulmods each per lane;
 //   2. binary: limb l of x = sum_i t_i * M_i[l] (the M_i limbs are built once
 //      per moduli set), lane-parallel over limbs, then one carry pass;
-//   3. centring x - M if x > M // 2 (runner.py:127-129) to sign + magnitude.
+//   3. centring x - M if x > M // 2 (runner.py:79-81) to sign + magnitude.
 #include <cuda_runtime.h>
 #include <stdint.h>
 

@@ -1,6 +1,6 @@
 // Dreams delta from exact limbs, and top-k selection.
 //
-// delta = -(1 + ln|p/q - L| / ln|q|) (reference runner.py:151-173).  With the
+// delta = -(1 + ln|p/q - L| / ln|q|) (reference runner.py:103-125).  With the
 // target as a ratio L = Lnum / Lden of integers (a dyadic Lden = 2^e for a
 // decimal/binary target), the error is computed without cancellation:
 //     |p/q - L| = |p*Lden - Lnum*q| / (|q| * Lden)

@@ -590,7 +590,8 @@ int chain_blocks(const DevShadowSeg* segs, uint32_t count) {
     return (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (items + kChainWarps - 1) / kChainWarps));
 }
 
-int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs) {
+int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs,
+                           bool whole_sm) {
     const uint32_t base = L.rows_regs + max_dim + L.m * L.m;
     uint32_t U = 1;
     for (uint32_t u : {4u, 2u})
@@ -617,7 +618,8 @@ int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevSh
     }
     L.grid = std::max(1, std::min((int)((L.items + wpb - 1) / wpb), occ * sms));
     L.block2 = 32 * kChainWarps;
-    L.smem2 = std::max(shadow_chain_smem(L.m, L.cls != 0) * kChainWarps, chain_hog_smem());
+    L.smem2 = shadow_chain_smem(L.m, L.cls != 0) * kChainWarps;
+    if (whole_sm) L.smem2 = std::max(L.smem2, chain_hog_smem());
     e = shadow_chain_dispatch(L.m, L.cls != 0, 0, L.block2, L.smem2, nullptr, sa, &occ);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
     if (occ < 1) {

@@ -87,7 +87,10 @@ struct LaunchSpec {
 // Interpreted-shadow launch geometry shared by batches and serving waves:
 // picks U and the per-warp rows of the evaluation kernel, the chain kernel's
 // shared memory, and both grids.  Returns DR_OK or an error status.
-int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs);
+// whole_sm: the chain blocks claim a whole SM's shared memory (batches,
+// whose walks run beside them); serving waves request only what they use.
+int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs,
+                           bool whole_sm = true);
 
 // FP64 chain kernels (interpreted chain, integer-difference shadow) run as
 // blocks of kChainWarps warps that claim a whole SM's shared memory, so no

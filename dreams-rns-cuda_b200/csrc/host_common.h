@@ -10,7 +10,7 @@ namespace dr {
 void set_error(const std::string& msg);
 const std::string& last_error();
 
-// The first K primes below 2^31, descending (reference runner.py:81-100).
+// The first K primes below 2^31, descending (reference runner.py:33-52).
 const std::vector<uint32_t>& prime_table(int K);
 
 // Montgomery constants for R = 2^32: pinv = -p^-1 mod 2^32, r1 = R mod p,

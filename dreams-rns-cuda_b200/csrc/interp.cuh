@@ -16,7 +16,7 @@
 
 namespace dr {
 
-// Residue interpreter (reference runner.py:246-308): registers, constants and
+// Residue interpreter (reference runner.py:198-260): registers, constants and
 // axis values are Montgomery residues [slot*32 + lane].  Returns true when an
 // INV met a zero operand (the reference's "dead lane", config.h:166-169).
 __device__ __forceinline__ bool interp_modp(const uint4* __restrict__ code, uint32_t n,
@@ -70,7 +70,7 @@ __device__ __forceinline__ double cube_rn(double x) {
     return __dadd_rn(p1, __fma_rn(e, x, e1));
 }
 
-// Float64 interpreter (reference runner.py:311-364, cmf_walk.py:261-313),
+// Float64 interpreter (reference runner.py:263-316, cmf_walk.py:261-313),
 // U sub-blocks of 32 steps at once: every decoded instruction is applied to
 // U independent values per lane, so the shared-memory round trips of one
 // sub-block overlap those of the others.  Register r of sub-block u for this

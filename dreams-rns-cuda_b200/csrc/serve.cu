@@ -320,7 +320,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
         s.queue = q++;
         if (s.kind == 1) {
             s.queue2 = q++;
-            const int rc = shadow_interp_geometry(s, max_dim, C.sms, segs.data() + s.off);
+            const int rc = shadow_interp_geometry(s, max_dim, C.sms, segs.data() + s.off, false);
             if (rc) return rc;
             continue;
         }

@@ -1,4 +1,4 @@
-// FP64 shadow walk (reference runner.py:429-446, cmf_walk.py:400-416):
+// FP64 shadow walk (reference runner.py:381-398, cmf_walk.py:400-416):
 //     P_f <- P_f @ M_f(s);  if max|P_f| > 1e10: P_f /= max, log_scale += ln(max)
 // The recurrence is inherently sequential (the rescale points depend on the
 // running values), so each walk's chain runs step by step; what is spread over

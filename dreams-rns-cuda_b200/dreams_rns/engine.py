@@ -68,7 +68,7 @@ class WalkRequest:
 def pcf_request(program, a0: int, depth: int, K: int = 32, shift_val: int = 1,
                 checkpoint: int = 0, shadow: bool = True) -> WalkRequest:
     """PCF walk: P0 = [[1, a0], [0, 1]], LOAD_X = shift + step * direction
-    (reference runner.py:386-461)."""
+    (reference runner.py:338-413)."""
     blob = program_blob(program)
     dirs = _directions(blob)
     return WalkRequest(blob=blob, K=K, depth=depth, a0=int(a0), pcf_init=True, q_row=1,

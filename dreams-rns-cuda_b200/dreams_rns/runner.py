@@ -31,7 +31,7 @@ __all__ = [
 
 @dataclass
 class WalkConfig:
-    """Walk configuration (reference runner.py:71-76)."""
+    """Walk configuration (reference runner.py:23-28)."""
 
     K: int = 32
     depth: int = 2000
@@ -39,7 +39,7 @@ class WalkConfig:
 
 
 def generate_rns_primes(K: int) -> np.ndarray:
-    """The K largest primes below 2^31, descending (reference runner.py:81-100)."""
+    """The K largest primes below 2^31, descending (reference runner.py:33-52)."""
     if K <= 0:
         return np.zeros(0, dtype=np.int64)
     if K > N.DR_MAX_K:
@@ -100,7 +100,7 @@ def crt_batch(residues: np.ndarray, K: int, moduli: Optional[Sequence[int]] = No
 
 
 def crt_reconstruct(residues, primes):
-    """(x, M): x = sum of mixed-radix digits, M = prod(primes) (runner.py:105-124).
+    """(x, M): x = sum of mixed-radix digits, M = prod(primes) (runner.py:57-76).
 
     Moduli must be odd and in [3, 2^31); the first residue is used as given
     (as the reference does) and must lie in [0, 2^32).
@@ -125,7 +125,7 @@ def crt_reconstruct(residues, primes):
 
 
 def centered(x, M):
-    """runner.py:127-129."""
+    """runner.py:79-81."""
     return x - M if x > M // 2 else x
 
 
@@ -133,7 +133,7 @@ def centered(x, M):
 
 def compute_dreams_delta_float(p_val: float, q_val: float, log_scale: float,
                                target: float) -> Tuple[float, float]:
-    """Approximate delta from the float shadow (runner.py:134-148)."""
+    """Approximate delta from the float shadow (runner.py:86-100)."""
     if not math.isfinite(p_val) or not math.isfinite(q_val) or abs(q_val) < 1e-300:
         return -1e10, 0.0
     est = p_val / q_val
@@ -192,7 +192,7 @@ def delta_batch(ps: Sequence[int], qs: Sequence[int], targets: Sequence[Tuple[in
 
 
 def compute_dreams_delta_exact(p_big: int, q_big: int, target, dps: int = 200):
-    """Exact delta from big integers (runner.py:151-173), computed on the GPU.
+    """Exact delta from big integers (runner.py:103-125), computed on the GPU.
 
     Like the reference it sets the process-wide mpmath precision to ``dps``;
     the target is taken as mpf(str(target)) at that precision.
@@ -204,7 +204,7 @@ def compute_dreams_delta_exact(p_big: int, q_big: int, target, dps: int = 200):
     try:
         num, den = target_ratio(target)
     except OverflowError:
-        # err = |approx - L| is inf (L infinite) or nan (L nan); runner.py:168-173
+        # err = |approx - L| is inf (L infinite) or nan (L nan); runner.py:120-125
         if abs(q_big) <= 1 or mp.isinf(mp.mpf(str(target))):
             return float("-inf")
         return float("nan")
@@ -214,7 +214,7 @@ def compute_dreams_delta_exact(p_big: int, q_big: int, target, dps: int = 200):
 # ---- PCF compilation ----------------------------------------------------------
 
 def compile_pcf(a_str: str, b_str: str) -> Optional[CmfProgram]:
-    """Companion bytecode of PCF(a, b) (runner.py:178-214): n is axis 0 with
+    """Companion bytecode of PCF(a, b) (runner.py:130-166): n is axis 0 with
     direction 1, entries (0,1)=b, (1,0)=1, (1,1)=a; None for imaginary input."""
     import sympy as sp
     from sympy.abc import n
@@ -235,7 +235,7 @@ def compile_pcf(a_str: str, b_str: str) -> Optional[CmfProgram]:
 
 
 def pcf_initial_values(a_str: str):
-    """a(0) as an int (runner.py:217-225)."""
+    """a(0) as an int (runner.py:169-177)."""
     import sympy as sp
     from sympy.abc import n
     return int(sp.sympify(a_str).subs(n, 0))
@@ -250,7 +250,7 @@ def _as_reference_dict(r: dict) -> dict:
 
 
 def run_pcf_walk(program: CmfProgram, a0: int, depth: int, K: int = 32, shift_val: int = 1):
-    """P = A * M(1) ... M(depth) on the GPU (reference runner.py:386-461).
+    """P = A * M(1) ... M(depth) on the GPU (reference runner.py:338-413).
 
     Returns p_residues, q_residues (int64 (K,)), p_float, q_float, log_scale
     (FP64 shadow) and primes, exactly like the reference.
@@ -267,7 +267,7 @@ def run_pcf_walk(program: CmfProgram, a0: int, depth: int, K: int = 32, shift_va
 
 def verify_pcf(a_str: str, b_str: str, limit_str: str, depth: int = 2000, K: int = 32,
                dps: int = 200):
-    """compile -> walk -> CRT -> delta (reference runner.py:464-524)."""
+    """compile -> walk -> CRT -> delta (reference runner.py:416-476)."""
     import sympy as sp
     import mpmath as mp
     mp.mp.dps = dps

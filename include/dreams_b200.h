@@ -49,8 +49,8 @@ extern "C" {
  *     (sn_a*td_a + s*tn_a*sd_a) * inv(sd_a*td_a)  (mod p)
  * with (sn, sd, tn, td) = axis_params[axis_offset + 4a .. +3]
  * (reference cmf_walk.py:221-224; the PCF walk is sn = shift, tn = direction,
- * sd = td = 1, runner.py:273-275).
- * Outputs: p = P[0][m-1], q = P[q_row][m-1] (PCF: q_row = 1, runner.py:449-450;
+ * sd = td = 1, runner.py:225-227).
+ * Outputs: p = P[0][m-1], q = P[q_row][m-1] (PCF: q_row = 1, runner.py:401-402;
  * CMF: q_row = m-1, cmf_walk.py:419-420) written to
  * p_res[res_offset + k], q_res[res_offset + k] for k < K.  With a non-zero
  * checkpoint the same outputs after `checkpoint` steps go to
@@ -102,7 +102,7 @@ const char *dr_last_error(void);
 int dr_version(void);
 
 /* The first K primes below 2^31 in descending order (reference
- * runner.py:81-100 generate_rns_primes). */
+ * runner.py:33-52 generate_rns_primes). */
 int dr_prime_table(int K, uint32_t *out);
 
 /* Validate a program blob (reference compiler.py:64-89 layout) and report how
@@ -113,7 +113,7 @@ int dr_program_info(const uint8_t *blob, uint64_t size, int32_t *cls_out,
                     int32_t *degree_out, int32_t *n_regs_out);
 
 /* ---- walks ------------------------------------------------------------
- * Batch of walks, host buffers (reference runner.py:386-461 run_pcf_walk and
+ * Batch of walks, host buffers (reference runner.py:338-413 run_pcf_walk and
  * cmf_walk.py:363-431 run_cmf_walk, one dict per walk).  blobs: all program
  * blobs back to back, blob_offsets[n_programs + 1].  tune may be NULL.     */
 int dr_walk_batch(const dr_walk_desc *walks, int32_t n_walks,
@@ -139,7 +139,7 @@ int dr_batch_stats(int32_t batch, uint64_t *prime_steps, uint32_t *n_tiles,
 
 /* Device pipeline after the walk, part of every dr_batch_run once set:
  * CRT of p, q (and the checkpoint's p, q) to centred limbs, the Dreams delta
- * (reference runner.py:151-173) and top-k by delta.  DR_DELTA_FIXED scores the
+ * (reference runner.py:103-125) and top-k by delta.  DR_DELTA_FIXED scores the
  * final convergent against one target L = lnum_sign * lnum / lden; DR_DELTA_SELF
  * scores the checkpoint convergent against the walk's own final convergent.   */
 #define DR_DELTA_NONE   0
@@ -174,7 +174,7 @@ int dr_batch_profile(int32_t batch, int32_t max_launches, int32_t *n_launches, i
                      int32_t *cls, int32_t *m, int32_t *degree, uint32_t *items, float *ms,
                      float *ms2);
 
-/* ---- CRT (reference runner.py:105-129 crt_reconstruct + centered) --------
+/* ---- CRT (reference runner.py:57-81 crt_reconstruct + centered) --------
  * residues[i*K + k] mod moduli[k] for n values.  Outputs the centred value
  * x - M if x > M/2 else x, where x in [0, M) is the reference's CRT result,
  * as sign (+1, -1 or 0) and magnitude limbs (little-endian u32,
@@ -205,7 +205,7 @@ int dr_crt_batch_device_noalloc(const uint32_t *residues_d, int32_t K, int32_t n
                                 uint32_t *limbs_d, int32_t limb_stride, int32_t *sign_d,
                                 void *stream);
 
-/* ---- delta (reference runner.py:151-173 compute_dreams_delta_exact) -----
+/* ---- delta (reference runner.py:103-125 compute_dreams_delta_exact) -----
  * delta = -(1 + ln|p/q - L| / ln|q|), q = 0 -> -inf, p/q == L -> +inf,
  * |q| <= 1 -> -inf.  p, q: sign + magnitude limbs as produced by dr_crt_batch
  * (stride limb_stride).  L = Lnum / Lden given as sign + limbs (stride

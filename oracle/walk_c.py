@@ -54,7 +54,7 @@ def walk(blob: bytes, depth: int, K: int, axis: np.ndarray, init: np.ndarray,
 
 def pcf_walk(blob: bytes, a0: int, depth: int, K: int = 32, shift: int = 1,
              shadow: bool = True):
-    """Same outputs as ``walk_np.pcf_walk`` (reference runner.py:386-461)."""
+    """Same outputs as ``walk_np.pcf_walk`` (reference runner.py:338-413)."""
     m, dim, _, _, dirs = parse_blob(blob)
     axis = np.array([[shift, 1, d, 1] for d in dirs], dtype=np.int64).reshape(-1)
     init = np.array([[1, a0], [0, 1]], dtype=np.int64)

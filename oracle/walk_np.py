@@ -35,7 +35,7 @@ def parse_blob(blob: bytes):
 
 @lru_cache(maxsize=None)
 def _prime_list(K: int) -> Tuple[int, ...]:
-    """runner.py:81-100: the K largest primes below 2^31, by trial division."""
+    """runner.py:33-52: the K largest primes below 2^31, by trial division."""
     out = []
     c = (1 << 31) - 1
     while len(out) < K and c >= (1 << 30):
@@ -50,7 +50,7 @@ def primes(K: int) -> np.ndarray:
 
 
 def const_residues(consts: Sequence[int], pp: np.ndarray) -> np.ndarray:
-    """runner.py:230-243: table[i, k] = consts[i] mod p_k in [0, p_k)."""
+    """runner.py:182-195: table[i, k] = consts[i] mod p_k in [0, p_k)."""
     table = np.zeros((len(consts), len(pp)), dtype=np.int64)
     for i, c in enumerate(consts):
         table[i] = [int(c) % int(p) for p in pp]
@@ -58,13 +58,13 @@ def const_residues(consts: Sequence[int], pp: np.ndarray) -> np.ndarray:
 
 
 def _modinv_vec(vals: np.ndarray, pp: np.ndarray) -> np.ndarray:
-    """runner.py:300-304: pow(v, p-2, p) per prime, so 0 maps to 0."""
+    """runner.py:252-256: pow(v, p-2, p) per prime, so 0 maps to 0."""
     return np.array([pow(int(v), int(p) - 2, int(p)) for v, p in zip(vals, pp)],
                     dtype=np.int64)
 
 
 def eval_modp(ops, m: int, step: int, axis_res, pp: np.ndarray, table: np.ndarray):
-    """runner.py:246-308 and cmf_walk.py:193-258: one step matrix mod every prime.
+    """runner.py:198-260 and cmf_walk.py:193-258: one step matrix mod every prime.
 
     ``axis_res(axis, step)`` returns the (K,) residue vector of LOAD_X.
     Registers start at zero every step; unwritten matrix entries are zero.
@@ -104,7 +104,7 @@ def eval_modp(ops, m: int, step: int, axis_res, pp: np.ndarray, table: np.ndarra
 
 
 def eval_float(ops, m: int, step: int, axis_val, consts) -> np.ndarray:
-    """runner.py:311-364 / cmf_walk.py:261-313: the same program in float64."""
+    """runner.py:263-316 / cmf_walk.py:261-313: the same program in float64."""
     regs: Dict[int, float] = {}
     M = np.zeros((m, m), dtype=np.float64)
     get = lambda r: regs.get(r, 0.0)  # noqa: E731
@@ -138,7 +138,7 @@ def eval_float(ops, m: int, step: int, axis_val, consts) -> np.ndarray:
 
 
 def matmul_mod(A: np.ndarray, B: np.ndarray, pp: np.ndarray) -> np.ndarray:
-    """runner.py:369-381 and cmf_walk.py:174-188: (A @ B) mod p per prime."""
+    """runner.py:321-333 and cmf_walk.py:174-188: (A @ B) mod p per prime."""
     r = A.shape[0]
     C = np.zeros_like(A)
     for i in range(r):
@@ -151,7 +151,7 @@ def matmul_mod(A: np.ndarray, B: np.ndarray, pp: np.ndarray) -> np.ndarray:
 
 
 def _shadow_step(P_f: np.ndarray, M_f: np.ndarray, log_scale: float):
-    """runner.py:442-446: P_f <- P_f @ M_f, renormalised when max |P_f| > 1e10."""
+    """runner.py:394-398: P_f <- P_f @ M_f, renormalised when max |P_f| > 1e10."""
     P_f = P_f @ M_f
     mx = np.max(np.abs(P_f))
     if mx > 1e10:
@@ -168,7 +168,7 @@ def _result(P, P_f, log_scale, pp, prow, qrow, col):
 
 def pcf_walk(blob: bytes, a0: int, depth: int, K: int = 32, shift: int = 1,
              checkpoints: Sequence[int] = ()):
-    """runner.py:386-461: P = A * M(1) ... M(depth), A = [[1, a0], [0, 1]].
+    """runner.py:338-413: P = A * M(1) ... M(depth), A = [[1, a0], [0, 1]].
 
     LOAD_X axis a at 0-based step s is shift + s * directions[a].  Returns the
     reference dict; with ``checkpoints`` also ``{"checkpoints": {d: dict}}``
@@ -301,7 +301,7 @@ def cmf_walk_vec(blob: bytes, depth: int, K: int, shift_vals, initial_state, acc
 
 
 def crt(residues, primes_) -> Tuple[int, int]:
-    """runner.py:105-124: iterative CRT, x in [0, M) for reduced residues."""
+    """runner.py:57-76: iterative CRT, x in [0, M) for reduced residues."""
     x = int(residues[0])
     M = int(primes_[0])
     for a, p in zip(list(residues)[1:], list(primes_)[1:]):
@@ -313,12 +313,12 @@ def crt(residues, primes_) -> Tuple[int, int]:
 
 
 def centered(x: int, M: int) -> int:
-    """runner.py:127-129."""
+    """runner.py:79-81."""
     return x - M if x > M // 2 else x
 
 
 def delta_exact(p: int, q: int, target, dps: int = 200) -> float:
-    """runner.py:151-173: -(1 + log|p/q - L| / log|q|) in mpmath at ``dps``."""
+    """runner.py:103-125: -(1 + log|p/q - L| / log|q|) in mpmath at ``dps``."""
     import mpmath as mp
     mp.mp.dps = dps
     if q == 0:
@@ -333,7 +333,7 @@ def delta_exact(p: int, q: int, target, dps: int = 200) -> float:
 
 
 def delta_float(p_val: float, q_val: float, log_scale: float, target: float):
-    """runner.py:134-148: approximate delta from the float shadow."""
+    """runner.py:86-100: approximate delta from the float shadow."""
     if not math.isfinite(p_val) or not math.isfinite(q_val) or abs(q_val) < 1e-300:
         return -1e10, 0.0
     abs_err = abs(p_val / q_val - target)

@@ -2,11 +2,11 @@
  * Plain-C restatement of the reference RNS walk (TEST INFRASTRUCTURE ONLY).
  *
  * Same per-step semantics as the reference numpy engine, one prime at a time:
- *   - bytecode interpreter: reference python/dreams_rns/runner.py:246-308 and
+ *   - bytecode interpreter: reference python/dreams_rns/runner.py:198-260 and
  *     cmf_walk.py:193-258 (registers reset to 0 every step, INV = a^(p-2),
  *     LOAD_X = (sn*td + s*tn*sd) * inv(sd*td) mod p, LOAD_N = s mod p);
- *   - P <- P * M mod p: runner.py:369-381, cmf_walk.py:174-188;
- *   - float64 shadow: runner.py:311-364 and 442-446 (numpy's m x m matmul
+ *   - P <- P * M mod p: runner.py:321-333, cmf_walk.py:174-188;
+ *   - float64 shadow: runner.py:263-316 and 394-398 (numpy's m x m matmul
  *     accumulates c = a0*b0 then c = fma(ak, bk, c); max |P| > 1e10 rescale).
  * Only the tests and the benchmark's CPU legs load this file's library.
  */
