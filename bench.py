@@ -428,30 +428,22 @@ def main():
                 "peak_source": "measured live: dr_bench_int_peak mix of mad.wide.u32 and add/min"}
     walk_only.close()
 
-    # ---- end to end through the public API with host buffers: the walk
-    # (descriptors and programs up, residues and shadows down), then CRT and
-    # delta (residues up, limbs down, limbs up, deltas down)
+    # ---- end to end through the public API with host buffers: one sweep()
+    # call per step packs the requests, uploads descriptors and programs,
+    # walks, runs CRT -> delta -> top-k on the device and copies residues,
+    # shadows, statuses, deltas and the top-k back to host memory
     e2e_times = []
-    h2d = d2h = 0
     n = len(reqs)
     for it in range(3):
         t0 = time.perf_counter()
-        res = run_walks(reqs)
-        p = np.stack([r["p_residues"] for r in res] + [r["checkpoint"]["p_residues"] for r in res]).astype(np.uint32)
-        q = np.stack([r["q_residues"] for r in res] + [r["checkpoint"]["q_residues"] for r in res]).astype(np.uint32)
-        pv = dr.crt_batch(p, K)
-        qv = dr.crt_batch(q, K)
-        targets = [((a if b > 0 else -a), abs(b)) for a, b in zip(pv[:n], qv[:n])]
-        deltas = dr.delta_batch(pv[n:], qv[n:], targets)
+        out = dr.sweep(reqs, delta="self", topk=TOPK)
         e2e_times.append(time.perf_counter() - t0)
-    limbs = (31 * K + 31) // 32 + 2
+    from dreams_rns import _native as N_
     blob_bytes = sum(len(b) for b in set(blobs))
-    h2d = (n * 72 + blob_bytes + n * 4 * 8          # descriptors, programs, axis parameters
-           + p.nbytes + q.nbytes                    # residues into CRT
-           + 2 * n * (limbs + 1) * 4 * 2 + n * (limbs + 1) * 4 * 2)   # limbs into delta
-    d2h = (2 * 2 * n * K * 4 + 6 * n * 8 + n * 4    # residues, shadows, status
-           + 2 * 2 * n * (limbs * 4 + 8)            # CRT limbs, signs, lengths
-           + n * 8)                                  # deltas
+    h2d = n * N_.WALK_DTYPE.itemsize + blob_bytes + 8 * n * 4      # descriptors, programs, axes
+    n_res = int(out["p_residues"].size)
+    d2h = 2 * 4 * n_res + 6 * n * 8 + 4 * n + 8 * n + TOPK * 12      # residues, shadows, status, deltas, top-k
+    assert np.array_equal(np.asarray(out["topk_idx"]), np.asarray(pipe["topk_idx"])), "sweep top-k differs"
     e2e_s = statistics.median(e2e_times)
     e2e_val = prime_steps * world / e2e_s
     n_launch = int(st["launches"]) + 1 + 1 + 1     # walk/shadow groups + CRT + delta + top-k
@@ -465,7 +457,8 @@ def main():
             "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": "prime-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_s,
-                    "path": "run_walks + crt_batch + delta_batch (host buffers)"},
+                    "path": "dreams_rns.sweep(requests, delta='self', topk=100): host descriptors "
+                            "in, residues/shadows/deltas/top-k out"},
             "gpu_launches": n_launch,
             "roofline": roofline,
             "top1_delta": float(pipe["topk_val"][0]) if len(pipe["topk_val"]) else None}

@@ -95,58 +95,66 @@ def cmf_request(program, depth: int, K: int, shift_vals, trajectory_vals=None,
 
 
 class _Packed:
-    """Flat C-ABI arrays for a list of requests."""
+    """Flat C-ABI arrays for a list of requests (built with numpy, one pass)."""
 
     def __init__(self, reqs: Sequence[WalkRequest]):
+        n = len(reqs)
         index: Dict[bytes, int] = {}
         blobs: List[bytes] = []
+        prog = []
         for r in reqs:
-            if r.blob not in index:
-                index[r.blob] = len(blobs)
+            j = index.get(r.blob)
+            if j is None:
+                j = index[r.blob] = len(blobs)
                 blobs.append(r.blob)
+            prog.append(j)
         self.n_programs = len(blobs)
         offs = np.zeros(len(blobs) + 1, dtype=np.uint64)
         np.cumsum([len(b) for b in blobs], out=offs[1:])
         self.offsets = offs
         self.blobs = np.frombuffer(b"".join(blobs) or b"\0", dtype=np.uint8).copy()
-        n = len(reqs)
-        desc = np.zeros(n, dtype=N.WALK_DTYPE)
-        axis: List[int] = []
-        res = 0
-        self.res_off = np.zeros(n, dtype=np.int64)
-        self.cp_off = np.full(n, -1, dtype=np.int64)
-        for i, r in enumerate(reqs):
-            if r.K < 1 or r.K > N.DR_MAX_K:
-                raise ValueError(f"K must be in 1..{N.DR_MAX_K}")
+        Ks = np.array([r.K for r in reqs], dtype=np.int64).reshape(n)
+        if n and (Ks.min() < 1 or Ks.max() > N.DR_MAX_K):
+            raise ValueError(f"K must be in 1..{N.DR_MAX_K}")
+        for r in reqs:            # the reference treats a negative depth as no steps
             if r.depth < 0:
                 r.depth = 0
-            d = desc[i]
-            d["program"] = index[r.blob]
-            d["K"] = r.K
-            d["depth"] = r.depth
-            d["checkpoint"] = r.checkpoint
-            if not -(1 << 63) <= r.a0 < (1 << 63):
-                raise OverflowError("a0 outside int64")
-            d["a0"] = r.a0
-            d["flags"] = (N.DR_WALK_INIT_PCF if r.pcf_init else 0) | (N.DR_WALK_SHADOW if r.shadow else 0)
-            d["q_row"] = r.q_row
-            d["axis_offset"] = len(axis)
-            for t in r.axis:
-                for v in t:
-                    if not -(1 << 63) <= v < (1 << 63):
-                        raise OverflowError("axis parameter outside int64")
-                axis.extend(int(v) for v in t)
-            d["res_offset"] = res
-            self.res_off[i] = res
-            res += r.K
-            if r.checkpoint:
-                d["cp_res_offset"] = res
-                self.cp_off[i] = res
-                res += r.K
+        cps = np.array([r.checkpoint for r in reqs], dtype=np.uint64).reshape(n)
+        try:
+            a0 = np.array([r.a0 for r in reqs], dtype=np.int64).reshape(n)
+        except OverflowError:
+            raise OverflowError("a0 outside int64") from None
+        try:
+            axis = np.array([v for r in reqs for t in r.axis for v in t], dtype=np.int64)
+        except OverflowError:
+            raise OverflowError("axis parameter outside int64") from None
+        alen = np.array([4 * len(r.axis) for r in reqs], dtype=np.uint64).reshape(n)
+        sizes = Ks + np.where(cps > 0, Ks, 0)
+        res_off = np.zeros(n, dtype=np.int64)
+        if n:
+            np.cumsum(sizes[:-1], out=res_off[1:])
+        desc = np.zeros(n, dtype=N.WALK_DTYPE)
+        desc["program"] = prog
+        desc["K"] = Ks
+        desc["depth"] = [r.depth for r in reqs]
+        desc["checkpoint"] = cps
+        desc["a0"] = a0
+        desc["flags"] = [(N.DR_WALK_INIT_PCF if r.pcf_init else 0) | (N.DR_WALK_SHADOW if r.shadow else 0)
+                         for r in reqs]
+        desc["q_row"] = [r.q_row for r in reqs]
+        aoff = np.zeros(n, dtype=np.uint64)
+        if n:
+            np.cumsum(alen[:-1], out=aoff[1:])
+        desc["axis_offset"] = aoff
+        desc["res_offset"] = res_off
+        cp_off = np.where(cps > 0, res_off + Ks, -1)
+        desc["cp_res_offset"] = np.where(cps > 0, cp_off, 0)
+        self.res_off = res_off
+        self.cp_off = cp_off
         self.desc = desc
-        self.axis = np.array(axis or [0], dtype=np.int64)
-        self.n_axis = len(axis)
-        self.n_res = max(res, 1)
+        self.axis = axis if axis.size else np.zeros(1, dtype=np.int64)
+        self.n_axis = int(axis.size)
+        self.n_res = max(int(sizes.sum()) if n else 0, 1)
         self.n = n
 
 
@@ -200,6 +208,33 @@ def run_walks(reqs: Sequence[WalkRequest], chunk_steps: int = 0,
     return _unpack(pk, reqs, p, q, sh, st)
 
 
+def sweep(reqs: Sequence[WalkRequest], delta: Optional[str] = None,
+          target: Optional[Tuple[int, int]] = None, topk: int = 0, values: bool = False,
+          chunk_steps: int = 0) -> dict:
+    """One call for a sweep of many walks: walk every request, then on the
+    device reconstruct p and q by CRT, score the Dreams delta (``delta="fixed"``
+    against ``target`` = (Lnum, Lden), or ``"self"``: each walk's checkpoint
+    convergent against its own final one) and select the ``topk`` best.
+
+    Returns arrays (see ``WalkBatch.read_arrays``) plus ``delta``, ``topk_idx``,
+    ``topk_val`` and, with ``values``, the centred p, q (and checkpoint p, q) as
+    Python ints.  The batched counterpart of calling run_pcf_walk /
+    run_cmf_walk, crt_reconstruct and compute_dreams_delta_exact per walk.
+    """
+    b = WalkBatch(reqs, chunk_steps=chunk_steps)
+    try:
+        piped = bool(delta) or topk > 0 or values
+        if piped:
+            b.set_pipeline(delta=delta, target=target, topk=topk)
+        b.run()
+        out = b.read_arrays()
+        if piped:
+            out.update(b.read_pipeline(values=values))
+        return out
+    finally:
+        b.close()
+
+
 class WalkBatch:
     """A batch of walks prepared once and resident on the device."""
 
@@ -232,6 +267,21 @@ class WalkBatch:
         N.check(N.lib().dr_batch_read(self.handle, N.ptr(p), N.ptr(q), pk.n_res, N.ptr(sh), N.ptr(st)),
                 "dr_batch_read")
         return _unpack(pk, self.reqs, p, q, sh, st)
+
+    def read_arrays(self) -> dict:
+        """Results as arrays, without per-walk dicts: residues of walk i at
+        ``res_offset[i]`` (``K`` entries; the checkpoint's at ``cp_res_offset[i]``),
+        shadows ``(n, 3)`` rows of (p_float, q_float, log_scale)."""
+        pk = self.pk
+        p = np.zeros(pk.n_res, dtype=np.uint32)
+        q = np.zeros(pk.n_res, dtype=np.uint32)
+        sh = np.zeros(6 * pk.n, dtype=np.float64)
+        st = np.zeros(pk.n, dtype=np.uint32)
+        N.check(N.lib().dr_batch_read(self.handle, N.ptr(p), N.ptr(q), pk.n_res, N.ptr(sh), N.ptr(st)),
+                "dr_batch_read")
+        return {"p_residues": p, "q_residues": q, "res_offset": pk.res_off,
+                "cp_res_offset": pk.cp_off, "shadow": sh[:3 * pk.n].reshape(pk.n, 3),
+                "checkpoint_shadow": sh[3 * pk.n:].reshape(pk.n, 3), "status": st}
 
     def set_pipeline(self, delta: Optional[str] = None, target: Optional[Tuple[int, int]] = None,
                      topk: int = 0, crt: bool = True) -> None:

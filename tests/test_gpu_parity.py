@@ -309,3 +309,41 @@ def test_pipeline_self_and_fixed():
         d = walk_np.delta_exact(pl2["p"][i], pl2["q"][i], mp.pi, 200)
         assert (pl2["delta"][i] == d) if math.isinf(d) else abs(pl2["delta"][i] - d) < 1e-9
     b.close()
+
+
+def test_sweep_matches_walks_crt_and_delta():
+    """sweep(): one call with array results equals run_walks + per-walk CRT and
+    delta through the oracle, for mixed K, checkpoints and rational programs."""
+    import mpmath as mp
+    from oracle import walk_np
+    rng = random.Random(23)
+    reqs = []
+    for i in range(40):
+        a = dr.synth.poly_str([rng.randrange(-9, 10) for _ in range(3)])
+        b = dr.synth.poly_str([rng.randrange(-9, 10) for _ in range(4)])
+        if i % 4 == 1:
+            b = f"({b})/({dr.synth.poly_str([rng.randrange(1, 9), rng.randrange(-3, 4)])})"
+        prog = dr.compile_pcf(a, b)
+        depth = rng.randrange(300, 1500)
+        reqs.append(pcf_request(prog, dr.pcf_initial_values(a), depth, rng.choice([16, 32, 64]),
+                                checkpoint=depth // 3))
+    out = dr.sweep(reqs, delta="self", topk=7, values=True)
+    res = run_walks(reqs)
+    for i, (req, r) in enumerate(zip(reqs, res)):
+        o = int(out["res_offset"][i])
+        c = int(out["cp_res_offset"][i])
+        assert list(out["p_residues"][o:o + req.K]) == list(r["p_residues"])
+        assert list(out["q_residues"][c:c + req.K]) == list(r["checkpoint"]["q_residues"])
+        assert out["shadow"][i][0] == r["p_float"] and out["shadow"][i][2] == r["log_scale"]
+        pr = [int(p) for p in dr.generate_rns_primes(req.K)]
+        vals = []
+        for arr in (r["p_residues"], r["q_residues"], r["checkpoint"]["p_residues"],
+                    r["checkpoint"]["q_residues"]):
+            x, M = walk_np.crt([int(v) for v in arr], pr)
+            vals.append(walk_np.centered(x, M))
+        assert [out["p"][i], out["q"][i], out["cp_p"][i], out["cp_q"][i]] == vals
+        mp.mp.dps = 200
+        d = walk_np.delta_exact(vals[2], vals[3], mp.mpf(vals[0]) / mp.mpf(vals[1]), 200)
+        assert (out["delta"][i] == d) if math.isinf(d) else abs(out["delta"][i] - d) < 1e-9
+    order = sorted(range(len(reqs)), key=lambda i: (-out["delta"][i], i))[:7]
+    assert list(out["topk_idx"]) == order
