@@ -2,6 +2,8 @@
 // CRT, delta and top-k entry points.
 #include "engine.h"
 
+#include <chrono>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -106,7 +108,45 @@ int crt_tables_std(int K, std::shared_ptr<CrtSet>* out) {
     return DR_OK;
 }
 
+void* devcache_take(size_t n, size_t* got) {
+    Context* c = g_ctx;
+    if (!c) return nullptr;
+    std::lock_guard<std::mutex> lk(c->cache_mu);
+    // smallest cached block that fits without wasting more than half of it
+    auto it = c->cache.lower_bound(n);
+    if (it == c->cache.end() || it->first > 2 * n + (1u << 20)) return nullptr;
+    void* p = it->second;
+    *got = it->first;
+    c->cached_bytes -= it->first;
+    c->cache.erase(it);
+    return p;
+}
+
+void devcache_put(void* p, size_t bytes) {
+    Context* c = g_ctx;
+    constexpr size_t kCap = 8ull << 30;
+    if (c) {
+        std::lock_guard<std::mutex> lk(c->cache_mu);
+        if (c->cached_bytes + bytes <= kCap) {
+            c->cache.emplace(bytes, p);
+            c->cached_bytes += bytes;
+            return;
+        }
+    }
+    cudaFree(p);
+}
+
+Batch::Batch() {
+    for (DevBuf* b : {&progs, &code, &consts, &walks, &axis, &tiles, &groups, &group_done, &chunkP,
+                      &chunkSig, &shadow_list, &queues, &res, &shadow, &status, &mf, &eval_items,
+                      &shadow_state, &tstamps, &crt_in, &crt_out, &limbs, &signs, &delta, &tgt_num,
+                      &tgt_den, &tgt_sign, &tk_keys[0], &tk_keys[1], &tk_idx[0], &tk_idx[1]})
+        b->pooled = true;
+}
+
 Batch::~Batch() {
+    // pooled buffers go back to the cache: no work of this batch may remain
+    if (g_ctx) cudaStreamSynchronize(g_ctx->stream);
     if (graph) cudaGraphExecDestroy(graph);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -148,6 +188,15 @@ uint32_t chunk_policy(uint64_t total_group_steps, uint64_t n_groups, int sms, co
 
 }  // namespace
 
+// host time of the phases of the last batch_build (diagnostics)
+static double g_build_ms[8];
+static std::chrono::steady_clock::time_point g_build_t0;
+static void build_mark(int i) {
+    const auto t = std::chrono::steady_clock::now();
+    if (i == 0) g_build_t0 = t;
+    else g_build_ms[i - 1] = std::chrono::duration<double, std::milli>(t - g_build_t0).count();
+}
+
 int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs,
                 const uint64_t* blob_offsets, int32_t n_programs, const int64_t* axis,
                 uint64_t n_axis, const dr_tune* tune, uint64_t n_res, std::unique_ptr<Batch>* out) {
@@ -162,6 +211,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     auto B = std::make_unique<Batch>();
     B->n_walks = (uint32_t)n_walks;
     B->n_res = n_res;
+    build_mark(0);
 
     // ---- programs
     std::vector<std::shared_ptr<Plan>> plans(n_programs);
@@ -203,6 +253,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         dprogs[i] = d;
     }
 
+    build_mark(1);
     // ---- walks
     std::vector<DevWalk> dwalks(n_walks);
     uint64_t total_group_steps = 0, n_groups = 0;
@@ -266,6 +317,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         B->prime_steps += (uint64_t)W.K * W.depth;
     }
 
+    build_mark(2);
     // ---- tiles and groups
     const bool plain = engine == DR_ENGINE_PLAIN;
     const uint32_t chunk = plain ? 0xffffffffu : chunk_policy(total_group_steps, n_groups, C.sms, tune);
@@ -351,6 +403,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     B->n_tiles = (uint32_t)tiles.size();
     B->n_groups = (uint32_t)groups.size();
 
+    build_mark(3);
     // ---- shadow work lists
     std::map<LaunchKey, std::vector<uint32_t>> shadow_sets;
     for (int32_t w = 0; w < n_walks; ++w) {
@@ -414,6 +467,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         B->launches.push_back(L);
     }
 
+    build_mark(4);
     // ---- launch geometry
     const int wpb = (tune && tune->warps_per_block) ? (int)tune->warps_per_block : 4;
     uint32_t q = 0;
@@ -467,6 +521,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     }
     B->n_queues = q;
 
+    build_mark(5);
     // ---- upload
     cudaStream_t st = C.stream;
     if ((rc = upload(B->progs, dprogs, st))) return rc;
@@ -511,7 +566,9 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     for (size_t i = 0; i < B->launches.size(); ++i)
         if (B->launches[i].kind == 1) DR_CUDA(cudaEventCreateWithFlags(&B->evals[i], cudaEventDisableTiming));
     for (auto& e : B->joins) DR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    build_mark(6);
     DR_CUDA(cudaStreamSynchronize(st));
+    build_mark(7);
     *out = std::move(B);
     return DR_OK;
 }
@@ -1264,6 +1321,11 @@ int dr_batch_read_pipeline(int32_t batch, double* delta, int32_t* topk_idx, doub
         }
     }
     if (signs) DR_CUDA(cudaMemcpy(signs, B->signs.p, 4ull * 4 * n, cudaMemcpyDeviceToHost));
+    return DR_OK;
+}
+
+int dr_debug_build_phases(double* ms, int32_t n) {
+    for (int i = 0; i < n && i < 7; ++i) ms[i] = g_build_ms[i];
     return DR_OK;
 }
 

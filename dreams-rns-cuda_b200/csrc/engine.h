@@ -16,16 +16,29 @@
 
 namespace dr {
 
-// Owning device allocation.
+// Device block cache of the context: prepared batches take their buffers
+// from it and give them back when destroyed (after the device is idle), so
+// building and dropping a batch per call costs no cudaMalloc / cudaFree (the
+// latter synchronises the whole device).  Bounded; larger surpluses are freed.
+void* devcache_take(size_t n, size_t* got);
+void devcache_put(void* p, size_t bytes);
+
+// Owning device allocation.  A pooled buffer comes from and returns to the
+// context's block cache; its owner guarantees no work still uses it when it
+// is released.
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    bool pooled = false;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pooled) devcache_put(p, bytes);
+            else cudaFree(p);
+        }
         p = nullptr;
         bytes = 0;
     }
@@ -33,8 +46,13 @@ struct DevBuf {
         if (n <= bytes && p) return cudaSuccess;
         release();
         if (n == 0) n = 16;
+        if (pooled) {
+            p = devcache_take(n, &bytes);
+            if (p) return cudaSuccess;
+        }
         cudaError_t e = cudaMalloc(&p, n);
         if (e == cudaSuccess) bytes = n;
+        else p = nullptr;
         return e;
     }
     template <class T> T* as() const { return static_cast<T*>(p); }
@@ -55,6 +73,9 @@ struct Context {
     std::mutex mu;
     std::unordered_map<std::string, std::shared_ptr<Plan>> plan_cache;
     std::map<int, std::shared_ptr<CrtSet>> crt_std;  // CRT tables of the standard primes
+    std::mutex cache_mu;
+    std::multimap<size_t, void*> cache;   // free device blocks by size
+    size_t cached_bytes = 0;
 };
 
 Context* ctx();           // nullptr before dr_init
@@ -142,6 +163,7 @@ struct Batch {
     bool stamping = false;
     float last_ms = 0.f;
     bool has_shadow = false;
+    Batch();
     ~Batch();
 };
 

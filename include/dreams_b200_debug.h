@@ -40,6 +40,11 @@ int dr_bench_int_peak(int32_t kind, double *lane_ops_per_s);
 int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t *n_launches,
                             float *spans);
 
+/* Host milliseconds (cumulative from the start) at the end of each phase of
+ * the last dr_batch_create: programs, walks, tiles, shadow lists, launch
+ * geometry, allocation and upload, final synchronisation (7 values). */
+int dr_debug_build_phases(double *ms, int32_t n);
+
 /* The FP64 shadow's rescale division on the device: out[i] = x[i] / b[i]
  * rounded to nearest through the same code path the shadow kernels use
  * (Markstein correction, IEEE fallback).  Host buffers; b[i] > 1e10. */
