@@ -320,7 +320,41 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     build_mark(2);
     // ---- tiles and groups
     const bool plain = engine == DR_ENGINE_PLAIN;
-    const uint32_t chunk = plain ? 0xffffffffu : chunk_policy(total_group_steps, n_groups, C.sms, tune);
+    // workload shape for the autotuner: per launch key, log2 buckets of the
+    // (walk, prime block) count and of their steps, plus the longest walk
+    {
+        std::map<LaunchKey, std::pair<uint64_t, uint64_t>> shape;
+        uint64_t longest = 0;
+        for (int32_t w = 0; w < n_walks; ++w) {
+            const DevWalk& W = dwalks[w];
+            const DevProgram& G = dprogs[W.prog];
+            const Plan& P = *plans[W.prog];
+            LaunchKey key{0, G.cls, G.m, 0};
+            if (G.cls != CLS_INTERP) key.D = (uint32_t)template_degree(P.cls, P.m, P.degree);
+            const uint64_t nb = (W.K + 31) / 32;
+            shape[key].first += nb;
+            shape[key].second += nb * W.depth;
+            longest = std::max<uint64_t>(longest, W.depth);
+        }
+        auto lg = [](uint64_t v) { int b = 0; while (v > 1) { v >>= 1; ++b; } return b; };
+        std::string sig = std::to_string(lg(longest)) + (B->has_shadow ? "s" : "n");
+        for (auto& kv : shape)
+            sig += "|" + std::to_string(kv.first.cls) + "," + std::to_string(kv.first.m) + "," +
+                   std::to_string(kv.first.D) + ":" + std::to_string(lg(kv.second.first)) + "," +
+                   std::to_string(lg(kv.second.second));
+        B->signature = sig;
+    }
+    // an autotuned choice for this shape applies unless the caller fixed one
+    uint32_t tuned_chunk = 0, tuned_wpb = 0;
+    if (!plain && !(tune && (tune->chunk_steps || tune->warps_per_block))) {
+        std::lock_guard<std::mutex> lk(C.cache_mu);
+        auto it = C.tuned.find(B->signature);
+        if (it != C.tuned.end()) std::tie(tuned_chunk, tuned_wpb) = it->second;
+    }
+    const uint32_t chunk = plain ? 0xffffffffu
+                         : tuned_chunk ? tuned_chunk
+                         : chunk_policy(total_group_steps, n_groups, C.sms, tune);
+    B->chunk_used = chunk;
     std::map<LaunchKey, std::vector<DevTile>> tile_sets;
     std::vector<DevGroup> groups;
     uint32_t slots = 0;
@@ -469,7 +503,9 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
 
     build_mark(4);
     // ---- launch geometry
-    const int wpb = (tune && tune->warps_per_block) ? (int)tune->warps_per_block : 4;
+    const int wpb = (tune && tune->warps_per_block) ? (int)tune->warps_per_block
+                  : tuned_wpb ? (int)tuned_wpb : 4;
+    B->wpb_used = (uint32_t)wpb;
     uint32_t q = 0;
     for (LaunchSpec& L : B->launches) {
         L.queue = q++;
@@ -1321,6 +1357,79 @@ int dr_batch_read_pipeline(int32_t batch, double* delta, int32_t* topk_idx, doub
         }
     }
     if (signs) DR_CUDA(cudaMemcpy(signs, B->signs.p, 4ull * 4 * n, cudaMemcpyDeviceToHost));
+    return DR_OK;
+}
+
+// Autotuner: time candidate depth-chunk lengths and warps per block on the
+// batch itself (graph replays, CUDA events, best of three after a capture
+// run) and remember the fastest for batches of the same shape.
+int dr_autotune(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs,
+                const uint64_t* blob_offsets, int32_t n_programs, const int64_t* axis_params,
+                uint64_t n_axis_params, dr_tune* best, float* best_ms) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    if (!best) return DR_ERR_ARG;
+    Context& C = *g_ctx;
+    uint64_t n_res = 0;
+    for (int32_t w = 0; w < n_walks; ++w) {
+        n_res = std::max<uint64_t>(n_res, walks[w].res_offset + walks[w].K);
+        if (walks[w].checkpoint) n_res = std::max<uint64_t>(n_res, walks[w].cp_res_offset + walks[w].K);
+    }
+    auto time_one = [&](const dr_tune& t, float* ms, uint32_t* chunk_used, std::string* sig) -> int {
+        std::unique_ptr<Batch> B;
+        int r = batch_build(walks, n_walks, blobs, blob_offsets, n_programs, axis_params, n_axis_params,
+                            &t, n_res, &B);
+        if (r) return r;
+        if (chunk_used) *chunk_used = B->chunk_used;
+        if (sig) *sig = B->signature;
+        if ((r = batch_run(*B, C.stream))) return r;
+        float m = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            if ((r = batch_run(*B, C.stream))) return r;
+            DR_CUDA(cudaEventSynchronize(B->ev1));
+            float x = 0.f;
+            cudaEventElapsedTime(&x, B->ev0, B->ev1);
+            m = std::min(m, x);
+        }
+        *ms = m;
+        return DR_OK;
+    };
+    // the default policy's chunk anchors the candidates
+    dr_tune t{};
+    t.engine = best->engine;
+    t.shadow_buffer_mb = best->shadow_buffer_mb;
+    t.warps_per_block = 4;
+    uint32_t c0 = 0;
+    std::string sig;
+    float ms0 = 0.f;
+    if ((rc = time_one(t, &ms0, &c0, &sig))) return rc;
+    dr_tune bt = t;
+    bt.chunk_steps = c0;
+    float bms = ms0;
+    for (uint32_t f : {1u, 2u, 4u}) {
+        for (uint32_t wpb : {1u, 2u, 4u}) {   // k_walk is compiled for at most 128 threads
+            for (int dir = 0; dir < 2; ++dir) {
+                if (f == 1 && dir == 1) continue;
+                const uint64_t c = dir == 0 ? (uint64_t)c0 * f : (uint64_t)c0 / f;
+                if (c < 256 || c > 4194304 || (f == 1 && wpb == 4)) continue;
+                dr_tune cand = t;
+                cand.chunk_steps = (uint32_t)c;
+                cand.warps_per_block = wpb;
+                float ms = 0.f;
+                rc = time_one(cand, &ms, nullptr, nullptr);
+                if (rc == DR_ERR_UNSUPPORTED) continue;   // e.g. shared memory of a wider block
+                if (rc) return rc;
+                if (ms < bms) { bms = ms; bt = cand; }
+            }
+        }
+    }
+    {
+        std::lock_guard<std::mutex> lk(C.cache_mu);
+        C.tuned[sig] = {bt.chunk_steps, bt.warps_per_block};
+    }
+    best->chunk_steps = bt.chunk_steps;
+    best->warps_per_block = bt.warps_per_block;
+    if (best_ms) *best_ms = bms;
     return DR_OK;
 }
 

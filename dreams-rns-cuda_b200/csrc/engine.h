@@ -73,6 +73,7 @@ struct Context {
     std::mutex mu;
     std::unordered_map<std::string, std::shared_ptr<Plan>> plan_cache;
     std::map<int, std::shared_ptr<CrtSet>> crt_std;  // CRT tables of the standard primes
+    std::map<std::string, std::pair<uint32_t, uint32_t>> tuned;   // signature -> (chunk, warps/block)
     std::mutex cache_mu;
     std::multimap<size_t, void*> cache;   // free device blocks by size
     size_t cached_bytes = 0;
@@ -163,6 +164,8 @@ struct Batch {
     bool stamping = false;
     float last_ms = 0.f;
     bool has_shadow = false;
+    std::string signature;              // autotuner cache key (workload shape)
+    uint32_t chunk_used = 0, wpb_used = 0;
     Batch();
     ~Batch();
 };

@@ -235,6 +235,20 @@ def sweep(reqs: Sequence[WalkRequest], delta: Optional[str] = None,
         b.close()
 
 
+def autotune(reqs: Sequence[WalkRequest]) -> dict:
+    """Time candidate launch shapes (depth-chunk length, warps per block) on
+    these walks and remember the fastest for every later batch of the same
+    workload shape.  Returns the choice and its time per run."""
+    N.init()
+    pk = _Packed(list(reqs))
+    t = _tune()
+    ms = ctypes.c_float()
+    N.check(N.lib().dr_autotune(N.ptr(pk.desc), pk.n, N.ptr(pk.blobs), N.ptr(pk.offsets),
+                                pk.n_programs, N.ptr(pk.axis), pk.n_axis, ctypes.byref(t),
+                                ctypes.byref(ms)), "dr_autotune")
+    return {"chunk_steps": t.chunk_steps, "warps_per_block": t.warps_per_block, "ms": ms.value}
+
+
 class WalkBatch:
     """A batch of walks prepared once and resident on the device."""
 

@@ -165,6 +165,18 @@ int dr_batch_read_pipeline(int32_t batch, double *delta, int32_t *topk_idx, doub
                            uint32_t *limbs, int32_t *signs, int32_t limb_stride);
 int dr_batch_destroy(int32_t batch);
 
+/* Autotuner: builds the given walks with candidate depth-chunk lengths and
+ * warps per block around the built-in policy, times each as a graph replay
+ * (best of three, CUDA events), and returns the fastest in *best (its engine
+ * and shadow_buffer_mb fields are inputs).  The choice is remembered for the
+ * workload's shape (per launch class: log2 of the (walk, prime block) count
+ * and of their steps, longest walk), so later batches of that shape built
+ * with a zero chunk_steps and warps_per_block use it.  No reference
+ * counterpart (the reference fixes its launch shape, persistent_kernel.cu:877-888). */
+int dr_autotune(const dr_walk_desc *walks, int32_t n_walks, const uint8_t *blobs,
+                const uint64_t *blob_offsets, int32_t n_programs, const int64_t *axis_params,
+                uint64_t n_axis_params, dr_tune *best, float *best_ms);
+
 /* Where a batch's time goes: runs every launch group of the batch alone, one
  * after another, timing each with CUDA events (walk kernels: kind 0; FP64
  * shadow: kind 1 interpreted, kind 2 integer differences).  ms: the launch

@@ -347,3 +347,19 @@ def test_sweep_matches_walks_crt_and_delta():
         assert (out["delta"][i] == d) if math.isinf(d) else abs(out["delta"][i] - d) < 1e-9
     order = sorted(range(len(reqs)), key=lambda i: (-out["delta"][i], i))[:7]
     assert list(out["topk_idx"]) == order
+
+
+def test_autotune_keeps_results():
+    """The autotuner only changes launch shapes: a batch built after tuning
+    (which then uses the remembered shape) gives the same residues."""
+    ws = dr.synth.uniform_pcfs(256, seed=31, depth=700, limit_depth=2100)
+    reqs = [pcf_request(dr.compile_pcf(w.a, w.b), w.a0, 2100, 32, checkpoint=700) for w in ws]
+    before = run_walks(reqs)
+    choice = dr.autotune(reqs)
+    assert choice["chunk_steps"] >= 256 and choice["warps_per_block"] in (1, 2, 4)
+    assert choice["ms"] > 0
+    after = run_walks(reqs)
+    for x, y in zip(before, after):
+        assert list(x["p_residues"]) == list(y["p_residues"])
+        assert list(x["checkpoint"]["q_residues"]) == list(y["checkpoint"]["q_residues"])
+        assert x["p_float"] == y["p_float"]
