@@ -145,13 +145,12 @@ class ClockSampler:
 
 # ---- roofline accounting ------------------------------------------------------
 
-def algorithmic_int_ops(info, K_, depth):
+def algorithmic_int_ops(info, K_, depth, m=2):
     """Integer lane-instructions one walk needs with the difference-table
     companion algorithm: per prime-step, D modular additions per stream
     (add + min) and for each of the m last-column entries m wide multiply-adds,
     2 per extra product beyond two (fold), and a Montgomery reduction (2 wide
     multiplies + add + min)."""
-    m = 2
     D = max(info["degree"], 1)
     per = 2 * m * D + m * (m + 2 * max(0, m - 2) + 4)
     return per * K_ * depth
@@ -234,7 +233,21 @@ def bench_cmf3(stream, torch, n_walks=16384):
         plain_ms.append(_time_batch(b, stream, torch, reps=1))
         b.close()
     plain_rate = 5000 * 64 / (statistics.median(plain_ms) * 1e-3)
+    # integer-pipe roofline of the walk kernels on this sweep (no shadow)
+    import ctypes
+    walk_only = WalkBatch([cmf_request(kb[w.program_key], w.depth, w.K, w.shifts, w.trajectory, shadow=False)
+                           for w in ws])
+    walk_ms = _time_batch(walk_only, stream, torch, reps=5)
+    walk_only.close()
+    infos = {k: N.program_info(b) for k, b in kb.items()}
+    ops = sum(algorithmic_int_ops(infos[w.program_key], w.K, w.depth, m=3) for w in ws)
+    peak = ctypes.c_double()
+    N.check(N.lib().dr_bench_int_peak(2, ctypes.byref(peak)), "int peak")
+    roof = {"bound": "int", "achieved": ops / (walk_ms * 1e-3) / 1e12, "peak": peak.value / 1e12,
+            "unit": "Tops/s", "frac": ops / (walk_ms * 1e-3) / peak.value, "kernel_ms": walk_ms,
+            "classes": sorted({(i["class"], i["degree"]) for i in infos.values()})}
     return {"walks": len(reqs), "prime_steps": st["prime_steps"], "ms": ms, "prime_steps_per_s": rate,
+            "walk_roofline": roof,
             "autotuned": tuned,
             "plain_one_walk_per_launch_prime_steps_per_s": plain_rate,
             "batched_over_plain": rate / plain_rate}

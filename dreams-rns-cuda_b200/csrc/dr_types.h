@@ -44,7 +44,8 @@ struct DevWalk {
     uint64_t axis_off;                 // into the int64 axis parameter array
     uint64_t res_off, cp_res_off;      // residue output offsets
     uint32_t shadow_mode;              // 0 none, 1 interpret, 2 integer differences
-    uint32_t pad;
+    uint32_t p_row;                    // row (state-vector walk: entry) of p
+    uint64_t vec_off;                  // state-vector walk: v(0) in the axis array
 };
 
 // One unit of walk work: a depth chunk of one (walk, prime block).

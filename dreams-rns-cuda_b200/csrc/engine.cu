@@ -262,7 +262,18 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         if (W.program >= (uint32_t)n_programs) { set_error("walk program index out of range"); return DR_ERR_ARG; }
         const DevProgram& G = dprogs[W.program];
         if (W.K < 1 || W.K > DR_MAX_K) { set_error("K outside 1..DR_MAX_K"); return DR_ERR_UNSUPPORTED; }
-        if (W.q_row >= G.m) { set_error("q_row >= m"); return DR_ERR_ARG; }
+        if (W.q_row >= G.m || W.p_row >= G.m) { set_error("p_row or q_row >= m"); return DR_ERR_ARG; }
+        if (W.flags & DR_WALK_VEC) {
+            if (W.flags & DR_WALK_INIT_PCF) {
+                set_error("a state-vector walk starts from v(0), not the PCF initial matrix");
+                return DR_ERR_ARG;
+            }
+            if (W.checkpoint) { set_error("state-vector walks have no checkpoint"); return DR_ERR_UNSUPPORTED; }
+            if (W.vec_offset + (uint64_t)G.m * W.K + G.m > n_axis) {
+                set_error("state-vector initial values out of range of the axis parameters");
+                return DR_ERR_ARG;
+            }
+        }
         if (W.checkpoint && W.checkpoint >= W.depth) { set_error("checkpoint must be < depth"); return DR_ERR_ARG; }
         if ((W.flags & DR_WALK_INIT_PCF) && G.m < 2) { set_error("PCF initial matrix needs m >= 2"); return DR_ERR_ARG; }
         if (W.res_offset + W.K > n_res || (W.checkpoint && W.cp_res_offset + W.K > n_res)) {
@@ -299,12 +310,14 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         d.axis_off = W.axis_offset;
         d.res_off = W.res_offset;
         d.cp_res_off = W.cp_res_offset;
+        d.p_row = W.p_row;
+        d.vec_off = W.vec_offset;
         d.shadow_mode = SHADOW_NONE;
         if (W.flags & DR_WALK_SHADOW) {
             d.shadow_mode = SHADOW_INTERP;
             const Plan& P = *plans[W.program];
             const int Dt = template_degree(P.cls, P.m, P.degree);
-            if (G.shadow_fd && G.cls != CLS_INTERP && Dt > 0) {
+            if (G.shadow_fd && G.cls != CLS_INTERP && Dt > 0 && !(W.flags & DR_WALK_VEC)) {
                 const double b = float_bound_log2(P, axis + W.axis_offset, W.depth + 1);
                 if (b < 53.0 && b + Dt < 61.0) d.shadow_mode = SHADOW_INTFD;
             }
@@ -448,7 +461,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         if (W.shadow_mode == SHADOW_INTFD)
             shadow_sets[LaunchKey{2, P.cls, P.m, (uint32_t)template_degree(P.cls, P.m, P.degree)}].push_back(w);
         else
-            shadow_sets[LaunchKey{1, G.fcomp, G.m, 0}].push_back(w);
+            shadow_sets[LaunchKey{1, G.fcomp | ((W.flags & DR_WALK_VEC) ? 2u : 0u), G.m, 0}].push_back(w);
     }
     std::vector<DevShadowSeg> shadow_list;
     std::vector<uint32_t> eval_items;
@@ -471,7 +484,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         if (kv.first.kind == 1) {
             // interpreted: the step-matrix buffer holds every step of every
             // walk when it fits under the cap, else the walks run in rounds
-            const uint32_t ne = shadow_entries(kv.first.m, kv.first.cls != 0);
+            const uint32_t ne = shadow_entries(kv.first.m, (kv.first.cls & 1u) != 0);
             uint64_t need = 0;
             for (uint32_t w : v) need += dwalks[w].depth * ne;
             uint64_t round = UINT64_MAX;
@@ -482,7 +495,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             std::vector<DevShadowSeg> segs;
             for (uint32_t w : v) segs.push_back(DevShadowSeg{w, kNoState, 0, dwalks[w].depth, 0, 0, 0});
             mf_doubles += shadow_interp_plan(B->launches, shadow_list, eval_items, segs, kv.first.m,
-                                             kv.first.cls != 0, rr, mf_doubles, round, state_slots);
+                                             kv.first.cls, rr, mf_doubles, round, state_slots);
             if (round != UINT64_MAX) state_slots += (uint32_t)v.size();
             continue;
         }
@@ -611,15 +624,15 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
 
 uint64_t shadow_interp_plan(std::vector<LaunchSpec>& launches, std::vector<DevShadowSeg>& list,
                             std::vector<uint32_t>& eval_items, const std::vector<DevShadowSeg>& segs,
-                            uint32_t m, bool comp, uint32_t rows_regs, uint64_t mf_base,
+                            uint32_t m, uint32_t shape, uint32_t rows_regs, uint64_t mf_base,
                             uint64_t round_steps, uint32_t slot_base) {
-    const uint32_t ne = shadow_entries(m, comp);
+    const uint32_t ne = shadow_entries(m, (shape & 1u) != 0);
     const bool rounds = round_steps != UINT64_MAX;
     uint64_t region = 0;
     for (uint64_t r = 0;; ++r) {
         LaunchSpec L{};
         L.kind = 1;
-        L.cls = comp ? 1u : 0u;
+        L.cls = shape;
         L.m = m;
         L.follow = r > 0;
         L.off = (uint32_t)list.size();
@@ -711,9 +724,9 @@ int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevSh
     }
     L.grid = std::max(1, std::min((int)((L.items + wpb - 1) / wpb), occ * sms));
     L.block2 = 32 * kChainWarps;
-    L.smem2 = shadow_chain_smem(L.m, L.cls != 0) * kChainWarps;
+    L.smem2 = shadow_chain_smem(L.m, (L.cls & 1u) != 0) * kChainWarps;
     if (whole_sm) L.smem2 = std::max(L.smem2, chain_hog_smem());
-    e = shadow_chain_dispatch(L.m, L.cls != 0, 0, L.block2, L.smem2, nullptr, sa, &occ);
+    e = shadow_chain_dispatch(L.m, L.cls, 0, L.block2, L.smem2, nullptr, sa, &occ);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
     if (occ < 1) {
         set_error("kernel cannot be resident with this shared memory size");
@@ -740,7 +753,7 @@ cudaError_t launch_shadow_interp(const LaunchSpec& L, ShadowArgs sa, uint32_t* q
     sa.n_items = L.items2;
     sa.queue = queues + L.queue2;
     if (sa.tstamp) sa.tstamp += 2;
-    return shadow_chain_dispatch(L.m, L.cls != 0, L.grid2, L.block2, L.smem2, s, sa, nullptr);
+    return shadow_chain_dispatch(L.m, L.cls, L.grid2, L.block2, L.smem2, s, sa, nullptr);
 }
 
 static CrtTables tables_of(const CrtSet& S);
@@ -964,7 +977,7 @@ int batch_profile(Batch& B, std::vector<float>* ms, std::vector<float>* ms2) {
             if (e == cudaSuccess) {
                 sa.n_items = L.items2;
                 sa.queue = B.queues.as<uint32_t>() + L.queue2;
-                e = shadow_chain_dispatch(L.m, L.cls != 0, L.grid2, L.block2, L.smem2, st, sa, nullptr);
+                e = shadow_chain_dispatch(L.m, L.cls, L.grid2, L.block2, L.smem2, st, sa, nullptr);
             }
         } else {
             if (L.items) e = launch_one(B, L, wa, sa, st);

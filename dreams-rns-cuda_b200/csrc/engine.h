@@ -91,7 +91,7 @@ int crt_limbs_for(int K);  // L: limbs of prod(moduli) + 1
 
 struct LaunchSpec {
     int kind;                  // 0 walk, 1 shadow (interpreted), 2 shadow (integer differences)
-    uint32_t cls, m, D;        // kind 1: cls = 1 when the float matrix has the companion shape
+    uint32_t cls, m, D;        // kind 1: cls bit 0 companion-shaped float matrix, bit 1 state vectors
     uint32_t off, count;       // tiles / list entries of this launch
     uint32_t items;            // work items (tiles, evaluation items or 32-walk groups)
     uint32_t queue;            // queue counter index
@@ -122,7 +122,8 @@ constexpr int kChainWarps = 4;
 int chain_blocks(const DevShadowSeg* segs, uint32_t count);
 size_t chain_hog_smem();
 
-// Builds the interpreted-shadow launches of one (m, companion-shape) group:
+// Builds the interpreted-shadow launches of one (m, shape) group (shape bit 0:
+// companion-shaped float matrix, bit 1: state-vector walks):
 // segs (sorted longest first) become one launch, or several rounds of at most
 // `round_steps` steps with resident state slots from slot_base (round_steps =
 // UINT64_MAX: one launch, the segments' own state slots).  Appends to list and
@@ -130,7 +131,7 @@ size_t chain_hog_smem();
 // (its segments' mf_off start at mf_base).
 uint64_t shadow_interp_plan(std::vector<LaunchSpec>& launches, std::vector<DevShadowSeg>& list,
                             std::vector<uint32_t>& eval_items, const std::vector<DevShadowSeg>& segs,
-                            uint32_t m, bool comp, uint32_t rows_regs, uint64_t mf_base,
+                            uint32_t m, uint32_t shape, uint32_t rows_regs, uint64_t mf_base,
                             uint64_t round_steps, uint32_t slot_base);
 
 struct Batch {

@@ -54,7 +54,8 @@ cudaError_t walk_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int bl
 // interpreted shadow: evaluation (U sub-blocks per pass) and chain kernels
 cudaError_t shadow_eval_dispatch(uint32_t U, int grid, int block, size_t smem, cudaStream_t st,
                                  const ShadowArgs& a, int* occ);
-cudaError_t shadow_chain_dispatch(uint32_t m, bool comp, int grid, int block, size_t smem,
+// flags: bit 0 companion-shaped step matrices, bit 1 state-vector walks
+cudaError_t shadow_chain_dispatch(uint32_t m, uint32_t flags, int grid, int block, size_t smem,
                                   cudaStream_t st, const ShadowArgs& a, int* occ);
 size_t shadow_chain_smem(uint32_t m, bool comp);
 cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block,

@@ -199,6 +199,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
         const uint32_t wi = (uint32_t)walks.size();
         DevWalk w{};
         w.prog = (uint32_t)pi; w.K = r->d.K; w.flags = r->d.flags; w.q_row = r->d.q_row;
+        w.p_row = r->d.p_row;
         w.a0 = r->d.a0; w.depth = r->d.depth; w.checkpoint = 0;
         w.axis_off = axis.size();
         axis.insert(axis.end(), r->axis.begin(), r->axis.end());
@@ -300,7 +301,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
             std::stable_sort(v.begin(), v.end(), [](const DevShadowSeg& x, const DevShadowSeg& y) {
                 return (x.s1 - x.s0) > (y.s1 - y.s0);
             });
-            mf_doubles += shadow_interp_plan(L, segs, eval_items, v, m, cls != 0, rr, mf_doubles,
+            mf_doubles += shadow_interp_plan(L, segs, eval_items, v, m, cls, rr, mf_doubles,
                                              UINT64_MAX, 0);
             continue;
         }
@@ -574,7 +575,11 @@ int dr_serve_submit(int32_t server, const dr_walk_desc* walk, const uint8_t* blo
     const Plan& P = *r->plan;
     if (P.m > (uint32_t)kServeMaxM) { set_error("serving supports m <= 4"); return DR_ERR_UNSUPPORTED; }
     if (walk->K < 1 || walk->K > DR_MAX_K) return DR_ERR_UNSUPPORTED;
-    if (walk->q_row >= P.m) return DR_ERR_ARG;
+    if (walk->q_row >= P.m || walk->p_row >= P.m) return DR_ERR_ARG;
+    if (walk->flags & DR_WALK_VEC) {
+        set_error("serving does not take state-vector walks");
+        return DR_ERR_UNSUPPORTED;
+    }
     if (walk->checkpoint) { set_error("serving walks take no checkpoint"); return DR_ERR_ARG; }
     if ((walk->flags & DR_WALK_INIT_PCF) && P.m < 2) return DR_ERR_ARG;
     if (P.dim && !axis_params) return DR_ERR_ARG;

@@ -15,12 +15,14 @@ cudaError_t shadow_eval_dispatch(uint32_t U, int grid, int block, size_t smem, c
     }
 }
 
-cudaError_t shadow_chain_dispatch(uint32_t m, bool comp, int grid, int block, size_t smem,
+cudaError_t shadow_chain_dispatch(uint32_t m, uint32_t flags, int grid, int block, size_t smem,
                                   cudaStream_t st, const ShadowArgs& a, int* occ) {
-    switch (m * 2 + (comp ? 1 : 0)) {
+    switch (m * 4 + (flags & 3u)) {
 #define DR_X(M_, D_) \
-    case M_ * 2: return run_kernel(k_shadow_chain<M_, false>, grid, block, smem, st, a, occ); \
-    case M_ * 2 + 1: return run_kernel(k_shadow_chain<M_, true>, grid, block, smem, st, a, occ);
+    case M_ * 4: return run_kernel(k_shadow_chain<M_, 0>, grid, block, smem, st, a, occ); \
+    case M_ * 4 + 1: return run_kernel(k_shadow_chain<M_, 1>, grid, block, smem, st, a, occ); \
+    case M_ * 4 + 2: return run_kernel(k_shadow_chain<M_, 2>, grid, block, smem, st, a, occ); \
+    case M_ * 4 + 3: return run_kernel(k_shadow_chain<M_, 3>, grid, block, smem, st, a, occ);
         DR_INTERP_INSTANCES(DR_X)
 #undef DR_X
         default: return cudaErrorInvalidValue;

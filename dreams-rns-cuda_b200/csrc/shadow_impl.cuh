@@ -29,6 +29,8 @@
 #pragma once
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "../../include/dreams_b200.h"
 #include "dr_types.h"
 #include "interp.cuh"
@@ -82,35 +84,34 @@ __device__ __forceinline__ int bexp(double x) { return (__double2hiint(x) >> 20)
 // only exponent bits of the inputs, so it completes on the integer pipe
 // while the reciprocal is in flight.  q takes the sign of x, which keeps the
 // sign of a zero.
-template <int M_>
-__device__ __forceinline__ void rescale(double (&P)[M_][M_], double mx) {
+template <int N_>
+__device__ __forceinline__ void rescale_n(double (&P)[N_], double mx) {
     const double y = __drcp_rn(mx);
     const int em = bexp(mx);
     const int t_hi = max(60, em - 1000) << 20;
     bool slow = em >= 2045;
 #pragma unroll
-    for (int i = 0; i < M_; ++i)
-#pragma unroll
-        for (int j = 0; j < M_; ++j) {
-            const int ahi = __double2hiint(P[i][j]) & 0x7fffffff;
-            slow |= (ahi < t_hi) & ((ahi | __double2loint(P[i][j])) != 0);
-        }
+    for (int i = 0; i < N_; ++i) {
+        const int ahi = __double2hiint(P[i]) & 0x7fffffff;
+        slow |= (ahi < t_hi) & ((ahi | __double2loint(P[i])) != 0);
+    }
     if (__builtin_expect(slow, 0)) {
 #pragma unroll
-        for (int i = 0; i < M_; ++i)
-#pragma unroll
-            for (int j = 0; j < M_; ++j) P[i][j] = div_slow(P[i][j], mx);
+        for (int i = 0; i < N_; ++i) P[i] = div_slow(P[i], mx);
         return;
     }
 #pragma unroll
-    for (int i = 0; i < M_; ++i)
-#pragma unroll
-        for (int j = 0; j < M_; ++j) {
-            const double x = P[i][j];
-            const double q0 = __dmul_rn(x, y);
-            const double r = __fma_rn(-q0, mx, x);
-            P[i][j] = copysign(__fma_rn(r, y, q0), x);
-        }
+    for (int i = 0; i < N_; ++i) {
+        const double x = P[i];
+        const double q0 = __dmul_rn(x, y);
+        const double r = __fma_rn(-q0, mx, x);
+        P[i] = copysign(__fma_rn(r, y, q0), x);
+    }
+}
+
+template <int M_>
+__device__ __forceinline__ void rescale(double (&P)[M_][M_], double mx) {
+    rescale_n<M_ * M_>(reinterpret_cast<double (&)[M_ * M_]>(P), mx);
 }
 
 // sc_m * 2^sc_e *= mx with sc_m kept in [0.5, 1) (frexp by exponent bits: the
@@ -231,7 +232,8 @@ struct FChain {
         st[66] = nan_seen ? 1.0 : 0.0;
     }
     // start of a segment: the walk's initial matrix at step 0, else the state
-    __device__ __forceinline__ void begin(const DevWalk& W, const DevShadowSeg& g, const double* state) {
+    __device__ __forceinline__ void begin(const DevWalk& W, const DevShadowSeg& g, const double* state,
+                                          const int64_t* /*axis*/) {
         if (g.s0 == 0 || g.state == kNoState) init(W);
         else load(state + (size_t)g.state * kShadowStateStride);
     }
@@ -246,13 +248,122 @@ struct FChain {
         }
     }
     __device__ __forceinline__ void write(double* out, const DevWalk& W) const {
-        double q = P[0][M_ - 1];
+        double p = P[0][M_ - 1], q = P[0][M_ - 1];
 #pragma unroll
-        for (int i = 0; i < M_; ++i)
+        for (int i = 0; i < M_; ++i) {
+            if ((uint32_t)i == W.p_row) p = P[i][M_ - 1];
             if ((uint32_t)i == W.q_row) q = P[i][M_ - 1];
-        out[0] = P[0][M_ - 1];
+        }
+        out[0] = p;
         out[1] = q;
         out[2] = __dadd_rn(log(sc_m), (double)sc_e * 0.69314718055994530942);
+    }
+};
+
+// State-vector shadow (reference cmf_walk.py:514-522): v <- M_f(s) @ v in
+// increasing s, then v /= max|v| when that exceeds 1e10.  numpy's float64
+// matrix @ vector goes through BLAS gemv; the summation order below is the one
+// the reference's numpy/OpenBLAS produced for m = 2, 3, 4 (checked against
+// numpy on random inputs): m = 2: a1*v1 then fma(a0, v0, .); m = 3: the same
+// then fma(a2, v2, .); m = 4: (a0v0 + a2v2) + (a1v1 + a3v3) with rounded
+// products; other m: a0*v0 then fma(a_k, v_k, .).  A NaN anywhere in v
+// reaches every new entry (NaN * x is NaN), so the new entries decide the
+// NaN case.
+template <int M_>
+struct FVec {
+    double v[M_];
+    double sc_m;
+    int sc_e;
+    bool nan_seen;
+
+    __device__ __forceinline__ void init(const DevWalk& W, const int64_t* axis) {
+        const int64_t* f = axis + W.vec_off + (uint64_t)M_ * W.K;
+#pragma unroll
+        for (int i = 0; i < M_; ++i) v[i] = __longlong_as_double(__ldg(f + i));
+        sc_m = 1.0;
+        sc_e = 0;
+        nan_seen = false;
+    }
+    __device__ __forceinline__ static double dot(const double* a, const double* x) {
+        if (M_ == 1) return __dmul_rn(a[0], x[0]);
+        if (M_ == 2) return __fma_rn(a[0], x[0], __dmul_rn(a[1], x[1]));
+        if (M_ == 3) return __fma_rn(a[2], x[2], __fma_rn(a[0], x[0], __dmul_rn(a[1], x[1])));
+        if (M_ == 4)
+            return __dadd_rn(__dadd_rn(__dmul_rn(a[0], x[0]), __dmul_rn(a[2], x[2])),
+                             __dadd_rn(__dmul_rn(a[1], x[1]), __dmul_rn(a[3], x[3 % M_])));
+        double c = __dmul_rn(a[0], x[0]);
+#pragma unroll
+        for (int k = 1; k < M_; ++k) c = __fma_rn(a[k], x[k], c);
+        return c;
+    }
+    __device__ __forceinline__ void step(const double (&X)[M_][M_]) {
+        double w[M_];
+        double mx = 0.0;
+        bool has_nan = false;
+#pragma unroll
+        for (int i = 0; i < M_; ++i) {
+            w[i] = dot(X[i], v);
+            has_nan |= w[i] != w[i];
+            mx = fmax(mx, fabs(w[i]));
+        }
+#pragma unroll
+        for (int i = 0; i < M_; ++i) v[i] = w[i];
+        if (!has_nan && mx > 1e10) {
+            rescale_n<M_>(v, mx);
+            scale_acc(sc_m, sc_e, mx);
+        }
+        nan_seen |= has_nan;
+    }
+    // companion-shaped step matrix from its last column: the dense product
+    // with the exact 0 and 1 entries
+    __device__ __forceinline__ void step_companion(const double (&c)[M_]) {
+        double X[M_][M_];
+#pragma unroll
+        for (int i = 0; i < M_; ++i)
+#pragma unroll
+            for (int j = 0; j < M_; ++j) X[i][j] = (j == M_ - 1) ? c[i] : (i == j + 1 ? 1.0 : 0.0);
+        step(X);
+    }
+    __device__ __forceinline__ void load(const double* st) {
+#pragma unroll
+        for (int i = 0; i < M_; ++i) v[i] = st[i];
+        sc_m = st[64];
+        sc_e = (int)st[65];
+        nan_seen = st[66] != 0.0;
+    }
+    __device__ __forceinline__ void store(double* st) const {
+#pragma unroll
+        for (int i = 0; i < M_; ++i) st[i] = v[i];
+        st[64] = sc_m;
+        st[65] = (double)sc_e;
+        st[66] = nan_seen ? 1.0 : 0.0;
+    }
+    __device__ __forceinline__ void begin(const DevWalk& W, const DevShadowSeg& g, const double* state,
+                                          const int64_t* axis) {
+        if (g.s0 == 0 || g.state == kNoState) init(W, axis);
+        else load(state + (size_t)g.state * kShadowStateStride);
+    }
+    __device__ __forceinline__ void write(double* out, const DevWalk& W) const {
+        double p = v[0], q = v[0];
+#pragma unroll
+        for (int i = 0; i < M_; ++i) {
+            if ((uint32_t)i == W.p_row) p = v[i];
+            if ((uint32_t)i == W.q_row) q = v[i];
+        }
+        out[0] = p;
+        out[1] = q;
+        out[2] = __dadd_rn(log(sc_m), (double)sc_e * 0.69314718055994530942);
+    }
+    __device__ __forceinline__ void end(const DevWalk& W, const DevShadowSeg& g, double* state,
+                                        double* shadow, uint32_t* status, uint32_t w) const {
+        if (g.s1 >= W.depth || g.state == kNoState) {
+            write(shadow + 3 * (size_t)w, W);
+            double pq[3];
+            write(pq, W);
+            if (nan_seen || !isfinite(pq[0])) atomicOr(status + w, DR_STATUS_SHADOW_NAN);
+        } else {
+            store(state + (size_t)g.state * kShadowStateStride);
+        }
     }
 };
 
@@ -337,8 +448,8 @@ __global__ void __launch_bounds__(128) k_shadow_eval(const ShadowArgs A) {
     stamp_end(A.tstamp);
 }
 
-template <int M_, bool COMP>
-__device__ __forceinline__ void chain_step(FChain<M_>& ch, const double (&X)[COMP ? M_ : M_ * M_]) {
+template <int M_, bool COMP, class Chain>
+__device__ __forceinline__ void chain_step(Chain& ch, const double (&X)[COMP ? M_ : M_ * M_]) {
     if (COMP) {
         double cv[M_];
 #pragma unroll
@@ -358,8 +469,13 @@ __device__ __forceinline__ void chain_step(FChain<M_>& ch, const double (&X)[COM
 // ([buffer][step][entry][lane]) while the current chunk runs; every lane only
 // reads what it copied itself, so the per-thread cp.async group wait is the
 // only synchronisation.
-template <int M_, bool COMP>
+// FLAGS: bit 0 the float step matrix has the companion shape (only its last
+// column is stored), bit 1 state-vector walks.
+template <int M_, int FLAGS>
 __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
+    constexpr bool COMP = (FLAGS & 1) != 0;
+    constexpr bool VEC = (FLAGS & 2) != 0;
+    using Chain = typename std::conditional<VEC, FVec<M_>, FChain<M_>>::type;
     constexpr int NE = COMP ? M_ : M_ * M_;
     constexpr int CS = chain_chunk_steps(NE);
     extern __shared__ double dsm_all[];
@@ -376,8 +492,8 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
         const bool active = (uint32_t)lane < count;
         const DevShadowSeg g = A.segs[first + (active ? lane : 0)];
         const DevWalk W = A.walks[g.walk];
-        FChain<M_> ch;
-        ch.begin(W, g, A.state);
+        Chain ch;
+        ch.begin(W, g, A.state, A.axis);
         const uint64_t len = active ? g.s1 - g.s0 : 0;
         const double* src = A.mf + g.mf_off;
         unsigned long long mlen = len;
@@ -422,7 +538,7 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
                     const int tn = t + 1 < CS ? t + 1 : t;
 #pragma unroll
                     for (int e = 0; e < NE; ++e) Y[e] = buf[(tn * NE + e) * 32 + lane];
-                    chain_step<M_, COMP>(ch, X);
+                    chain_step<M_, COMP, Chain>(ch, X);
 #pragma unroll
                     for (int e = 0; e < NE; ++e) X[e] = Y[e];
                 }
@@ -434,7 +550,7 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
                         double X[NE];
 #pragma unroll
                         for (int e = 0; e < NE; ++e) X[e] = buf[(t * NE + e) * 32 + lane];
-                        chain_step<M_, COMP>(ch, X);
+                        chain_step<M_, COMP, Chain>(ch, X);
                         if (rel == cp_rel) ch.write(A.shadow + 3 * ((size_t)A.n_walks + g.walk), W);
                     }
                 }
@@ -501,7 +617,7 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
 #pragma unroll
                     for (int i = 0; i < NS; ++i) fd[i][j] -= fd[i][j - 1];
         FChain<M_> ch;
-        ch.begin(W, g, A.state);
+        ch.begin(W, g, A.state, A.axis);
         const uint64_t s_end = active ? g.s1 : g.s0;
         for (uint64_t s = g.s0; s < s_end; ++s) {
             if (CLS == CLS_COMPANION) {

@@ -90,27 +90,44 @@ __device__ __forceinline__ Mont tile_setup(const WalkArgs& A, const DevTile& T, 
         const uint32_t tn = to_mont_i64(__ldg(ax + 2), M), td = to_mont_i64(__ldg(ax + 3), M);
         // inv(sd*td); the reference skips the inverse when sd*td == 1
         const uint32_t icd = (__ldg(ax + 1) == 1 && __ldg(ax + 3) == 1) ? M.one : minv(mmul(sd, td, M), M);
-        wm.x0[a * 32 + lane] = mmul(mmul(sn, td, M), icd, M);
-        wm.dx[a * 32 + lane] = mmul(mmul(tn, sd, M), icd, M);
+        uint32_t x0 = mmul(mmul(sn, td, M), icd, M);
+        uint32_t dx = mmul(mmul(tn, sd, M), icd, M);
+        if (W.flags & DR_WALK_VEC) {
+            // state-vector walk: steps run depth-1 .. 0, so the axis
+            // progression starts at x(depth-1) and moves by -dx
+            x0 = addm(x0, mmul(to_mont_u64(W.depth - 1, M), dx, M), M.p);
+            dx = negm(dx, M.p);
+        }
+        wm.x0[a * 32 + lane] = x0;
+        wm.dx[a * 32 + lane] = dx;
     }
     if (G.zero_reg != 0xffffffffu) wm.rf[G.zero_reg * 32 + lane] = 0u;
     __syncwarp();
     return M;
 }
 
-__device__ __forceinline__ void set_axes(const WarpMem& wm, uint32_t dim, uint32_t s_m,
-                                         const Mont& M, int lane) {
+// LOAD_N value (Montgomery) at walk position s: the step index itself, or
+// depth-1-s for a state-vector walk, whose product runs M(depth-1) ... M(0).
+__device__ __forceinline__ uint32_t step_mont(const DevWalk& W, uint64_t s, const Mont& M) {
+    return to_mont_u64((W.flags & DR_WALK_VEC) ? W.depth - 1 - s : s, M);
+}
+
+// Axis values at walk position t with x0/dx from tile_setup (already reversed
+// for a state-vector walk).
+__device__ __forceinline__ void set_axes_at(const WarpMem& wm, uint32_t dim, uint64_t t,
+                                            const Mont& M, int lane) {
+    const uint32_t t_m = to_mont_u64(t, M);
     for (uint32_t a = 0; a < dim; ++a)
-        wm.cur[a * 32 + lane] = addm(wm.x0[a * 32 + lane], mmul(s_m, wm.dx[a * 32 + lane], M), M.p);
+        wm.cur[a * 32 + lane] = addm(wm.x0[a * 32 + lane], mmul(t_m, wm.dx[a * 32 + lane], M), M.p);
 }
 
 // Evaluate the original program at step s into stage[entry][lane] (m*m entries,
 // zero where not stored, as the reference's fresh zero matrix).
-__device__ __forceinline__ bool eval_original(const WalkArgs& A, const DevProgram& G,
+__device__ __forceinline__ bool eval_original(const WalkArgs& A, const DevWalk& W, const DevProgram& G,
                                               const WarpMem& wm, uint64_t s, const Mont& M,
                                               int lane) {
-    const uint32_t s_m = to_mont_u64(s, M);
-    set_axes(wm, G.dim, s_m, M, lane);
+    const uint32_t s_m = step_mont(W, s, M);
+    set_axes_at(wm, G.dim, s, M, lane);
     for (uint32_t e = 0; e < G.m * G.m; ++e) wm.stage[e * 32 + lane] = 0u;
     // the derived program may have used the zero register's slot
     if (G.zero_reg != 0xffffffffu) wm.rf[G.zero_reg * 32 + lane] = 0u;
@@ -171,9 +188,25 @@ __device__ __forceinline__ void emit(const WalkArgs& A, const DevTile& T, const 
                                      bool scaled, const Mont& M, int lane) {
     uint32_t pv = P[0][M_ - 1];
     uint32_t qv = P[0][M_ - 1];
+    if (W.flags & DR_WALK_VEC) {
+        // v = P v(0): the two requested entries as dot products with the
+        // walk's initial state residues for this prime
+        const uint32_t k = T.prime0 + min((uint32_t)lane, T.nprimes - 1u);
+        uint32_t w[M_];
 #pragma unroll
-    for (int i = 0; i < M_; ++i)
-        if ((uint32_t)i == W.q_row) qv = P[i][M_ - 1];
+        for (int j = 0; j < M_; ++j) w[j] = to_mont_i64(__ldg(A.axis + W.vec_off + (uint64_t)j * W.K + k), M);
+#pragma unroll
+        for (int i = 0; i < M_; ++i) {
+            if ((uint32_t)i == W.p_row) pv = mdot<M_>(P[i], w, M);
+            if ((uint32_t)i == W.q_row) qv = mdot<M_>(P[i], w, M);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < M_; ++i) {
+            if ((uint32_t)i == W.p_row) pv = P[i][M_ - 1];
+            if ((uint32_t)i == W.q_row) qv = P[i][M_ - 1];
+        }
+    }
     if (scaled) {
         const uint32_t iv = minv(sig, M);
         pv = mmul(pv, iv, M);
@@ -247,14 +280,14 @@ __device__ __forceinline__ void finish_tile(const WalkArgs& A, const DevTile& T,
 // Difference tables: fd[i][j] = Delta^j stream_i(s0), from the derived
 // program evaluated at s0 .. s0+Dp (Dp = program degree <= D).
 template <int NS, int D>
-__device__ __forceinline__ bool fd_init(uint32_t (&fd)[NS][D + 1], const WalkArgs& A,
+__device__ __forceinline__ bool fd_init(uint32_t (&fd)[NS][D + 1], const WalkArgs& A, const DevWalk& W,
                                         const DevProgram& G, const WarpMem& wm, uint64_t s0,
                                         const Mont& M, int lane) {
     const uint32_t Dp = G.degree;
     bool inv0 = false;
     for (uint32_t j = 0; j <= Dp; ++j) {
-        const uint32_t s_m = to_mont_u64(s0 + j, M);
-        set_axes(wm, G.dim, s_m, M, lane);
+        const uint32_t s_m = step_mont(W, s0 + j, M);
+        set_axes_at(wm, G.dim, s0 + j, M, lane);
         __syncwarp();
         inv0 |= interp_modp(A.code + G.dop_off, G.dn_ops, wm.rf, wm.cst, wm.cur, s_m,
                             wm.stage + j * NS * 32, M, lane);
@@ -291,7 +324,7 @@ __device__ __forceinline__ void tile_companion(const WalkArgs& A, const DevTile&
                                                const DevProgram& G, const WarpMem& wm, int lane) {
     const Mont M = tile_setup(A, T, W, G, wm, lane);
     uint32_t fd[M_][D + 1];
-    bool inv0 = fd_init<M_, D>(fd, A, G, wm, T.s0, M, lane);
+    bool inv0 = fd_init<M_, D>(fd, A, W, G, wm, T.s0, M, lane);
     uint32_t P[M_][M_];
     init_P<M_>(P, W, T.s0 == 0, M);
     const uint32_t n = (uint32_t)(T.s1 - T.s0);
@@ -322,7 +355,7 @@ __device__ __forceinline__ void tile_rational(const WalkArgs& A, const DevTile& 
                                               const DevProgram& G, const WarpMem& wm, int lane) {
     const Mont M = tile_setup(A, T, W, G, wm, lane);
     uint32_t fd[M_ + 1][D + 1];
-    bool inv0 = fd_init<M_ + 1, D>(fd, A, G, wm, T.s0, M, lane);
+    bool inv0 = fd_init<M_ + 1, D>(fd, A, W, G, wm, T.s0, M, lane);
     uint32_t P[M_][M_];
     init_P<M_>(P, W, T.s0 == 0, M);
     uint32_t sig = M.one;
@@ -334,7 +367,7 @@ __device__ __forceinline__ void tile_rational(const WalkArgs& A, const DevTile& 
             // some denominator is 0 mod p: the reference's INV(0) -> 0 step,
             // re-evaluated exactly from the original bytecode
             inv0 = true;
-            eval_original(A, G, wm, T.s0 + t, M, lane);
+            eval_original(A, W, G, wm, T.s0 + t, M, lane);
             mat_mul_stage<M_>(P, wm.stage, M, lane);
         } else {
             uint32_t c[M_];
@@ -364,7 +397,7 @@ __device__ __forceinline__ void tile_dense(const WalkArgs& A, const DevTile& T, 
                                            const DevProgram& G, const WarpMem& wm, int lane) {
     const Mont M = tile_setup(A, T, W, G, wm, lane);
     uint32_t fd[M_ * M_][D + 1];
-    bool inv0 = fd_init<M_ * M_, D>(fd, A, G, wm, T.s0, M, lane);
+    bool inv0 = fd_init<M_ * M_, D>(fd, A, W, G, wm, T.s0, M, lane);
     uint32_t P[M_][M_];
     init_P<M_>(P, W, T.s0 == 0, M);
     const uint32_t n = (uint32_t)(T.s1 - T.s0);
@@ -390,9 +423,11 @@ __device__ __forceinline__ void tile_interp(const WalkArgs& A, const DevTile& T,
     uint32_t P[M_][M_];
     init_P<M_>(P, W, T.s0 == 0, M);
     bool inv0 = false;
-    // axis values advance by dx per step; the step counter by one
-    uint32_t s_m = to_mont_u64(T.s0, M);
-    set_axes(wm, G.dim, s_m, M, lane);
+    // axis values advance by dx per step; the step counter by one (down by
+    // one for a state-vector walk)
+    uint32_t s_m = step_mont(W, T.s0, M);
+    set_axes_at(wm, G.dim, T.s0, M, lane);
+    const bool rev = (W.flags & DR_WALK_VEC) != 0;
     const uint32_t n = (uint32_t)(T.s1 - T.s0);
 #pragma unroll 1
     for (uint32_t t = 0; t < n; ++t) {
@@ -401,7 +436,7 @@ __device__ __forceinline__ void tile_interp(const WalkArgs& A, const DevTile& T,
         inv0 |= interp_modp(A.code + G.op_off, G.n_ops, wm.rf, wm.cst, wm.cur, s_m, wm.stage, M, lane);
         __syncwarp();
         mat_mul_stage<M_>(P, wm.stage, M, lane);
-        s_m = addm(s_m, M.one, M.p);
+        s_m = rev ? subm(s_m, M.one, M.p) : addm(s_m, M.one, M.p);
         for (uint32_t a = 0; a < G.dim; ++a)
             wm.cur[a * 32 + lane] = addm(wm.cur[a * 32 + lane], wm.dx[a * 32 + lane], M.p);
         __syncwarp();

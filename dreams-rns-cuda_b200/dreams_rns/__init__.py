@@ -11,13 +11,14 @@ exact delta run in hand-written CUDA behind libdreams_b200.so.
 """
 
 from .compiler import CmfCompiler, CmfProgram, Instruction, Opcode, compile_cmf, compile_cmf_from_dict
-from .engine import WalkBatch, WalkRequest, autotune, cmf_request, pcf_request, run_walks, sweep
+from .engine import (WalkBatch, WalkRequest, autotune, cmf_request, pcf_request, run_walks, sweep,
+                     vec_request)
 from .gpu_walk import (gpu_available, run_cmf_walk_batch_gpu, run_cmf_walk_gpu,
                        run_pcf_walk_batch_gpu, run_pcf_walk_gpu)
 from .runner import (WalkConfig, centered, compile_pcf, compute_dreams_delta_exact,
                      compute_dreams_delta_float, crt_batch, crt_reconstruct, delta_batch,
                      generate_rns_primes, pcf_initial_values, run_pcf_walk, verify_pcf)
-from .cmf_walk import compile_cmf_spec, run_cmf_walk
+from .cmf_walk import compile_cmf_spec, run_cmf_walk, run_cmf_walk_vec
 from . import runner, synth
 
 __version__ = "1.0.0"
@@ -27,7 +28,7 @@ __all__ = [
     "compute_dreams_delta_float", "compute_dreams_delta_exact", "compile_pcf",
     "pcf_initial_values", "run_pcf_walk", "verify_pcf",
     "gpu_available", "run_pcf_walk_gpu", "run_pcf_walk_batch_gpu", "run_cmf_walk_gpu",
-    "run_cmf_walk_batch_gpu", "run_cmf_walk", "compile_cmf_spec",
+    "run_cmf_walk_batch_gpu", "run_cmf_walk", "run_cmf_walk_vec", "vec_request", "compile_cmf_spec",
     "WalkBatch", "WalkRequest", "pcf_request", "cmf_request", "run_walks", "sweep", "autotune", "crt_batch",
     "delta_batch",
 ]

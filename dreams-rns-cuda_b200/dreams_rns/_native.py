@@ -31,6 +31,7 @@ DR_ERR_BUSY = -12
 
 DR_WALK_INIT_PCF = 0x1
 DR_WALK_SHADOW = 0x2
+DR_WALK_VEC = 0x4
 
 DR_STATUS_INV0 = 0x1
 DR_STATUS_SHADOW_NAN = 0x2
@@ -57,12 +58,16 @@ class WalkDesc(ctypes.Structure):
         ("axis_offset", ctypes.c_uint64),
         ("res_offset", ctypes.c_uint64),
         ("cp_res_offset", ctypes.c_uint64),
+        ("p_row", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("vec_offset", ctypes.c_uint64),
     ]
 
 
 WALK_DTYPE = np.dtype([("program", "<u4"), ("K", "<u4"), ("depth", "<u8"), ("checkpoint", "<u8"),
                        ("a0", "<i8"), ("flags", "<u4"), ("q_row", "<u4"), ("axis_offset", "<u8"),
-                       ("res_offset", "<u8"), ("cp_res_offset", "<u8")], align=True)
+                       ("res_offset", "<u8"), ("cp_res_offset", "<u8"), ("p_row", "<u4"),
+                       ("reserved", "<u4"), ("vec_offset", "<u8")], align=True)
 assert WALK_DTYPE.itemsize == ctypes.sizeof(WalkDesc)
 
 

@@ -14,7 +14,7 @@ from typing import Dict, List, Optional, Tuple
 import numpy as np
 
 from .compiler import CmfCompiler, CmfProgram, Opcode
-from .engine import cmf_request, run_walks
+from .engine import cmf_request, run_walks, vec_request
 from .runner import centered, crt_reconstruct, generate_rns_primes
 
 __all__ = ["compile_cmf_spec", "shift_to_axis_offsets", "run_cmf_walk", "run_cmf_walk_vec"]
@@ -94,9 +94,9 @@ def run_cmf_walk(program: CmfProgram, depth: int, K: int, shift_vals, trajectory
 
 def run_cmf_walk_vec(program: CmfProgram, depth: int, K: int, shift_vals, initial_state,
                      acc_idx: int, const_idx: int, trajectory_vals=None):
-    """State-vector walk v(N) = M(N-1) ... M(0) v(0) (cmf_walk.py:445-531).
-
-    Not yet on the engine: raises NotImplementedError rather than computing on
-    the CPU.
-    """
-    raise NotImplementedError("run_cmf_walk_vec is not implemented on the B200 engine yet")
+    """State-vector walk v(N) = M(N-1) ... M(0) v(0) on the GPU (reference
+    cmf_walk.py:445-531): p = v[acc_idx], q = v[const_idx], with the FP64
+    shadow of v rescaled like the reference's."""
+    req = vec_request(program, max(int(depth), 0), int(K), shift_vals, initial_state, acc_idx,
+                      const_idx, trajectory_vals)
+    return _ref_dict(run_walks([req])[0])

@@ -63,6 +63,8 @@ class WalkRequest:
     checkpoint: int = 0
     shadow: bool = True
     tag: dict = field(default_factory=dict)
+    p_row: int = 0
+    vec: Optional[List[int]] = None     # state-vector walk: v(0) residues then float bits
 
 
 def pcf_request(program, a0: int, depth: int, K: int = 32, shift_val: int = 1,
@@ -74,6 +76,40 @@ def pcf_request(program, a0: int, depth: int, K: int = 32, shift_val: int = 1,
     return WalkRequest(blob=blob, K=K, depth=depth, a0=int(a0), pcf_init=True, q_row=1,
                        axis=[(int(shift_val), 1, d, 1) for d in dirs], checkpoint=checkpoint,
                        shadow=shadow)
+
+
+def vec_request(program, depth: int, K: int, shift_vals, initial_state, acc_idx: int,
+                const_idx: int, trajectory_vals=None, shadow: bool = True) -> WalkRequest:
+    """State-vector walk v(N) = M(N-1) ... M(0) v(0) with p = v[acc_idx],
+    q = v[const_idx] (reference cmf_walk.py:445-531).  v(0) entries are
+    rationals: their residues per prime are num * den^(p-2) mod p, as the
+    reference computes them (a denominator divisible by p gives 0)."""
+    from fractions import Fraction
+    req = cmf_request(program, depth, K, shift_vals, trajectory_vals, shadow=shadow)
+    m = req.q_row + 1
+    if len(initial_state) < m:
+        raise IndexError("initial_state has fewer entries than the matrix size")
+    if not (0 <= acc_idx < m and 0 <= const_idx < m):
+        raise IndexError("acc_idx / const_idx outside the state vector")
+    primes = [int(p) for p in N.prime_table(K)]
+    res: List[int] = []
+    fl = []
+    for i in range(m):
+        f = Fraction(initial_state[i])
+        fl.append(float(f))
+        if f == 0:
+            res.extend([0] * K)
+            continue
+        num, den = f.numerator, f.denominator
+        for p in primes:
+            n = num % p
+            res.append(n if den == 1 else n * pow(den, p - 2, p) % p)
+    bits = np.array(fl, dtype=np.float64).view(np.int64)
+    req.vec = res + [int(b) for b in bits]
+    req.p_row = int(acc_idx)
+    req.q_row = int(const_idx)
+    req.pcf_init = False
+    return req
 
 
 def cmf_request(program, depth: int, K: int, shift_vals, trajectory_vals=None,
@@ -125,10 +161,12 @@ class _Packed:
         except OverflowError:
             raise OverflowError("a0 outside int64") from None
         try:
-            axis = np.array([v for r in reqs for t in r.axis for v in t], dtype=np.int64)
+            axis = np.array([v for r in reqs for t in r.axis for v in t] +
+                            [v for r in reqs if r.vec is not None for v in r.vec], dtype=np.int64)
         except OverflowError:
             raise OverflowError("axis parameter outside int64") from None
         alen = np.array([4 * len(r.axis) for r in reqs], dtype=np.uint64).reshape(n)
+        vlen = np.array([len(r.vec) if r.vec is not None else 0 for r in reqs], dtype=np.uint64).reshape(n)
         sizes = Ks + np.where(cps > 0, Ks, 0)
         res_off = np.zeros(n, dtype=np.int64)
         if n:
@@ -140,8 +178,15 @@ class _Packed:
         desc["checkpoint"] = cps
         desc["a0"] = a0
         desc["flags"] = [(N.DR_WALK_INIT_PCF if r.pcf_init else 0) | (N.DR_WALK_SHADOW if r.shadow else 0)
-                         for r in reqs]
+                         | (N.DR_WALK_VEC if r.vec is not None else 0) for r in reqs]
         desc["q_row"] = [r.q_row for r in reqs]
+        desc["p_row"] = [r.p_row for r in reqs]
+        voff = np.zeros(n, dtype=np.uint64)
+        if n:
+            voff[:] = int(alen.sum())
+            np.cumsum(vlen[:-1], out=voff[1:])
+            voff[1:] += int(alen.sum())
+        desc["vec_offset"] = np.where(vlen > 0, voff, 0)
         aoff = np.zeros(n, dtype=np.uint64)
         if n:
             np.cumsum(alen[:-1], out=aoff[1:])

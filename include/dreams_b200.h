@@ -50,7 +50,7 @@ extern "C" {
  * with (sn, sd, tn, td) = axis_params[axis_offset + 4a .. +3]
  * (reference cmf_walk.py:221-224; the PCF walk is sn = shift, tn = direction,
  * sd = td = 1, runner.py:225-227).
- * Outputs: p = P[0][m-1], q = P[q_row][m-1] (PCF: q_row = 1, runner.py:401-402;
+ * Outputs: p = P[p_row][m-1], q = P[q_row][m-1] (PCF: q_row = 1, runner.py:401-402;
  * CMF: q_row = m-1, cmf_walk.py:419-420) written to
  * p_res[res_offset + k], q_res[res_offset + k] for k < K.  With a non-zero
  * checkpoint the same outputs after `checkpoint` steps go to
@@ -58,6 +58,13 @@ extern "C" {
  * shadow[3*w], and shadow[3*(n_walks + w)] for the checkpoint.            */
 #define DR_WALK_INIT_PCF   0x1u   /* P0 = [[1, a0], [0, 1]], else P0 = I     */
 #define DR_WALK_SHADOW     0x2u   /* compute the FP64 shadow                  */
+#define DR_WALK_VEC        0x4u   /* state-vector walk (reference cmf_walk.py:445-531):
+                                     v(depth) = M(depth-1) ... M(0) v(0); p = v[p_row],
+                                     q = v[q_row].  v(0) sits in axis_params at
+                                     vec_offset: m*K residues (entry i for prime k at
+                                     vec_offset + i*K + k, each in [0, p_k)) then the
+                                     m doubles of the float v(0) as int64 bit patterns.
+                                     No checkpoint, no DR_WALK_INIT_PCF.          */
 
 typedef struct dr_walk_desc {
     uint32_t program;       /* index into the program blob list              */
@@ -70,6 +77,10 @@ typedef struct dr_walk_desc {
     uint64_t axis_offset;   /* index of this walk's first axis parameter     */
     uint64_t res_offset;    /* residue output offset                         */
     uint64_t cp_res_offset; /* checkpoint residue output offset              */
+    uint32_t p_row;         /* row of p in the last column (0 for the reference's
+                               walks; DR_WALK_VEC: state entry of p)          */
+    uint32_t reserved;
+    uint64_t vec_offset;    /* DR_WALK_VEC: index of v(0) in axis_params      */
 } dr_walk_desc;
 
 /* walk status bits (status_out[w]) */

@@ -363,3 +363,54 @@ def test_autotune_keeps_results():
         assert list(x["p_residues"]) == list(y["p_residues"])
         assert list(x["checkpoint"]["q_residues"]) == list(y["checkpoint"]["q_residues"])
         assert x["p_float"] == y["p_float"]
+
+
+def test_vec_walk_golden(golden):
+    """run_cmf_walk_vec against the reference's own output (fixture)."""
+    from fractions import Fraction
+    for w in golden["vec_walks"]:
+        prog = CmfProgramFromHex(w["blob"])
+        r = dr.run_cmf_walk_vec(prog, w["depth"], w["K"], [tuple(x) for x in w["shifts"]],
+                                [Fraction(a, b) for a, b in w["initial_state"]], w["acc_idx"],
+                                w["const_idx"], [tuple(x) for x in w["trajectory"]])
+        assert list(r["p_residues"]) == w["p_residues"], w["name"]
+        assert list(r["q_residues"]) == w["q_residues"], w["name"]
+        pf, qf, ls = (float.fromhex(w[k]) for k in ("p_float", "q_float", "log_scale"))
+        assert _close(r["p_float"], pf) and _close(r["q_float"], qf) and _close(r["log_scale"], ls, 1e-13)
+
+
+def CmfProgramFromHex(h):
+    return dr.CmfProgram.deserialize(bytes.fromhex(h))
+
+
+def test_vec_walks_vs_oracle():
+    """State-vector walks of random m x m programs (m = 2..4, rational shifts
+    and trajectories, rational v(0), any acc/const entries) against the numpy
+    restatement of the reference, batched with ordinary walks."""
+    from fractions import Fraction
+    from oracle import walk_np
+    rng = random.Random(41)
+    cases, reqs = [], []
+    for trial in range(24):
+        blob, m, dim = random_program(rng, m_choices=(2, 3, 4))
+        shifts = [(rng.randrange(-5, 6), rng.choice([1, 2, 3])) for _ in range(dim)]
+        traj = [(rng.randrange(-3, 4), rng.choice([1, 2])) for _ in range(dim)]
+        v0 = [Fraction(rng.randrange(-9, 10), rng.randrange(1, 5)) for _ in range(m)]
+        acc, const = rng.randrange(m), rng.randrange(m)
+        depth = rng.randrange(0, 400)
+        K = rng.choice([8, 32, 40])
+        cases.append((blob, depth, K, shifts, v0, acc, const, traj))
+        reqs.append(dr.vec_request(blob, depth, K, shifts, v0, acc, const, traj))
+        if trial % 4 == 0:   # ordinary walks in the same batch
+            reqs.append(cmf_request(blob, depth, K, shifts, traj))
+            cases.append(None)
+    res = run_walks(reqs)
+    for c, r in zip(cases, res):
+        if c is None:
+            continue
+        blob, depth, K, shifts, v0, acc, const, traj = c
+        o = walk_np.cmf_walk_vec(blob, depth, K, shifts, v0, acc, const, traj)
+        assert list(r["p_residues"]) == list(o["p_residues"]), (depth, K)
+        assert list(r["q_residues"]) == list(o["q_residues"]), (depth, K)
+        if not (math.isnan(o["p_float"]) or math.isnan(r["p_float"])):
+            assert _close(r["p_float"], o["p_float"], 1e-9) and _close(r["q_float"], o["q_float"], 1e-9)
