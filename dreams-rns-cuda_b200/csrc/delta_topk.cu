@@ -11,6 +11,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "../../include/dreams_b200.h"
+#include "dr_types.h"
 #include "launch.h"
 
 namespace dr {
@@ -143,6 +145,49 @@ __global__ void __launch_bounds__(128) k_delta(DeltaArgs D) {
         if (lane == 0) D.out[v] = result;
         __syncwarp();
     }
+}
+
+// CRT overflow test (reference euler2ai_full_verify.py:152-167): the ratio of
+// the reconstructed p and q must agree with the float shadow's p_f / q_f to 1%
+// (relative when |p_f/q_f| > 1e-10, absolute otherwise); q = 0 or a
+// non-finite ratio also counts as overflow.  One thread per (walk, final or
+// checkpoint); rows 4w+0..3 of limbs hold p, q, checkpoint p, checkpoint q.
+__global__ void k_crt_check(const uint32_t* __restrict__ limbs, const int32_t* __restrict__ signs,
+                            int L, int n, const DevWalk* __restrict__ walks,
+                            const double* __restrict__ shadow, uint32_t* status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * n) return;
+    const int w = i >> 1, cp = i & 1;
+    const DevWalk W = walks[w];
+    if (!(W.flags & DR_WALK_SHADOW) || (cp && !W.checkpoint)) return;
+    const double* sh = shadow + 3 * ((size_t)(cp ? n : 0) + w);
+    const double est = sh[0] / sh[1];
+    const uint32_t* p = limbs + (size_t)(4 * w + 2 * cp) * L;
+    const uint32_t* q = p + L;
+    const int tp = top_limb(p, L), tq = top_limb(q, L);
+    bool bad;
+    if (tq < 0 || !isfinite(est)) {
+        bad = true;
+    } else {
+        double ratio = 0.0;
+        if (tp >= 0) {
+            const double lr = (ln_big(p, tp) - ln_big(q, tq)) * 1.4426950408889634;   // log2 |p/q|
+            ratio = lr > 1024.0 ? INFINITY : exp2(lr);
+            if (signs[4 * w + 2 * cp] * signs[4 * w + 2 * cp + 1] < 0) ratio = -ratio;
+        }
+        if (!isfinite(ratio)) bad = true;
+        else if (fabs(est) > 1e-10) bad = fabs(ratio - est) / fabs(est) > 0.01;
+        else bad = fabs(ratio - est) > 0.01;
+    }
+    if (bad) atomicOr(status + w, cp ? DR_STATUS_CP_CRT_OVERFLOW : DR_STATUS_CRT_OVERFLOW);
+}
+
+cudaError_t launch_crt_check(const uint32_t* limbs, const int32_t* signs, int L, int n,
+                             const DevWalk* walks, const double* shadow, uint32_t* status,
+                             cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_crt_check<<<(2 * n + 127) / 128, 128, 0, st>>>(limbs, signs, L, n, walks, shadow, status);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_delta(const DeltaArgs& D, int sms, cudaStream_t st) {

@@ -772,6 +772,12 @@ static int enqueue_pipeline(Batch& B, cudaStream_t st) {
                                    B.crt_in.as<uint64_t>() + g.off, B.crt_out.as<uint32_t>() + g.off);
         if (e != cudaSuccess) return cuda_fail(e, "pipeline crt");
     }
+    if (B.has_shadow && !B.crt_groups.empty()) {
+        cudaError_t e = launch_crt_check(B.limbs.as<uint32_t>(), B.signs.as<int32_t>(), B.Lmax,
+                                         (int)B.n_walks, B.walks.as<DevWalk>(), B.shadow.as<double>(),
+                                         B.status.as<uint32_t>(), st);
+        if (e != cudaSuccess) return cuda_fail(e, "pipeline crt check");
+    }
     if (B.pipe.delta_mode != DR_DELTA_NONE) {
         DeltaArgs D{};
         const bool self = B.pipe.delta_mode == DR_DELTA_SELF;

@@ -44,6 +44,11 @@ cudaError_t launch_crt(const uint32_t* res, int n, const CrtTables& T, uint32_t*
                        int32_t* sign, int32_t* nl, uint32_t* ul, int sms, cudaStream_t st,
                        const uint64_t* in_off = nullptr, const uint32_t* out_idx = nullptr);
 cudaError_t launch_delta(const DeltaArgs& D, int sms, cudaStream_t st);
+struct DevWalk;
+// Per-walk CRT overflow flags from the pipeline's limbs and the FP64 shadow.
+cudaError_t launch_crt_check(const uint32_t* limbs, const int32_t* signs, int L, int n,
+                             const DevWalk* walks, const double* shadow, uint32_t* status,
+                             cudaStream_t st);
 cudaError_t launch_topk_tile(const double* vals, const uint64_t* in_keys, const uint32_t* in_idx,
                              int n, int k, uint64_t* out_keys, uint32_t* out_idx, cudaStream_t st);
 int topk_tile_size();

@@ -36,6 +36,8 @@ DR_WALK_VEC = 0x4
 DR_STATUS_INV0 = 0x1
 DR_STATUS_SHADOW_NAN = 0x2
 DR_STATUS_FALLBACK = 0x4
+DR_STATUS_CRT_OVERFLOW = 0x8
+DR_STATUS_CP_CRT_OVERFLOW = 0x10
 
 DR_ENGINE_AUTO = 0
 DR_ENGINE_INTERP = 1

@@ -191,6 +191,56 @@ def delta_batch(ps: Sequence[int], qs: Sequence[int], targets: Sequence[Tuple[in
     return [float(v) for v in out]
 
 
+def estimate_K(a_str: str, b_str: str, depth: int, safety: float = 1.5) -> int:
+    """Primes needed for an exact CRT of a depth-N PCF convergent
+    (reference euler2ai_full_verify.py:40-93): bits ~ d*log2(N!) + N*log2(c)
+    for entries of degree d and largest coefficient c, times ``safety`` plus
+    100, at least 64 primes; 1000+ when the expressions do not parse."""
+    import sympy as sp
+    try:
+        a_expr = sp.sympify(a_str)
+        b_expr = sp.sympify(b_str)
+        n = sp.Symbol("n")
+        deg_a = sp.degree(a_expr, n) if a_expr.has(n) else 0
+        deg_b = sp.degree(b_expr, n) if b_expr.has(n) else 0
+        max_deg = max(int(deg_a), int(deg_b), 1)
+        max_coeff = 1
+        for expr in (a_expr, b_expr):
+            try:
+                for c in sp.Poly(expr, n).all_coeffs():
+                    max_coeff = max(max_coeff, abs(int(c)))
+            except Exception:  # noqa: BLE001 - non-polynomial entries, as the reference
+                max_coeff = max(max_coeff, 100)
+        if depth > 1:
+            log2_fact = depth * math.log2(depth / math.e) + 0.5 * math.log2(2 * math.pi * depth)
+        else:
+            log2_fact = 1
+        coeff_bits = math.log2(max_coeff + 1) if max_coeff > 1 else 0
+        bits = int((max_deg * log2_fact + depth * coeff_bits) * safety) + 100
+        return max(bits // 31 + 1, 64)
+    except Exception:  # noqa: BLE001 - the reference's conservative fallback
+        log2_fact = depth * math.log2(max(depth, 2) / math.e)
+        return max(int(4 * log2_fact * safety / 31) + 1, 1000)
+
+
+def crt_overflowed(p_big: int, q_big: int, est_float: float) -> bool:
+    """CRT overflow test (reference euler2ai_full_verify.py:152-167): the
+    exact p/q must agree with the float shadow's estimate to 1%.  The device
+    pipeline sets DR_STATUS_CRT_OVERFLOW by the same rule."""
+    import mpmath as mp
+    if q_big == 0:
+        return True
+    try:
+        crt_ratio = float(mp.mpf(p_big) / mp.mpf(q_big))
+        if not math.isfinite(crt_ratio) or not math.isfinite(est_float):
+            return True
+        if abs(est_float) > 1e-10:
+            return abs(crt_ratio - est_float) / abs(est_float) > 0.01
+        return abs(crt_ratio - est_float) > 0.01
+    except Exception:  # noqa: BLE001 - as the reference
+        return True
+
+
 def compute_dreams_delta_exact(p_big: int, q_big: int, target, dps: int = 200):
     """Exact delta from big integers (runner.py:103-125), computed on the GPU.
 

@@ -88,6 +88,12 @@ typedef struct dr_walk_desc {
                                        config.h:166-169 "dead lane")         */
 #define DR_STATUS_SHADOW_NAN  0x2u  /* shadow became non-finite               */
 #define DR_STATUS_FALLBACK    0x4u  /* walk ran on the per-step interpreter   */
+#define DR_STATUS_CRT_OVERFLOW    0x8u  /* device pipeline: the CRT value of p/q
+                                           disagrees with the FP64 shadow's
+                                           p_float/q_float by more than 1% (K too
+                                           small; reference euler2ai_full_verify.py
+                                           :152-167 crt_overflowed)               */
+#define DR_STATUS_CP_CRT_OVERFLOW 0x10u /* the same for the checkpoint values      */
 
 /* engine selection for dr_walk_batch */
 #define DR_ENGINE_AUTO    0   /* planned fast path (difference tables), else

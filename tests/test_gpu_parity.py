@@ -414,3 +414,29 @@ def test_vec_walks_vs_oracle():
         assert list(r["q_residues"]) == list(o["q_residues"]), (depth, K)
         if not (math.isnan(o["p_float"]) or math.isnan(r["p_float"])):
             assert _close(r["p_float"], o["p_float"], 1e-9) and _close(r["q_float"], o["q_float"], 1e-9)
+
+
+def test_device_crt_overflow_flag_matches_host_rule():
+    """The pipeline's CRT-overflow status bits equal the host rule
+    (runner.crt_overflowed, the reference's 1% test against the shadow) for
+    walks whose K ranges from far too small to ample."""
+    from dreams_rns.runner import crt_overflowed
+    rng = random.Random(43)
+    reqs = []
+    for i in range(48):
+        a = dr.synth.poly_str([rng.randrange(-9, 10) for _ in range(3)])
+        b = dr.synth.poly_str([rng.randrange(-9, 10) for _ in range(4)])
+        depth = rng.randrange(60, 900)
+        reqs.append(pcf_request(dr.compile_pcf(a, b), dr.pcf_initial_values(a), depth,
+                                rng.choice([1, 2, 4, 8, 16, 64, 128]), checkpoint=depth // 2))
+    out = dr.sweep(reqs, values=True)
+    flagged = 0
+    for i, r in enumerate(reqs):
+        sh, cps = out["shadow"][i], out["checkpoint_shadow"][i]
+        want = crt_overflowed(out["p"][i], out["q"][i], sh[0] / sh[1])
+        want_cp = crt_overflowed(out["cp_p"][i], out["cp_q"][i], cps[0] / cps[1])
+        st = int(out["status"][i])
+        assert bool(st & N.DR_STATUS_CRT_OVERFLOW) == want, (i, r.K, r.depth)
+        assert bool(st & N.DR_STATUS_CP_CRT_OVERFLOW) == want_cp, (i, r.K, r.depth)
+        flagged += want
+    assert 0 < flagged < len(reqs)

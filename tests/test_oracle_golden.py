@@ -104,3 +104,16 @@ def test_delta_float(golden):
         want, wlq = float(d["delta"]), float(d["log_q"])
         assert (got == want) or (math.isnan(got) and math.isnan(want))
         assert lq == wlq
+
+
+def test_estimate_k_and_overflow_match_reference():
+    """Auto-K and the CRT-overflow rule (host side) against the reference's
+    own outputs (tests/golden/make_estimate_k.py)."""
+    import json
+    import os
+    from dreams_rns.runner import crt_overflowed, estimate_K
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "estimate_k.json")))
+    for a, b, d, want in g["estimate_K"]:
+        assert estimate_K(a, b, d) == want, (a, b, d)
+    for p, q, e, want in g["crt_overflowed"]:
+        assert crt_overflowed(int(p), int(q), float(e)) == want, (p, q, e)
