@@ -69,12 +69,17 @@ __global__ void __launch_bounds__(128) k_delta(DeltaArgs D) {
     uint32_t* A = reinterpret_cast<uint32_t*>(col + 2 * ML);
     uint32_t* B = A + ML;
     for (int v = blockIdx.x * wpb + warp; v < D.n; v += gridDim.x * wpb) {
-        const uint32_t* p = D.p + (size_t)v * D.istride;
-        const uint32_t* q = D.q + (size_t)v * D.istride;
-        const int ti = D.per_item ? v : 0;
+        size_t row = (size_t)v;
+        int ti = D.per_item ? v : 0;
+        if (D.bank_n > 0) {
+            row = D.rows[v / D.bank_n];
+            ti = v % D.bank_n;
+        }
+        const uint32_t* p = D.p + row * D.istride;
+        const uint32_t* q = D.q + row * D.istride;
         const uint32_t* ln = D.ln + (size_t)ti * D.listride;
         const uint32_t* ld = D.ld + (size_t)ti * D.listride;
-        const int ps = D.ps[(size_t)v * D.sstride], qs = D.qs[(size_t)v * D.sstride];
+        const int ps = D.ps[row * D.sstride], qs = D.qs[row * D.sstride];
         const int lns = D.lns[(size_t)ti * D.lsstride] * (D.lds ? D.lds[(size_t)ti * D.lsstride] : 1);
         const int tp = top_limb(p, D.nl), tq = top_limb(q, D.nl);
         const int tn = top_limb(ln, D.lnl), td = top_limb(ld, D.lnl);

@@ -140,7 +140,8 @@ Batch::Batch() {
     for (DevBuf* b : {&progs, &code, &consts, &walks, &axis, &tiles, &groups, &group_done, &chunkP,
                       &chunkSig, &shadow_list, &queues, &res, &shadow, &status, &mf, &eval_items,
                       &shadow_state, &tstamps, &crt_in, &crt_out, &limbs, &signs, &delta, &tgt_num,
-                      &tgt_den, &tgt_sign, &tk_keys[0], &tk_keys[1], &tk_idx[0], &tk_idx[1]})
+                      &tgt_den, &tgt_sign, &tk_keys[0], &tk_keys[1], &tk_idx[0], &tk_idx[1],
+                      &bank_num, &bank_den, &bank_sign, &bank_out})
         b->pooled = true;
 }
 
@@ -824,6 +825,32 @@ static int enqueue_pipeline(Batch& B, cudaStream_t st) {
                                  B.tk_idx[dst].as<uint32_t>(), st);
             if (e != cudaSuccess) return cuda_fail(e, "pipeline topk");
         }
+        if (B.bank_n > 0 && !B.tk_counts.empty()) {
+            // every top-k hit's final p/q against every bank constant
+            DeltaArgs K{};
+            K.p = lim;
+            K.q = lim + L;
+            K.ps = sg;
+            K.qs = sg + 1;
+            K.nl = B.Lmax;
+            K.istride = 4 * L;
+            K.sstride = 4;
+            K.ln = B.bank_num.as<uint32_t>();
+            K.ld = B.bank_den.as<uint32_t>();
+            K.lns = B.bank_sign.as<int32_t>();
+            K.lds = nullptr;
+            K.lnl = B.bank_l;
+            K.per_item = 1;
+            K.listride = (size_t)B.bank_l;
+            K.lsstride = 1;
+            K.rows = B.tk_idx[B.tk_final].as<uint32_t>();
+            K.bank_n = B.bank_n;
+            K.n = std::min<int>(B.pipe.topk, (int)B.n_walks) * B.bank_n;
+            K.out = B.bank_out.as<double>();
+            K.maxlen = ((B.Lmax + std::max(B.Lmax, B.bank_l) + 4) + 1) & ~1;
+            e = launch_delta(K, C.sms, st);
+            if (e != cudaSuccess) return cuda_fail(e, "pipeline bank");
+        }
     }
     return DR_OK;
 }
@@ -1339,6 +1366,45 @@ int dr_batch_set_pipeline(int32_t batch, const dr_pipeline* pl) {
         B->tk_final = (int)((B->tk_counts.size() - 1) & 1);
     }
     DR_CUDA(cudaStreamSynchronize(st));
+    return DR_OK;
+}
+
+int dr_batch_set_bank(int32_t batch, int32_t n_consts, int32_t l_limbs, const uint32_t* num,
+                      const int32_t* num_sign, const uint32_t* den) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    if (n_consts < 0 || (n_consts > 0 && (l_limbs < 1 || !num || !num_sign || !den))) return DR_ERR_ARG;
+    if (n_consts > 4096 || l_limbs > 1024) { set_error("bank above 4096 constants or 1024 limbs"); return DR_ERR_UNSUPPORTED; }
+    DR_CUDA(cudaDeviceSynchronize());
+    if (B->graph) { cudaGraphExecDestroy(B->graph); B->graph = nullptr; }
+    B->bank_n = n_consts;
+    B->bank_l = l_limbs;
+    if (!n_consts) return DR_OK;
+    cudaStream_t st = g_ctx->stream;
+    std::vector<uint32_t> nv(num, num + (size_t)n_consts * l_limbs), dv(den, den + (size_t)n_consts * l_limbs);
+    std::vector<int32_t> sv(num_sign, num_sign + n_consts);
+    if ((rc = upload(B->bank_num, nv, st))) return rc;
+    if ((rc = upload(B->bank_den, dv, st))) return rc;
+    if ((rc = upload(B->bank_sign, sv, st))) return rc;
+    DR_CUDA(B->bank_out.alloc(8ull * std::max<uint32_t>(B->n_walks, 1) * n_consts));
+    DR_CUDA(cudaStreamSynchronize(st));
+    return DR_OK;
+}
+
+int dr_batch_read_bank(int32_t batch, double* delta, int32_t max_values) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    if (!B->pipe_on || B->tk_counts.empty() || B->bank_n <= 0) {
+        set_error("no constant bank with top-k on this batch");
+        return DR_ERR_ARG;
+    }
+    DR_CUDA(cudaDeviceSynchronize());
+    const int64_t n = (int64_t)std::min<int>(B->pipe.topk, (int)B->n_walks) * B->bank_n;
+    DR_CUDA(cudaMemcpy(delta, B->bank_out.p, 8ull * std::min<int64_t>(n, max_values), cudaMemcpyDeviceToHost));
     return DR_OK;
 }
 

@@ -153,6 +153,8 @@ struct Batch {
     std::vector<CrtGroup> crt_groups;
     DevBuf crt_in, crt_out, limbs, signs, delta, tgt_num, tgt_den, tgt_sign;
     DevBuf tk_keys[2], tk_idx[2];
+    int bank_n = 0, bank_l = 0;          // constant bank scored after top-k
+    DevBuf bank_num, bank_den, bank_sign, bank_out;
     std::vector<int> tk_counts;         // values entering each top-k pass
     int tk_final = 0;                   // buffer holding the final top-k
     std::vector<uint32_t> h_walk_K;

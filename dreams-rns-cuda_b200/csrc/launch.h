@@ -34,6 +34,10 @@ struct DeltaArgs {
     size_t listride, lsstride;
     double* out;
     int maxlen;                              // product length bound (limbs)
+    // bank mode (bank_n > 0): item i scores row rows[i / bank_n] of p, q
+    // against target i % bank_n (the top-k hits against a constant bank)
+    const uint32_t* rows;
+    int bank_n;
 };
 
 cudaError_t launch_crt_setup(const uint32_t* moduli, int K, int L, uint32_t* pinv, uint32_t* r2,

@@ -127,6 +127,8 @@ _SIGNATURES = {
     "dr_batch_set_pipeline": (ctypes.c_int, [_I32, _P]),
     "dr_batch_profile": (ctypes.c_int, [_I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "dr_autotune": (ctypes.c_int, [_P, _I32, _P, _P, _I32, _P, _U64, _P, _P]),
+    "dr_batch_set_bank": (ctypes.c_int, [_I32, _I32, _I32, _P, _P, _P]),
+    "dr_batch_read_bank": (ctypes.c_int, [_I32, _P, _I32]),
     "dr_batch_read_pipeline": (ctypes.c_int, [_I32, _P, _P, _P, _P, _P, _I32]),
     "dr_crt_batch": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P]),
     "dr_crt_batch_device": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _I32, _P, _P, _P]),

@@ -255,7 +255,7 @@ def run_walks(reqs: Sequence[WalkRequest], chunk_steps: int = 0,
 
 def sweep(reqs: Sequence[WalkRequest], delta: Optional[str] = None,
           target: Optional[Tuple[int, int]] = None, topk: int = 0, values: bool = False,
-          chunk_steps: int = 0) -> dict:
+          chunk_steps: int = 0, bank=None) -> dict:
     """One call for a sweep of many walks: walk every request, then on the
     device reconstruct p and q by CRT, score the Dreams delta (``delta="fixed"``
     against ``target`` = (Lnum, Lden), or ``"self"``: each walk's checkpoint
@@ -263,7 +263,9 @@ def sweep(reqs: Sequence[WalkRequest], delta: Optional[str] = None,
 
     Returns arrays (see ``WalkBatch.read_arrays``) plus ``delta``, ``topk_idx``,
     ``topk_val`` and, with ``values``, the centred p, q (and checkpoint p, q) as
-    Python ints.  The batched counterpart of calling run_pcf_walk /
+    Python ints.  With ``bank`` (constants from constants.load_constants) each
+    top-k hit is also scored against every constant (``bank_delta``,
+    ``bank_best``).  The batched counterpart of calling run_pcf_walk /
     run_cmf_walk, crt_reconstruct and compute_dreams_delta_exact per walk.
     """
     b = WalkBatch(reqs, chunk_steps=chunk_steps)
@@ -271,10 +273,14 @@ def sweep(reqs: Sequence[WalkRequest], delta: Optional[str] = None,
         piped = bool(delta) or topk > 0 or values
         if piped:
             b.set_pipeline(delta=delta, target=target, topk=topk)
+        if bank:
+            b.set_bank(bank)
         b.run()
         out = b.read_arrays()
         if piped:
             out.update(b.read_pipeline(values=values))
+        if bank and topk > 0:
+            out.update(b.read_bank())
         return out
     finally:
         b.close()
@@ -399,6 +405,37 @@ class WalkBatch:
             out["cp_p"] = vals[2::4]
             out["cp_q"] = vals[3::4]
         return out
+
+    def set_bank(self, constants) -> None:
+        """Score every top-k hit's final p/q against each constant (dicts from
+        constants.load_constants) on the device after each run."""
+        from .constants import bank_ratios
+        from .runner import int_to_limbs
+        self.bank = list(constants)
+        if not self.bank:
+            N.check(N.lib().dr_batch_set_bank(self.handle, 0, 0, None, None, None), "dr_batch_set_bank")
+            return
+        rat = bank_ratios(self.bank)
+        width = max(max(abs(a).bit_length(), b.bit_length()) for a, b in rat)
+        nl = (width + 31) // 32 + 1
+        num = np.zeros((len(rat), nl), dtype=np.uint32)
+        den = np.zeros((len(rat), nl), dtype=np.uint32)
+        sg = np.zeros(len(rat), dtype=np.int32)
+        for i, (a, b) in enumerate(rat):
+            sg[i], num[i] = int_to_limbs(int(a), nl)
+            _, den[i] = int_to_limbs(int(b), nl)
+        N.check(N.lib().dr_batch_set_bank(self.handle, len(rat), nl, N.ptr(num), N.ptr(sg), N.ptr(den)),
+                "dr_batch_set_bank")
+
+    def read_bank(self) -> dict:
+        """delta[hit][constant] for the top-k hits, and each hit's best match."""
+        k = min(self.pipeline["topk"], self.pk.n)
+        nb = len(self.bank)
+        d = np.zeros(max(k * nb, 1), dtype=np.float64)
+        N.check(N.lib().dr_batch_read_bank(self.handle, N.ptr(d), k * nb), "dr_batch_read_bank")
+        d = d[:k * nb].reshape(k, nb)
+        best = [self.bank[int(np.argmax(row))]["name"] if nb else None for row in d]
+        return {"bank_delta": d, "bank_names": [c["name"] for c in self.bank], "bank_best": best}
 
     def stats(self) -> dict:
         ps, nt, nl, ms = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_float()

@@ -440,3 +440,34 @@ def test_device_crt_overflow_flag_matches_host_rule():
         assert bool(st & N.DR_STATUS_CP_CRT_OVERFLOW) == want_cp, (i, r.K, r.depth)
         flagged += want
     assert 0 < flagged < len(reqs)
+
+
+def test_constant_bank_on_device():
+    """Device bank scores of the top-k hits equal the reference rule
+    (compute_delta_against_constant, fixture values for fixed pairs; mpmath
+    for the hits) within 1e-9, and the single-pair GPU path matches the
+    reference's fixture."""
+    import json
+    import os
+    import mpmath as mp
+    from dreams_rns import constants as C
+    from oracle import walk_np
+    consts = C.load_constants(200)
+    by = {c["name"]: c for c in consts}
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "constants.json")))
+    for p, q, name, want in g["delta_against"]:
+        got = C.compute_delta_against_constant(int(p), int(q), by[name]["value"], 200)
+        assert (got == want) if math.isinf(want) else abs(got - want) < 1e-9, (p, q, name, got, want)
+    ws = dr.synth.uniform_pcfs(64, seed=47, depth=300, limit_depth=900)
+    reqs = [pcf_request(dr.compile_pcf(w.a, w.b), w.a0, 900, 64, checkpoint=300) for w in ws]
+    out = dr.sweep(reqs, delta="self", topk=6, values=True, bank=consts)
+    bd = out["bank_delta"]
+    assert bd.shape == (6, len(consts))
+    mp.mp.dps = 200
+    for h, w in enumerate(out["topk_idx"]):
+        p, q = out["p"][w], out["q"][w]
+        for j in (0, 1, 29, 30, 35, len(consts) - 1):
+            want = walk_np.delta_exact(p, q, consts[j]["value"], 200)
+            got = bd[h][j]
+            assert (got == want) if math.isinf(want) else abs(got - want) < 1e-9, (h, j, got, want)
+        assert out["bank_best"][h] == consts[int(np.argmax(bd[h]))]["name"]

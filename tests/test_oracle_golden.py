@@ -117,3 +117,19 @@ def test_estimate_k_and_overflow_match_reference():
         assert estimate_K(a, b, d) == want, (a, b, d)
     for p, q, e, want in g["crt_overflowed"]:
         assert crt_overflowed(int(p), int(q), float(e)) == want, (p, q, e)
+
+
+def test_constant_bank_host_side_matches_reference():
+    """Registry, digit matching and proximity lists equal the reference's
+    (tests/golden/make_constants.py)."""
+    import json
+    import os
+    from dreams_rns import constants as C
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "constants.json")))
+    assert [[e["name"], e["sympy_expr"]] for e in C.CONSTANTS_REGISTRY] == g["registry"]
+    consts = C.load_constants(200)
+    for e, name, digits in g["match_digits"]:
+        got = C.compute_match_digits(e, consts)
+        assert got[0] == name and abs(got[1] - digits) < 1e-9, (e, got, name, digits)
+    for e, names in g["near"]:
+        assert [m["name"] for m in C.match_against_constants(e, consts, 1e-2)] == names
