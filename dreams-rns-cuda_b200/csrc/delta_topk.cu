@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(128) k_delta(DeltaArgs D) {
         size_t row = (size_t)v;
         int ti = D.per_item ? v : 0;
         if (D.bank_n > 0) {
-            row = D.rows[v / D.bank_n];
+            row = D.rows ? D.rows[v / D.bank_n] : (uint32_t)(v / D.bank_n);
             ti = v % D.bank_n;
         }
         const uint32_t* p = D.p + row * D.istride;

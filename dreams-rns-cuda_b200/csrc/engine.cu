@@ -825,32 +825,35 @@ static int enqueue_pipeline(Batch& B, cudaStream_t st) {
                                  B.tk_idx[dst].as<uint32_t>(), st);
             if (e != cudaSuccess) return cuda_fail(e, "pipeline topk");
         }
-        if (B.bank_n > 0 && !B.tk_counts.empty()) {
-            // every top-k hit's final p/q against every bank constant
-            DeltaArgs K{};
-            K.p = lim;
-            K.q = lim + L;
-            K.ps = sg;
-            K.qs = sg + 1;
-            K.nl = B.Lmax;
-            K.istride = 4 * L;
-            K.sstride = 4;
-            K.ln = B.bank_num.as<uint32_t>();
-            K.ld = B.bank_den.as<uint32_t>();
-            K.lns = B.bank_sign.as<int32_t>();
-            K.lds = nullptr;
-            K.lnl = B.bank_l;
-            K.per_item = 1;
-            K.listride = (size_t)B.bank_l;
-            K.lsstride = 1;
-            K.rows = B.tk_idx[B.tk_final].as<uint32_t>();
-            K.bank_n = B.bank_n;
-            K.n = std::min<int>(B.pipe.topk, (int)B.n_walks) * B.bank_n;
-            K.out = B.bank_out.as<double>();
-            K.maxlen = ((B.Lmax + std::max(B.Lmax, B.bank_l) + 4) + 1) & ~1;
-            e = launch_delta(K, C.sms, st);
-            if (e != cudaSuccess) return cuda_fail(e, "pipeline bank");
-        }
+    }
+    if (B.bank_n > 0) {
+        // the top-k hits (or, without a top-k, every walk): final p/q against
+        // every bank constant
+        const bool hits = !B.tk_counts.empty();
+        const size_t L = (size_t)B.Lmax;
+        DeltaArgs K{};
+        K.p = B.limbs.as<uint32_t>();
+        K.q = B.limbs.as<uint32_t>() + L;
+        K.ps = B.signs.as<int32_t>();
+        K.qs = B.signs.as<int32_t>() + 1;
+        K.nl = B.Lmax;
+        K.istride = 4 * L;
+        K.sstride = 4;
+        K.ln = B.bank_num.as<uint32_t>();
+        K.ld = B.bank_den.as<uint32_t>();
+        K.lns = B.bank_sign.as<int32_t>();
+        K.lds = nullptr;
+        K.lnl = B.bank_l;
+        K.per_item = 1;
+        K.listride = (size_t)B.bank_l;
+        K.lsstride = 1;
+        K.rows = hits ? B.tk_idx[B.tk_final].as<uint32_t>() : nullptr;
+        K.bank_n = B.bank_n;
+        K.n = (hits ? std::min<int>(B.pipe.topk, (int)B.n_walks) : (int)B.n_walks) * B.bank_n;
+        K.out = B.bank_out.as<double>();
+        K.maxlen = ((B.Lmax + std::max(B.Lmax, B.bank_l) + 4) + 1) & ~1;
+        cudaError_t e = launch_delta(K, C.sms, st);
+        if (e != cudaSuccess) return cuda_fail(e, "pipeline bank");
     }
     return DR_OK;
 }
@@ -1398,12 +1401,13 @@ int dr_batch_read_bank(int32_t batch, double* delta, int32_t max_values) {
     if (rc) return rc;
     Batch* B = find_batch(batch);
     if (!B) return DR_ERR_HANDLE;
-    if (!B->pipe_on || B->tk_counts.empty() || B->bank_n <= 0) {
-        set_error("no constant bank with top-k on this batch");
+    if (!B->pipe_on || B->bank_n <= 0) {
+        set_error("no constant bank on this batch");
         return DR_ERR_ARG;
     }
     DR_CUDA(cudaDeviceSynchronize());
-    const int64_t n = (int64_t)std::min<int>(B->pipe.topk, (int)B->n_walks) * B->bank_n;
+    const int64_t n = (int64_t)(B->tk_counts.empty() ? (int)B->n_walks
+                                                     : std::min<int>(B->pipe.topk, (int)B->n_walks)) * B->bank_n;
     DR_CUDA(cudaMemcpy(delta, B->bank_out.p, 8ull * std::min<int64_t>(n, max_values), cudaMemcpyDeviceToHost));
     return DR_OK;
 }

@@ -34,8 +34,9 @@ struct DeltaArgs {
     size_t listride, lsstride;
     double* out;
     int maxlen;                              // product length bound (limbs)
-    // bank mode (bank_n > 0): item i scores row rows[i / bank_n] of p, q
-    // against target i % bank_n (the top-k hits against a constant bank)
+    // bank mode (bank_n > 0): item i scores row rows[i / bank_n] (row i / bank_n
+    // when rows is null) of p, q against target i % bank_n (hits or every walk
+    // against a constant bank)
     const uint32_t* rows;
     int bank_n;
 };

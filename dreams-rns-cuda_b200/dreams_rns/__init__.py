@@ -19,7 +19,7 @@ from .runner import (WalkConfig, centered, compile_pcf, compute_dreams_delta_exa
                      compute_dreams_delta_float, crt_batch, crt_reconstruct, delta_batch,
                      generate_rns_primes, pcf_initial_values, run_pcf_walk, verify_pcf)
 from .cmf_walk import compile_cmf_spec, run_cmf_walk, run_cmf_walk_vec
-from . import constants, runner, synth
+from . import cmf_sweep, constants, runner, synth
 
 __version__ = "1.0.0"
 __all__ = [

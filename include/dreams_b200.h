@@ -176,11 +176,11 @@ typedef struct dr_pipeline {
 
 int dr_batch_set_pipeline(int32_t batch, const dr_pipeline *pl);
 /* Constant bank (reference constants.py:182-207 compute_delta_against_constant
- * for every registry constant, after top-k): with a pipeline that selects the
- * top-k, each run also scores the final p/q of every hit against n_consts
- * targets C_j = sign_j * num_j / den_j (limbs little-endian, l_limbs each,
- * num and den rows of one array each, den > 0).  n_consts = 0 removes it.
- * dr_batch_read_bank returns delta[hit][constant] for the top-k order.       */
+ * for every registry constant): with a device pipeline set, each run also
+ * scores the final p/q of every top-k hit (or, with no top-k, of every walk)
+ * against n_consts targets C_j = sign_j * num_j / den_j (limbs little-endian,
+ * l_limbs each, num and den rows of one array each, den > 0).  n_consts = 0
+ * removes it.  dr_batch_read_bank returns delta[hit or walk][constant].      */
 int dr_batch_set_bank(int32_t batch, int32_t n_consts, int32_t l_limbs, const uint32_t *num,
                       const int32_t *num_sign, const uint32_t *den);
 int dr_batch_read_bank(int32_t batch, double *delta, int32_t max_values);

@@ -471,3 +471,66 @@ def test_constant_bank_on_device():
             got = bd[h][j]
             assert (got == want) if math.isinf(want) else abs(got - want) < 1e-9, (h, j, got, want)
         assert out["bank_best"][h] == consts[int(np.argmax(bd[h]))]["name"]
+
+
+def test_cmf_sweep_front_end_matches_host_rule():
+    """run_cmf_sweep (device walks, CRT, overflow check, bank) reproduces the
+    reference's per-walk hit rule computed on the host from the numpy oracle."""
+    import mpmath as mp
+    from dreams_rns import constants as C
+    from dreams_rns.cmf_sweep import run_cmf_sweep
+    from dreams_rns.cmf_walk import compile_cmf_spec, shift_to_axis_offsets
+    from oracle import walk_np
+    consts = C.load_constants(200)
+    specs = [{"name": "2F1_a", "p": 2, "q": 1, "a_params": ["1/2", "1"], "b_params": ["3/2"]},
+             {"name": "3F2_b", "p": 3, "q": 2, "a_params": ["1", "1", "1"], "b_params": ["2", "2"]}]
+    trajs = {2: [[1, 1, 1], [1, 0, 1], [2, 1, 1]], 3: [[1, 1, 1, 1, 1], [1, 0, 0, 1, 1]]}
+    shifts = [{"nums": [0, 0, 0, 0, 0]}, {"nums": [1, 0, 2, 0, 1]}, {"nums": [0, 3, 0, 1, 0]}]
+    hits = []
+    for spec in specs:
+        _, h, stats = run_cmf_sweep([spec], trajs[spec["p"]], shifts, depth=120, K=64,
+                                    constants=consts, proximity=5e-2)
+        hits += h
+    mp.mp.dps = 200
+    want = []
+    for spec in specs:
+        dim = spec["p"] + spec["q"]
+        for ti, traj in enumerate(trajs[spec["p"]]):
+            blob = compile_cmf_spec(spec, trajectory=traj).serialize()
+            for si, sh in enumerate(shifts):
+                so = (shift_to_axis_offsets(sh, spec["p"]) + [1] * dim)[:dim]
+                r = walk_np.cmf_walk(blob, 120, 64, so)
+                pr = [int(p) for p in r["primes"]]
+                x, M = walk_np.crt([int(v) for v in r["p_residues"]], pr)
+                y, _ = walk_np.crt([int(v) for v in r["q_residues"]], pr)
+                p_big, q_big = walk_np.centered(x, M), walk_np.centered(y, M)
+                est = r["p_float"] / r["q_float"] if abs(r["q_float"]) > 1e-300 else float("nan")
+                if not math.isfinite(est):
+                    continue
+                try:
+                    cr = float(p_big) / float(q_big)
+                    ok = math.isfinite(cr) and ((abs(cr - est) / abs(est) < 0.01) if abs(est) > 1e-10
+                                                else abs(cr - est) < 0.01)
+                except (OverflowError, ZeroDivisionError):
+                    ok = False
+                prox = C.match_against_constants(est, consts, 5e-2)
+                log_q = r["log_scale"] + (math.log(abs(r["q_float"])) if abs(r["q_float"]) > 1e-300 else 0.0)
+                cand = ([next(c for c in consts if c["name"] == m["name"]) for m in prox] if prox
+                        else [c for c in consts if abs(est - c["value_float"]) < 1.0])
+                best, bc = float("-inf"), None
+                for c in cand:
+                    if ok:
+                        d = walk_np.delta_exact(p_big, q_big, c["value"], 200)
+                    else:
+                        err = abs(est - c["value_float"])
+                        d = -(1.0 + math.log(err) / log_q) if err > 0 and log_q > 0 else float("-inf")
+                    if d > best:
+                        best, bc = d, c["name"]
+                if best > 0 or prox:
+                    want.append((spec["name"], ti, si, bc, best, [m["name"] for m in prox]))
+    got = [(h["cmf_name"], h["traj_idx"], h["shift_idx"], h["best_const"], h["best_delta"],
+            h["proximity_matches"]) for h in hits]
+    assert len(got) == len(want) and len(want) > 0
+    for g, w in zip(got, want):
+        assert g[:4] == w[:4] and g[5] == w[5], (g, w)
+        assert (g[4] == w[4]) if math.isinf(w[4]) else abs(g[4] - w[4]) < 1e-9, (g, w)
