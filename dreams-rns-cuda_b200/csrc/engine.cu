@@ -773,12 +773,6 @@ static int enqueue_pipeline(Batch& B, cudaStream_t st) {
                                    B.crt_in.as<uint64_t>() + g.off, B.crt_out.as<uint32_t>() + g.off);
         if (e != cudaSuccess) return cuda_fail(e, "pipeline crt");
     }
-    if (B.has_shadow && !B.crt_groups.empty()) {
-        cudaError_t e = launch_crt_check(B.limbs.as<uint32_t>(), B.signs.as<int32_t>(), B.Lmax,
-                                         (int)B.n_walks, B.walks.as<DevWalk>(), B.shadow.as<double>(),
-                                         B.status.as<uint32_t>(), st);
-        if (e != cudaSuccess) return cuda_fail(e, "pipeline crt check");
-    }
     if (B.pipe.delta_mode != DR_DELTA_NONE) {
         DeltaArgs D{};
         const bool self = B.pipe.delta_mode == DR_DELTA_SELF;
@@ -856,6 +850,15 @@ static int enqueue_pipeline(Batch& B, cudaStream_t st) {
         if (e != cudaSuccess) return cuda_fail(e, "pipeline bank");
     }
     return DR_OK;
+}
+
+// CRT overflow flags: the pipeline's values against the finished FP64 shadow.
+static int enqueue_crt_check(Batch& B, cudaStream_t st) {
+    if (!B.pipe_on || !B.has_shadow || B.crt_groups.empty()) return DR_OK;
+    cudaError_t e = launch_crt_check(B.limbs.as<uint32_t>(), B.signs.as<int32_t>(), B.Lmax,
+                                     (int)B.n_walks, B.walks.as<DevWalk>(), B.shadow.as<double>(),
+                                     B.status.as<uint32_t>(), st);
+    return e == cudaSuccess ? DR_OK : cuda_fail(e, "pipeline crt check");
 }
 
 static void batch_args(Batch& B, WalkArgs& wa, ShadowArgs& sa) {
@@ -968,15 +971,20 @@ static int enqueue_batch(Batch& B, cudaStream_t st, std::vector<cudaEvent_t>* en
             }
         }
     }
-    // rejoin every forked stream (also on errors, so a capture can end cleanly)
+    // rejoin the walk streams first: CRT, delta, top-k and the bank need only
+    // the residues and run while the FP64 shadow chains are still going; the
+    // shadow streams join before the CRT overflow check, which reads them
+    // (every forked stream is rejoined, also on errors, so a capture ends cleanly)
+    const size_t n_hi = std::min(k_hi, C.hpool.size());
     for (size_t i = 0; i < used.size(); ++i) {
         cudaEventRecord(B.joins[i], used[i]);
-        cudaStreamWaitEvent(st, B.joins[i], 0);
+        if (i >= n_hi) cudaStreamWaitEvent(st, B.joins[i], 0);
     }
+    if (rc == DR_OK && B.pipe_on) rc = enqueue_pipeline(B, st);
+    for (size_t i = 0; i < n_hi && i < used.size(); ++i) cudaStreamWaitEvent(st, B.joins[i], 0);
     if (rc != DR_OK) return rc;
     DR_CUDA(cudaGetLastError());
-    if (B.pipe_on) return enqueue_pipeline(B, st);
-    return DR_OK;
+    return enqueue_crt_check(B, st);
 }
 
 // Every launch group alone, one after another on one stream, timed with
