@@ -320,6 +320,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the rational, CMF-sweep and serving measurements")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the built-in launch-shape policy (profiler captures)")
     ap.add_argument("--walks", type=int, default=N_WALKS,
                     help="PCFs per GPU (default 4096, the benchmark workload; smaller values "
                          "give the same workload shape for profiler captures)")
@@ -372,7 +374,7 @@ def main():
 
     N.init(local)
     reqs = [pcf_request(b, w.a0, DEPTH, K, checkpoint=CHECKPOINT) for b, w in zip(blobs, ws)]
-    tuned = dr.autotune(reqs)          # launch shape by measurement (untimed set-up)
+    tuned = None if args.no_autotune else dr.autotune(reqs)   # launch shape by measurement (untimed set-up)
     batch = WalkBatch(reqs)
     batch.set_pipeline(delta="self", topk=TOPK)
     stream = torch.cuda.Stream()       # a real stream: the legacy default stream's handle is 0

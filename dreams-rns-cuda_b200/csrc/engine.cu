@@ -50,7 +50,8 @@ int cuda_fail(cudaError_t e, const char* where) {
     } while (0)
 
 int get_plan(const uint8_t* blob, uint64_t size, std::shared_ptr<Plan>* out, std::string* err) {
-    std::string key(reinterpret_cast<const char*>(blob), (size_t)size);
+    // the cache is keyed by the blob's bytes; lookups hash them in place
+    const std::string_view key(reinterpret_cast<const char*>(blob), (size_t)size);
     {
         std::lock_guard<std::mutex> lk(g_ctx->mu);
         auto it = g_ctx->plan_cache.find(key);
@@ -64,9 +65,11 @@ int get_plan(const uint8_t* blob, uint64_t size, std::shared_ptr<Plan>* out, std
     int rc = parse_blob(blob, size, &raw, err);
     if (rc == DR_OK) rc = plan_program(raw, plan.get(), err);
     if (rc != DR_OK) return rc;
+    plan->fcomp = float_companion_shape(*plan);
+    plan->blob.assign(key.data(), key.size());
     std::lock_guard<std::mutex> lk(g_ctx->mu);
     if (g_ctx->plan_cache.size() > 200000) g_ctx->plan_cache.clear();
-    g_ctx->plan_cache.emplace(std::move(key), plan);
+    g_ctx->plan_cache.emplace(std::string_view(plan->blob), plan);
     *out = plan;
     return DR_OK;
 }
@@ -219,6 +222,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     std::vector<DevProgram> dprogs(n_programs);
     std::vector<uint4> code;
     std::vector<int64_t> consts;
+    code.reserve((size_t)n_programs * 24);
+    consts.reserve((size_t)n_programs * 8);
     for (int32_t i = 0; i < n_programs; ++i) {
         if (blob_offsets[i + 1] < blob_offsets[i]) {
             set_error("blob_offsets not increasing");
@@ -250,7 +255,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         d.n_streams = P.n_streams;
         d.zero_reg = P.zero_reg;
         d.shadow_fd = (!P.has_inv && (P.cls == CLS_COMPANION || P.cls == CLS_DENSE)) ? 1u : 0u;
-        d.fcomp = float_companion_shape(P) ? 1u : 0u;
+        d.fcomp = P.fcomp ? 1u : 0u;
         dprogs[i] = d;
     }
 

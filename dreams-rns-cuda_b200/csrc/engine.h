@@ -7,6 +7,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <string_view>
 #include <unordered_map>
 #include <vector>
 
@@ -71,7 +72,8 @@ struct Context {
     std::vector<cudaStream_t> hpool;  // high-priority streams for the FP64 shadow launches
     DevBuf primes, pinv, r2;   // DR_MAX_K-entry prime table
     std::mutex mu;
-    std::unordered_map<std::string, std::shared_ptr<Plan>> plan_cache;
+    // plan cache keyed by program bytes (views into each Plan's own copy)
+    std::unordered_map<std::string_view, std::shared_ptr<Plan>> plan_cache;
     std::map<int, std::shared_ptr<CrtSet>> crt_std;  // CRT tables of the standard primes
     std::map<std::string, std::pair<uint32_t, uint32_t>> tuned;   // signature -> (chunk, warps/block)
     std::mutex cache_mu;

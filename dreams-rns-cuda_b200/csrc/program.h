@@ -36,6 +36,8 @@ struct Plan {
     bool has_inv = false;           // the executed prefix contains INV
     std::vector<Insn> exec;         // executed prefix, uncompacted (bounds analysis)
     std::vector<int32_t> dirs;
+    bool fcomp = false;             // float_companion_shape(*this), set once planned
+    std::string blob;               // the program bytes (plan cache key storage)
 };
 
 // Status codes mirror the public DR_ERR_* values.

@@ -148,7 +148,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     for (Req* r : sel)
         if (r->shadow_mode == SHADOW_INTERP && !r->shadow_done) {
             ++n_interp;
-            ne_max = std::max<uint64_t>(ne_max, shadow_entries(r->plan->m, float_companion_shape(*r->plan)));
+            ne_max = std::max<uint64_t>(ne_max, shadow_entries(r->plan->m, r->plan->fcomp));
         }
     uint64_t seg_shadow = 8192;
     if (n_interp) {
@@ -189,7 +189,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
             d.c_off = (uint32_t)consts.size(); d.n_consts = (uint32_t)P.consts.size();
             consts.insert(consts.end(), P.consts.begin(), P.consts.end());
             d.n_streams = P.n_streams; d.zero_reg = P.zero_reg;
-            d.fcomp = float_companion_shape(P) ? 1u : 0u;
+            d.fcomp = P.fcomp ? 1u : 0u;
             pi = (int)progs.size();
             progs.push_back(d);
             pidx.emplace(r->blob, pi);
