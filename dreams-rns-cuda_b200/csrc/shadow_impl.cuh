@@ -386,7 +386,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // Steps per staged chunk of the chain kernel (entries * steps = 16 doubles
 // per lane and buffer, at least two steps): a chunk of chain steps takes
 // thousands of cycles, far more than the copy of the next one, so small
-// buffers suffice and leave shared memory to the walk kernels running beside.
+// buffers suffice (longer chunks measured slower).
 __host__ __device__ constexpr int chain_chunk_steps(int ne) { return ne >= 8 ? 2 : 16 / ne; }
 
 // Evaluation: each warp takes items of kEvalSteps steps of one segment and
