@@ -16,8 +16,9 @@ from .engine import (WalkBatch, WalkRequest, autotune, cmf_request, pcf_request,
 from .gpu_walk import (gpu_available, run_cmf_walk_batch_gpu, run_cmf_walk_gpu,
                        run_pcf_walk_batch_gpu, run_pcf_walk_gpu)
 from .runner import (WalkConfig, centered, compile_pcf, compute_dreams_delta_exact,
-                     compute_dreams_delta_float, crt_batch, crt_reconstruct, delta_batch,
-                     generate_rns_primes, pcf_initial_values, run_pcf_walk, verify_pcf)
+                     compute_dreams_delta_float, crt_batch, crt_overflowed, crt_reconstruct,
+                     delta_batch, estimate_K, generate_rns_primes, pcf_initial_values,
+                     run_pcf_walk, verify_pcf)
 from .cmf_walk import compile_cmf_spec, run_cmf_walk, run_cmf_walk_vec
 from . import cmf_sweep, constants, runner, synth
 
@@ -30,5 +31,5 @@ __all__ = [
     "gpu_available", "run_pcf_walk_gpu", "run_pcf_walk_batch_gpu", "run_cmf_walk_gpu",
     "run_cmf_walk_batch_gpu", "run_cmf_walk", "run_cmf_walk_vec", "vec_request", "compile_cmf_spec",
     "WalkBatch", "WalkRequest", "pcf_request", "cmf_request", "run_walks", "sweep", "autotune", "crt_batch",
-    "delta_batch",
+    "delta_batch", "estimate_K", "crt_overflowed",
 ]
