@@ -522,6 +522,21 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
 
     build_mark(4);
     // ---- launch geometry
+    // expected duration of the walk kernels: algorithmic lane-ops per
+    // prime-step (difference-table streams, product, reduction; the bytecode
+    // interpreter ~10x that) at the ~1.7e13 lane-ops/s the walk kernels reach;
+    // the FP64 shadow chains beside them are sized against it
+    double walk_ops = 0.0;
+    for (int32_t w = 0; w < n_walks; ++w) {
+        const DevWalk& W = dwalks[w];
+        const DevProgram& G = dprogs[W.prog];
+        const double m = G.m, D = std::max<uint32_t>(G.degree, 1);
+        double per = 2.0 * m * D + m * (m + 4.0 + 2.0 * std::max(0.0, m - 2.0));
+        if (G.cls == CLS_DENSE) per *= m;
+        if (G.cls == CLS_INTERP) per *= 10.0;
+        walk_ops += per * (double)W.K * (double)W.depth;
+    }
+    const double walk_ns = walk_ops / 1.7e13 * 1e9;
     const int wpb = (tune && tune->warps_per_block) ? (int)tune->warps_per_block
                   : tuned_wpb ? (int)tuned_wpb : 4;
     B->wpb_used = (uint32_t)wpb;
@@ -530,14 +545,16 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         L.queue = q++;
         if (L.kind == 1) {
             L.queue2 = q++;
-            if ((rc = shadow_interp_geometry(L, max_dim, C.sms, shadow_list.data() + L.off))) return rc;
+            if ((rc = shadow_interp_geometry(L, max_dim, C.sms, shadow_list.data() + L.off, true, walk_ns)))
+                return rc;
             continue;
         }
         if (L.kind == 2) {
             const size_t per_warp = (size_t)L.rows_per_warp * 32 * 8;
-            L.block = 32 * kChainWarps;
-            L.smem = std::max(per_warp * kChainWarps, chain_hog_smem());
-            if (per_warp * kChainWarps > L.smem) {
+            const bool coloc = chain_colocate(shadow_list.data() + L.off, L.count, L.m, walk_ns);
+            L.block = coloc ? 32 : 32 * kChainWarps;
+            L.smem = coloc ? per_warp : std::max(per_warp * kChainWarps, chain_hog_smem());
+            if (per_warp * (L.block / 32) > L.smem || L.smem > 227 * 1024) {
                 set_error("program needs more shared memory per warp than a block offers");
                 return DR_ERR_UNSUPPORTED;
             }
@@ -549,7 +566,9 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
                 set_error("kernel cannot be resident with this shared memory size");
                 return DR_ERR_UNSUPPORTED;
             }
-            L.grid = std::min(chain_blocks(shadow_list.data() + L.off, L.count), occ * C.sms);
+            L.grid = coloc ? std::min((int)L.items, occ * C.sms)
+                           : std::min(chain_blocks(shadow_list.data() + L.off, L.count, L.m, walk_ns),
+                                      occ * C.sms);
             continue;
         }
         L.block = 32 * wpb;
@@ -686,10 +705,20 @@ size_t chain_hog_smem() {
     return bytes;
 }
 
-int chain_blocks(const DevShadowSeg* segs, uint32_t count) {
+bool chain_colocate(const DevShadowSeg* segs, uint32_t count, uint32_t m, double walk_ns) {
+    uint64_t longest = 0;
+    if (count) longest = segs[0].s1 - segs[0].s0;   // sorted longest first
+    for (uint32_t k = 0; k < count && k < 64; ++k) longest = std::max<uint64_t>(longest, segs[k].s1 - segs[k].s0);
+    // shared issue slots slow a chain by ~1.6x; keep a margin on top
+    return walk_ns > 0 && 3.0 * (double)longest * chain_step_ns(m) < walk_ns;
+}
+
+int chain_blocks(const DevShadowSeg* segs, uint32_t count, uint32_t m, double walk_ns) {
     // segments are sorted longest first; a warp takes 32 of them, so item k
     // lasts as long as segment 32k.  Enough warps that the total chain work
-    // spread over them ends with the longest chain, plus one block of slack.
+    // spread over them ends with the longest chain, or with the walk kernels
+    // when those take longer (a chain step is ~300 ns), plus one block of slack.
+    const double kStepNs = chain_step_ns(m);
     uint64_t total = 0, longest = 0;
     for (uint32_t k = 0; k < count; k += 32) {
         const uint64_t len = segs[k].s1 - segs[k].s0;
@@ -697,13 +726,14 @@ int chain_blocks(const DevShadowSeg* segs, uint32_t count) {
         longest = std::max<uint64_t>(longest, std::max<uint64_t>(len, 1));
     }
     const uint32_t items = (count + 31) / 32;
-    const uint64_t warps = longest ? (total + longest - 1) / longest : 1;
+    const double span = std::max((double)longest * kStepNs, walk_ns);
+    const uint64_t warps = span > 0 ? (uint64_t)std::ceil((double)total * kStepNs / span) : 1;
     const uint64_t blocks = (warps + kChainWarps - 1) / kChainWarps + 1;
     return (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (items + kChainWarps - 1) / kChainWarps));
 }
 
 int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs,
-                           bool whole_sm) {
+                           bool whole_sm, double walk_ns) {
     const uint32_t base = L.rows_regs + max_dim + L.m * L.m;
     uint32_t U = 1;
     for (uint32_t u : {4u, 2u})
@@ -729,16 +759,18 @@ int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevSh
         return DR_ERR_UNSUPPORTED;
     }
     L.grid = std::max(1, std::min((int)((L.items + wpb - 1) / wpb), occ * sms));
-    L.block2 = 32 * kChainWarps;
-    L.smem2 = shadow_chain_smem(L.m, (L.cls & 1u) != 0) * kChainWarps;
-    if (whole_sm) L.smem2 = std::max(L.smem2, chain_hog_smem());
+    const bool coloc = whole_sm && chain_colocate(segs, L.count, L.m, walk_ns);
+    L.block2 = coloc ? 32 : 32 * kChainWarps;
+    L.smem2 = shadow_chain_smem(L.m, (L.cls & 1u) != 0) * (L.block2 / 32);
+    if (whole_sm && !coloc) L.smem2 = std::max(L.smem2, chain_hog_smem());
     e = shadow_chain_dispatch(L.m, L.cls, 0, L.block2, L.smem2, nullptr, sa, &occ);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
     if (occ < 1) {
         set_error("kernel cannot be resident with this shared memory size");
         return DR_ERR_UNSUPPORTED;
     }
-    L.grid2 = std::min(chain_blocks(segs, L.count), occ * sms);
+    L.grid2 = coloc ? std::min((int)L.items2, occ * sms)
+                    : std::min(chain_blocks(segs, L.count, L.m, walk_ns), occ * sms);
     return DR_OK;
 }
 

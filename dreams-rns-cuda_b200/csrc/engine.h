@@ -114,14 +114,23 @@ struct LaunchSpec {
 // whole_sm: the chain blocks claim a whole SM's shared memory (batches,
 // whose walks run beside them); serving waves request only what they use.
 int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs,
-                           bool whole_sm = true);
+                           bool whole_sm = true, double walk_ns = 0.0);
 
 // FP64 chain kernels (interpreted chain, integer-difference shadow) run as
 // blocks of kChainWarps warps that claim a whole SM's shared memory, so no
 // walk block shares their SM's issue slots; the grid is sized so the chains
 // finish with the longest one.
 constexpr int kChainWarps = 4;
-int chain_blocks(const DevShadowSeg* segs, uint32_t count);
+// walk_ns: expected duration of the walk kernels running beside the chains
+// (0: unknown); the chains get enough SMs to finish within the longer of it
+// and their own longest chain, and no more.
+int chain_blocks(const DevShadowSeg* segs, uint32_t count, uint32_t m, double walk_ns = 0.0);
+// Whether chains this short next to the walks run best spread over all SMs
+// beside the walk warps (one warp per block, no whole-SM claim): their
+// longest chain, even slowed by sharing issue slots, ends well before the walks.
+bool chain_colocate(const DevShadowSeg* segs, uint32_t count, uint32_t m, double walk_ns);
+// FP64 chain step time (ns) of an m x m shadow, rescaling every step.
+inline double chain_step_ns(uint32_t m) { return 75.0 * m * m; }
 size_t chain_hog_smem();
 
 // Builds the interpreted-shadow launches of one (m, shape) group (shape bit 0:
