@@ -286,12 +286,16 @@ def bench_serving(seconds=3.0, rate=1000.0):
             arrivals.append((t, kind, req))
     lat = {}
     kinds = {}
-    with WalkServer(max_inflight=3) as srv:
+    with WalkServer(max_inflight=6) as srv:
         t0 = time.perf_counter()
         ids = []
         for at, kind, req in arrivals:
-            while time.perf_counter() - t0 < at:
-                pass
+            while True:     # wait for the arrival time: sleep, then spin the last half millisecond
+                left = at - (time.perf_counter() - t0)
+                if left <= 0:
+                    break
+                if left > 1e-3:
+                    time.sleep(left - 5e-4)
             rid = srv.submit(req)
             ids.append(rid)
             kinds[rid] = kind

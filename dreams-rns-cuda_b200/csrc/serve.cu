@@ -24,6 +24,7 @@
 #include <unordered_map>
 
 #include "../../include/dreams_b200.h"
+#include "../../include/dreams_b200_debug.h"
 #include "engine.h"
 #include "host_common.h"
 #include "launch.h"
@@ -60,23 +61,41 @@ struct Req {
 
 struct Wave {
     cudaStream_t st = nullptr;
-    cudaEvent_t ev = nullptr;
+    cudaEvent_t ev0 = nullptr, ev = nullptr;
     bool busy = false;
+    bool has_long = false;                // carries requests that need more waves
+    size_t log = 0;                       // index of this launch in Server::wlog
     std::vector<int64_t> reqs;            // requests with a segment in this wave
     std::vector<uint8_t> walk_final;      // per request: walk part finishes here
     std::vector<uint8_t> shadow_final;    // per request: shadow finishes here
     std::vector<uint64_t> walk_end, shadow_end;
     std::vector<uint64_t> res_off;        // output offsets of finishing walks
     std::vector<uint32_t> widx;           // walk-table index per request
-    DevBuf progs, code, consts, walks, axis, tiles, groups, done_ctr, chunkP, chunkSig, segs,
-        queues, res, shadow, status, mf, eval_items;
+    // one upload (programs, code, constants, walks, axes, tiles, groups,
+    // shadow segments, eval items) and one zero-filled block (combine
+    // counters, queues, status); buffers only grow, from the engine's pool,
+    // so a wave never frees device memory while other waves run
+    DevBuf up, zero, chunkP, chunkSig, res, shadow, mf;
+    uint8_t* h_up = nullptr;              // pinned staging of the upload
     uint32_t* h_res = nullptr;            // pinned outputs
     double* h_sh = nullptr;
     uint32_t* h_st = nullptr;
-    size_t h_res_cap = 0, h_walk_cap = 0;
+    size_t h_up_cap = 0, h_res_cap = 0, h_sh_cap = 0, h_st_cap = 0;
     uint64_t n_res = 0;
     uint32_t n_walks = 0;
     uint64_t prime_steps = 0;
+    uint64_t n_tiles = 0, max_span = 0;   // walk tiles and longest shadow segment of the launch
+    Wave() {
+        for (DevBuf* b : {&up, &zero, &chunkP, &chunkSig, &res, &shadow, &mf}) b->pooled = true;
+    }
+};
+
+// Per-launch record of the scheduler (dr_debug_serve_waves).
+struct WaveLog {
+    double t_sel = 0, t_launched = 0, t_harvest = 0;   // ms since dr_serve_open
+    float gpu_ms = 0;
+    uint32_t n_req = 0, has_long = 0, wave = 0;
+    uint64_t walk_tiles = 0, shadow_span = 0;
 };
 
 struct Server {
@@ -94,6 +113,8 @@ struct Server {
     std::vector<uint32_t> free_slots, free_shadow;
     std::deque<Wave> waves;               // deque: elements never move
     uint64_t completed = 0, prime_steps = 0;
+    Clock::time_point t_open;
+    std::vector<WaveLog> wlog;            // capped at kMaxWaveLog entries
     std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, size_t>, int> occ_cache;
     int error = DR_OK;
     std::string error_msg;
@@ -109,17 +130,45 @@ Server* find_server(int32_t h) {
     return it == g_servers.end() ? nullptr : it->second.get();
 }
 
+constexpr size_t kMaxWaveLog = 1u << 16;
+
+double ms_since(const Server& S, Clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(t - S.t_open).count();
+}
+
 uint64_t request_bytes(const Req& r) {
     const uint64_t nb = (r.d.K + 31) / 32;
     return nb * (kServeStride + 32) * 4 + (r.shadow_mode ? kShadowStateStride * 8 : 0) + 8ull * r.d.K;
 }
 
-template <class T>
-cudaError_t put(DevBuf& b, const std::vector<T>& v, cudaStream_t st) {
-    cudaError_t e = b.alloc(sizeof(T) * std::max<size_t>(v.size(), 1));
-    if (e != cudaSuccess || v.empty()) return e;
-    return cudaMemcpyAsync(b.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, st);
+// Grow-only device buffer with headroom, so steady-state waves allocate nothing.
+cudaError_t grow(DevBuf& b, size_t n) {
+    if (b.p && n <= b.bytes) return cudaSuccess;
+    return b.alloc(std::max<size_t>(n + n / 2, 1u << 16));
 }
+
+// Grow-only pinned host buffer (cudaFreeHost waits for the whole device, so
+// growth doubles and is rare).
+template <class T>
+cudaError_t grow_host(T*& p, size_t& cap, size_t n) {
+    if (p && n <= cap) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = std::max<size_t>(2 * n, (1u << 18) / sizeof(T));
+    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), sizeof(T) * cap);
+    if (e != cudaSuccess) { p = nullptr; cap = 0; }
+    return e;
+}
+
+// Layout of the packed upload: byte offset of each array, 16-byte aligned.
+struct Packer {
+    size_t total = 0;
+    template <class T> size_t add(const std::vector<T>& v) {
+        const size_t off = total;
+        total += (sizeof(T) * v.size() + 15) & ~size_t(15);
+        return off;
+    }
+};
 
 int occupancy(Server& S, int kind, uint32_t cls, uint32_t m, uint32_t D, int block, size_t smem) {
     auto key = std::make_tuple(kind, cls, m, D, smem);
@@ -166,6 +215,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     std::map<std::tuple<int, uint32_t, uint32_t, uint32_t>, std::vector<DevShadowSeg>> ssets;
     uint32_t slots = 0;
     uint64_t nres = 0, ps = 0;
+    W.max_span = 0;
     W.reqs.clear();
     W.walk_final.clear();
     W.shadow_final.clear();
@@ -246,6 +296,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
         if (r->shadow_mode != SHADOW_NONE && !r->shadow_done) {
             se = std::min<uint64_t>(r->d.depth, r->shadow_next + seg_shadow);
             sfinal = se >= r->d.depth;
+            W.max_span = std::max<uint64_t>(W.max_span, se - r->shadow_next);
             DevShadowSeg g{wi, (uint32_t)r->shadow_slot, r->shadow_next, se, 0, 0, 0};
             if (r->shadow_mode == SHADOW_INTFD)
                 ssets[std::make_tuple(2, (uint32_t)P.cls, P.m, (uint32_t)r->tdeg)].push_back(g);
@@ -334,71 +385,79 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     cudaStream_t st = W.st;
     cudaError_t e = cudaSuccess;
 #define SV(x) do { e = (x); if (e != cudaSuccess) return cuda_fail(e, #x); } while (0)
-    SV(put(W.progs, progs, st));
-    SV(put(W.code, code, st));
-    SV(put(W.consts, consts, st));
-    SV(put(W.walks, walks, st));
-    SV(put(W.axis, axis, st));
-    SV(put(W.tiles, tiles, st));
-    SV(put(W.groups, groups, st));
-    SV(put(W.segs, segs, st));
-    SV(put(W.eval_items, eval_items, st));
-    SV(W.mf.alloc(8ull * std::max<uint64_t>(mf_doubles, 1)));
-    SV(W.done_ctr.alloc(4ull * std::max<size_t>(groups.size(), 1)));
-    SV(cudaMemsetAsync(W.done_ctr.p, 0, 4ull * std::max<size_t>(groups.size(), 1), st));
-    SV(W.chunkP.alloc(4ull * std::max<uint32_t>(slots, 1) * kServeStride));
-    SV(W.chunkSig.alloc(4ull * std::max<uint32_t>(slots, 1) * 32));
-    SV(W.queues.alloc(4ull * std::max<uint32_t>(q, 1)));
-    SV(cudaMemsetAsync(W.queues.p, 0, 4ull * std::max<uint32_t>(q, 1), st));
-    SV(W.res.alloc(8ull * W.n_res));
-    SV(W.shadow.alloc(8ull * 6 * std::max<uint32_t>(W.n_walks, 1)));
-    SV(W.status.alloc(4ull * std::max<uint32_t>(W.n_walks, 1)));
-    SV(cudaMemsetAsync(W.status.p, 0, 4ull * std::max<uint32_t>(W.n_walks, 1), st));
+    SV(cudaEventRecord(W.ev0, st));
+    W.n_tiles = tiles.size();
+    Packer pk;
+    const size_t o_progs = pk.add(progs), o_code = pk.add(code), o_consts = pk.add(consts),
+                 o_walks = pk.add(walks), o_axis = pk.add(axis), o_tiles = pk.add(tiles),
+                 o_groups = pk.add(groups), o_segs = pk.add(segs), o_eval = pk.add(eval_items);
+    SV(grow_host(W.h_up, W.h_up_cap, pk.total + 16));
+    auto stage = [&](size_t off, const auto& v) {
+        if (!v.empty()) std::memcpy(W.h_up + off, v.data(), sizeof(v[0]) * v.size());
+    };
+    stage(o_progs, progs); stage(o_code, code); stage(o_consts, consts); stage(o_walks, walks);
+    stage(o_axis, axis); stage(o_tiles, tiles); stage(o_groups, groups); stage(o_segs, segs);
+    stage(o_eval, eval_items);
+    SV(grow(W.up, pk.total + 16));
+    if (pk.total) SV(cudaMemcpyAsync(W.up.p, W.h_up, pk.total, cudaMemcpyHostToDevice, st));
+    auto at = [&](size_t off) { return static_cast<uint8_t*>(W.up.p) + off; };
+    // zero-filled: combine counters | queues | status
+    const size_t n_done = std::max<size_t>(groups.size(), 1), n_q = std::max<uint32_t>(q, 1),
+                 n_st = std::max<uint32_t>(W.n_walks, 1);
+    const size_t zbytes = 4ull * (n_done + n_q + n_st);
+    SV(grow(W.zero, zbytes));
+    SV(cudaMemsetAsync(W.zero.p, 0, zbytes, st));
+    uint32_t* z_done = W.zero.as<uint32_t>();
+    uint32_t* z_queue = z_done + n_done;
+    uint32_t* z_status = z_queue + n_q;
+    SV(grow(W.mf, 8ull * std::max<uint64_t>(mf_doubles, 1)));
+    SV(grow(W.chunkP, 4ull * std::max<uint32_t>(slots, 1) * kServeStride));
+    SV(grow(W.chunkSig, 4ull * std::max<uint32_t>(slots, 1) * 32));
+    SV(grow(W.res, 8ull * W.n_res));
+    SV(grow(W.shadow, 8ull * 6 * std::max<uint32_t>(W.n_walks, 1)));
     WalkArgs wa{};
-    wa.progs = W.progs.as<DevProgram>(); wa.code = W.code.as<uint4>(); wa.consts = W.consts.as<int64_t>();
-    wa.walks = W.walks.as<DevWalk>(); wa.axis = W.axis.as<int64_t>(); wa.groups = W.groups.as<DevGroup>();
-    wa.group_done = W.done_ctr.as<uint32_t>(); wa.chunk_P = W.chunkP.as<uint32_t>();
+    wa.progs = reinterpret_cast<const DevProgram*>(at(o_progs));
+    wa.code = reinterpret_cast<const uint4*>(at(o_code));
+    wa.consts = reinterpret_cast<const int64_t*>(at(o_consts));
+    wa.walks = reinterpret_cast<const DevWalk*>(at(o_walks));
+    wa.axis = reinterpret_cast<const int64_t*>(at(o_axis));
+    wa.groups = reinterpret_cast<const DevGroup*>(at(o_groups));
+    wa.group_done = z_done; wa.chunk_P = W.chunkP.as<uint32_t>();
     wa.chunk_stride = kServeStride; wa.chunk_sig = W.chunkSig.as<uint32_t>();
     wa.state_P = S.stP.as<uint32_t>(); wa.state_sig = S.stSig.as<uint32_t>();
     wa.primes = C.primes.as<uint32_t>(); wa.pinv = C.pinv.as<uint32_t>(); wa.r2 = C.r2.as<uint32_t>();
-    wa.p_res = W.res.as<uint32_t>(); wa.q_res = W.res.as<uint32_t>() + W.n_res; wa.status = W.status.as<uint32_t>();
+    wa.p_res = W.res.as<uint32_t>(); wa.q_res = W.res.as<uint32_t>() + W.n_res; wa.status = z_status;
     ShadowArgs sa{};
     sa.progs = wa.progs; sa.code = wa.code; sa.consts = wa.consts; sa.walks = wa.walks; sa.axis = wa.axis;
     sa.shadow = W.shadow.as<double>(); sa.n_walks = W.n_walks; sa.status = wa.status;
     sa.state = S.stShadow.as<double>();
     sa.mf = W.mf.as<double>();
+    const DevTile* d_tiles = reinterpret_cast<const DevTile*>(at(o_tiles));
+    const DevShadowSeg* d_segs = reinterpret_cast<const DevShadowSeg*>(at(o_segs));
+    const uint32_t* d_eval = reinterpret_cast<const uint32_t*>(at(o_eval));
     for (auto& s : L) {
         if (s.items == 0 && s.items2 == 0) continue;
         if (s.kind == 0) {
-            wa.tiles = W.tiles.as<DevTile>() + s.off; wa.n_tiles = s.count;
-            wa.queue = W.queues.as<uint32_t>() + s.queue;
+            wa.tiles = d_tiles + s.off; wa.n_tiles = s.count;
+            wa.queue = z_queue + s.queue;
             wa.rows_regs = s.rows_regs; wa.rows_consts = s.rows_consts; wa.rows_stage = s.rows_stage;
             wa.rows_per_warp = s.rows_per_warp;
             SV(walk_dispatch(s.cls, s.m, s.D, s.grid, s.block, s.smem, st, wa, nullptr));
         } else {
-            sa.segs = W.segs.as<DevShadowSeg>() + s.off; sa.n_items = s.items; sa.n_list = s.count;
-            sa.queue = W.queues.as<uint32_t>() + s.queue; sa.rows_regs = s.rows_regs;
+            sa.segs = d_segs + s.off; sa.n_items = s.items; sa.n_list = s.count;
+            sa.queue = z_queue + s.queue; sa.rows_regs = s.rows_regs;
             sa.rows_per_warp = s.rows_per_warp;
-            if (s.kind == 1) SV(launch_shadow_interp(s, sa, W.queues.as<uint32_t>(), W.eval_items.as<uint32_t>(), st));
+            if (s.kind == 1) SV(launch_shadow_interp(s, sa, z_queue, d_eval, st));
             else SV(shadow_fd_dispatch(s.cls, s.m, s.D, s.grid, s.block, s.smem, st, sa, nullptr));
         }
     }
     // outputs back to pinned host memory
-    if (W.h_res_cap < 2 * W.n_res) {
-        if (W.h_res) cudaFreeHost(W.h_res);
-        W.h_res_cap = 2 * W.n_res + 1024;
-        SV(cudaMallocHost(&W.h_res, 4 * W.h_res_cap));
-    }
-    if (W.h_walk_cap < W.n_walks) {
-        if (W.h_sh) cudaFreeHost(W.h_sh);
-        if (W.h_st) cudaFreeHost(W.h_st);
-        W.h_walk_cap = W.n_walks + 256;
-        SV(cudaMallocHost(&W.h_sh, 8 * 6 * W.h_walk_cap));
-        SV(cudaMallocHost(&W.h_st, 4 * W.h_walk_cap));
-    }
+    SV(grow_host(W.h_res, W.h_res_cap, 2 * W.n_res));
+    SV(grow_host(W.h_sh, W.h_sh_cap, 3ull * W.n_walks));
+    SV(grow_host(W.h_st, W.h_st_cap, (size_t)W.n_walks));
     SV(cudaMemcpyAsync(W.h_res, W.res.p, 8ull * W.n_res, cudaMemcpyDeviceToHost, st));
     SV(cudaMemcpyAsync(W.h_sh, W.shadow.p, 8ull * 3 * W.n_walks, cudaMemcpyDeviceToHost, st));
-    SV(cudaMemcpyAsync(W.h_st, W.status.p, 4ull * W.n_walks, cudaMemcpyDeviceToHost, st));
+    SV(cudaMemcpyAsync(W.h_st, z_status, 4ull * W.n_walks, cudaMemcpyDeviceToHost, st));
     SV(cudaEventRecord(W.ev, st));
 #undef SV
     W.busy = true;
@@ -415,6 +474,12 @@ void release(Server& S, Req& r) {
 }
 
 void harvest(Server& S, Wave& W) {
+    if (W.log < S.wlog.size()) {
+        WaveLog& g = S.wlog[W.log];
+        g.t_harvest = ms_since(S, Clock::now());
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, W.ev0, W.ev) == cudaSuccess) g.gpu_ms = ms;
+    }
     for (size_t i = 0; i < W.reqs.size(); ++i) {
         auto it = S.reqs.find(W.reqs[i]);
         if (it == S.reqs.end()) continue;
@@ -472,6 +537,33 @@ void admit(Server& S) {
     }
 }
 
+// Load every kernel a wave can launch (lazy module loading would otherwise
+// put each kernel's first load, about a millisecond, on the latency of the
+// requests in the wave that first needs it) and give each wave its first
+// staging buffers.
+void prewarm(Server& S) {
+    WalkArgs wa{};
+    ShadowArgs sa{};
+    int occ = 0;
+    for (uint32_t cls : {(uint32_t)CLS_COMPANION, (uint32_t)CLS_RATIONAL, (uint32_t)CLS_DENSE, (uint32_t)CLS_INTERP})
+        for (uint32_t m = 1; m <= (uint32_t)kServeMaxM; ++m)
+            for (uint32_t D = 0; D <= (cls == CLS_INTERP ? 0u : 32u); ++D) {
+                walk_dispatch(cls, m, D, 0, 128, 0, nullptr, wa, &occ);
+                if (cls == CLS_COMPANION || cls == CLS_DENSE) shadow_fd_dispatch(cls, m, D, 0, 128, 0, nullptr, sa, &occ);
+            }
+    for (uint32_t U : {1u, 2u, 4u}) shadow_eval_dispatch(U, 0, 128, 0, nullptr, sa, &occ);
+    for (uint32_t m = 1; m <= (uint32_t)kServeMaxM; ++m)
+        for (uint32_t f = 0; f < 4; ++f) shadow_chain_dispatch(m, f, 0, 32, 0, nullptr, sa, &occ);
+    cudaGetLastError();   // the instances that do not exist answered cudaErrorInvalidValue
+    for (Wave& W : S.waves) {
+        grow_host(W.h_up, W.h_up_cap, 1);
+        grow_host(W.h_res, W.h_res_cap, 1);
+        grow_host(W.h_sh, W.h_sh_cap, 1);
+        grow_host(W.h_st, W.h_st_cap, 1);
+        for (DevBuf* b : {&W.up, &W.zero, &W.chunkP, &W.chunkSig, &W.res, &W.shadow, &W.mf}) grow(*b, 1);
+    }
+}
+
 void loop(Server* Sp) {
     Server& S = *Sp;
     cudaSetDevice(ctx()->device);
@@ -486,30 +578,75 @@ void loop(Server* Sp) {
             S.cv.notify_all();
             if (S.stop) break;
             admit(S);
-            for (Wave& W : S.waves)
+            uint32_t free_idx = 0;
+            for (Wave& W : S.waves) {
                 if (!W.busy) { free_wave = &W; break; }
+                ++free_idx;
+            }
             if (free_wave) {
+                // requests that need more waves ("long": deep walks, long
+                // shadows) never share a wave with ones that finish in this
+                // wave, and hold at most all but one wave slot, so short
+                // requests always find a wave that is not held up by a long
+                // segment
+                const uint64_t seg_walk = (uint64_t)(S.cfg.chunk_steps ? S.cfg.chunk_steps : 4096) * 16;
+                auto is_long = [&](const Req& r) {
+                    return (!r.walk_done && r.d.depth - r.walk_next > seg_walk) ||
+                           (r.shadow_mode != SHADOW_NONE && !r.shadow_done && r.d.depth - r.shadow_next > 8192);
+                };
+                uint32_t long_waves = 0;
+                for (const Wave& W : S.waves) long_waves += W.busy && W.has_long;
+                bool short_pending = false, long_pending = false;
+                for (int64_t id : S.active) {
+                    const Req& r = *S.reqs[id];
+                    if (r.inflight || r.done || r.cancelled) continue;
+                    (is_long(r) ? long_pending : short_pending) = true;
+                }
+                const bool take_long = long_pending && long_waves + 1 < (uint32_t)S.waves.size();
+                const bool want_long = take_long && !short_pending ? true : (take_long && long_waves == 0);
                 uint64_t tiles = 0;
                 for (int64_t id : S.active) {
                     Req& r = *S.reqs[id];
                     if (r.inflight || r.done) continue;
                     if (r.cancelled) continue;
+                    const bool lg = is_long(r);
+                    if (short_pending && !want_long ? lg : !lg) continue;
+                    if (lg && !take_long) continue;
                     const uint64_t nb = (r.d.K + 31) / 32;
-                    const uint64_t span = std::min<uint64_t>(r.d.depth - r.walk_next,
-                                                             (uint64_t)(S.cfg.chunk_steps ? S.cfg.chunk_steps : 4096) * 16);
+                    const uint64_t span = std::min<uint64_t>(r.d.depth - r.walk_next, seg_walk);
                     const uint64_t t = r.walk_done ? 0 : nb * std::max<uint64_t>(1, (span + 4095) / 4096);
                     if (!sel.empty() && tiles + t > max_tiles) break;
                     tiles += t;
                     r.inflight = true;
                     sel.push_back(&r);
                 }
+                free_wave->has_long = !sel.empty() && is_long(*sel.front());
             }
             if (sel.empty()) {
                 S.cv.wait_for(lk, std::chrono::microseconds(200));
                 continue;
             }
+            free_wave->log = SIZE_MAX;
+            if (S.wlog.size() < kMaxWaveLog) {
+                WaveLog g;
+                g.t_sel = ms_since(S, Clock::now());
+                g.n_req = (uint32_t)sel.size();
+                g.has_long = free_wave->has_long;
+                g.wave = free_idx;
+                free_wave->log = S.wlog.size();
+                S.wlog.push_back(g);
+            }
         }
         int rc = launch_wave(S, *free_wave, sel);
+        {
+            std::lock_guard<std::mutex> lk(S.mu);
+            if (free_wave->log < S.wlog.size()) {
+                WaveLog& g = S.wlog[free_wave->log];
+                g.t_launched = ms_since(S, Clock::now());
+                g.walk_tiles = free_wave->n_tiles;
+                g.shadow_span = free_wave->max_span;
+            }
+        }
         if (rc != DR_OK) {
             std::lock_guard<std::mutex> lk(S.mu);
             S.error = rc;
@@ -551,9 +688,12 @@ int dr_serve_open(const dr_serve_config* cfg, int32_t* server_out) {
     S->waves.resize(nw);
     for (Wave& W : S->waves) {
         cudaError_t e = cudaStreamCreateWithFlags(&W.st, cudaStreamNonBlocking);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&W.ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreate(&W.ev0);
+        if (e == cudaSuccess) e = cudaEventCreate(&W.ev);
         if (e != cudaSuccess) return cuda_fail(e, "dr_serve_open");
     }
+    prewarm(*S);
+    S->t_open = Clock::now();
     Server* raw = S.get();
     S->thr = std::thread(loop, raw);
     std::lock_guard<std::mutex> lk(g_srv_mu);
@@ -677,10 +817,29 @@ int dr_serve_close(int32_t server) {
     for (Wave& W : S->waves) {
         if (W.st) cudaStreamSynchronize(W.st);
         if (W.ev) cudaEventDestroy(W.ev);
+        if (W.ev0) cudaEventDestroy(W.ev0);
         if (W.st) cudaStreamDestroy(W.st);
+        if (W.h_up) cudaFreeHost(W.h_up);
         if (W.h_res) cudaFreeHost(W.h_res);
         if (W.h_sh) cudaFreeHost(W.h_sh);
         if (W.h_st) cudaFreeHost(W.h_st);
+    }
+    return DR_OK;
+}
+
+int dr_debug_serve_waves(int32_t server, int32_t max_waves, int32_t* n_waves, double* rows) {
+    Server* S = find_server(server);
+    if (!S) return DR_ERR_HANDLE;
+    if (!n_waves || (max_waves > 0 && !rows)) return DR_ERR_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    *n_waves = (int32_t)S->wlog.size();
+    const size_t n = std::min<size_t>(S->wlog.size(), (size_t)std::max(max_waves, 0));
+    for (size_t i = 0; i < n; ++i) {
+        const WaveLog& g = S->wlog[i];
+        double* o = rows + 9 * i;
+        o[0] = g.t_sel; o[1] = g.t_launched; o[2] = g.t_harvest; o[3] = g.gpu_ms;
+        o[4] = g.n_req; o[5] = g.has_long; o[6] = g.wave; o[7] = (double)g.walk_tiles;
+        o[8] = (double)g.shadow_span;
     }
     return DR_OK;
 }

@@ -144,6 +144,7 @@ _SIGNATURES = {
     "dr_bench_int_peak": (ctypes.c_int, [_I32, _P]),
     "dr_debug_rescale": (ctypes.c_int, [_P, _P, _I32, _P]),
     "dr_debug_batch_timeline": (ctypes.c_int, [_I32, _I32, _P, _P]),
+    "dr_debug_serve_waves": (ctypes.c_int, [_I32, _I32, _P, _P]),
     "dr_debug_build_phases": (ctypes.c_int, [_P, _I32]),
     "dr_debug_sim_walk": (ctypes.c_int, [ctypes.c_char_p, _U64, _I32, _U64, _U64, _P, _I32, _I64,
                                          _U32, _U64, _I32, _P, _P, _P, _P]),

@@ -107,6 +107,17 @@ class WalkServer:
         return {"completed": c.value, "prime_steps": ps.value, "admitted_bytes": ab.value,
                 "queue_depth": qd.value}
 
+    def wave_log(self) -> np.ndarray:
+        """Scheduler record of the wave launches, one row each: selection, launch-issued
+        and harvest times (ms after open), device ms, requests, long-request wave, wave
+        slot, walk tiles, longest shadow segment."""
+        n = ctypes.c_int32()
+        N.check(N.lib().dr_debug_serve_waves(self.handle, 0, ctypes.byref(n), None), "dr_debug_serve_waves")
+        rows = np.zeros((max(n.value, 1), 9))
+        N.check(N.lib().dr_debug_serve_waves(self.handle, n.value, ctypes.byref(n), rows.ctypes.data),
+                "dr_debug_serve_waves")
+        return rows[:n.value]
+
     def close(self) -> None:
         if self.handle:
             N.lib().dr_serve_close(self.handle)

@@ -88,3 +88,28 @@ def test_oversize_and_cancel():
         res = srv.wait([r2])[r2]
     g = run_walks([pcf_request(dr.compile_pcf("2", "n**2"), 2, 2000, 32)])[0]
     _same(res, g)
+
+
+def test_short_requests_overtake_a_long_one():
+    """A long request (many shadow segments) runs in its own waves; a short
+    request submitted behind it completes first, with the same results as a
+    batch, and the scheduler's wave record is consistent."""
+    long = pcf_request(dr.compile_pcf("2*n+1", "-n**2 + 3"), 1, 150_000, 96)
+    short = pcf_request(dr.compile_pcf("2", "n**2"), 2, 2000, 32)
+    with WalkServer(max_inflight=3) as srv:
+        rl = srv.submit(long)
+        rs = srv.submit(short)
+        got_s = srv.wait([rs])[rs]
+        assert srv.poll(rl) is None          # the long request is still in flight
+        got_l = srv.wait([rl], timeout=120)[rl]
+        log = srv.wave_log()
+    ref = run_walks([long, short])
+    _same(got_l, ref[0])
+    _same(got_s, ref[1])
+    assert got_s["latency_s"] < got_l["latency_s"]
+    assert len(log) >= 150_000 // 8192
+    t_sel, t_launched, t_harvest, gpu_ms, n_req, has_long, slot = (log[:, i] for i in range(7))
+    assert np.all(t_sel <= t_launched) and np.all(t_launched <= t_harvest)
+    assert np.all(gpu_ms > 0) and np.all(n_req >= 1)
+    assert set(np.unique(has_long)) <= {0.0, 1.0} and has_long.max() == 1.0
+    assert np.all((slot >= 0) & (slot < 3))
