@@ -171,6 +171,7 @@ struct Batch {
     std::vector<uint32_t> h_walk_K;
     std::vector<uint64_t> h_res_off, h_cp_off;
     cudaGraphExec_t graph = nullptr;
+    uint32_t runs = 0;             // dr_batch_run calls so far (the first launches directly)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr, join = nullptr;
     std::vector<cudaEvent_t> joins;
     std::vector<cudaEvent_t> evals;     // per launch: its step-matrix evaluation is done

@@ -51,7 +51,7 @@ def _rational(v) -> Tuple[int, int]:
     return int(v), 1
 
 
-@dataclass
+@dataclass(slots=True)
 class WalkRequest:
     blob: bytes
     K: int
@@ -131,42 +131,55 @@ def cmf_request(program, depth: int, K: int, shift_vals, trajectory_vals=None,
 
 
 class _Packed:
-    """Flat C-ABI arrays for a list of requests (built with numpy, one pass)."""
+    """Flat C-ABI arrays for a list of requests: one Python pass gathers each
+    request's scalars, numpy does the rest."""
 
     def __init__(self, reqs: Sequence[WalkRequest]):
         n = len(reqs)
         index: Dict[bytes, int] = {}
         blobs: List[bytes] = []
-        prog = []
+        flat: List[int] = []                 # 10 scalars per request
+        axis_vals: List[int] = []
+        vec_vals: List[int] = []
+        put_row, put_axis = flat.extend, axis_vals.extend
+        f_init, f_shadow, f_vec = N.DR_WALK_INIT_PCF, N.DR_WALK_SHADOW, N.DR_WALK_VEC
         for r in reqs:
-            j = index.get(r.blob)
+            b = r.blob
+            j = index.get(b)
             if j is None:
-                j = index[r.blob] = len(blobs)
-                blobs.append(r.blob)
-            prog.append(j)
+                j = index[b] = len(blobs)
+                blobs.append(b)
+            ax = r.axis
+            for t in ax:
+                put_axis(t)
+            v = r.vec
+            if r.depth < 0:          # the reference treats a negative depth as no steps
+                r.depth = 0
+            put_row((j, r.K, r.depth, r.checkpoint, r.a0,
+                     (f_init if r.pcf_init else 0) | (f_shadow if r.shadow else 0) | (f_vec if v is not None else 0),
+                     r.q_row, r.p_row, 4 * len(ax), 0 if v is None else len(v)))
+            if v is not None:
+                vec_vals.extend(v)
         self.n_programs = len(blobs)
         offs = np.zeros(len(blobs) + 1, dtype=np.uint64)
-        np.cumsum([len(b) for b in blobs], out=offs[1:])
+        np.cumsum(np.fromiter(map(len, blobs), dtype=np.uint64, count=len(blobs)), out=offs[1:])
         self.offsets = offs
-        self.blobs = np.frombuffer(b"".join(blobs) or b"\0", dtype=np.uint8).copy()
-        Ks = np.array([r.K for r in reqs], dtype=np.int64).reshape(n)
+        self.blobs = np.frombuffer(b"".join(blobs) or b"\0", dtype=np.uint8)   # read-only: passed as const
+        try:
+            cols = np.fromiter(flat, dtype=np.int64, count=len(flat)).reshape(n, 10)
+        except OverflowError:
+            if any(not -2**63 <= int(r.a0) < 2**63 for r in reqs):
+                raise OverflowError("a0 outside int64") from None
+            raise
+        prog, Ks, depth, cps, a0, flags, q_row, p_row, alen, vlen = cols.T
         if n and (Ks.min() < 1 or Ks.max() > N.DR_MAX_K):
             raise ValueError(f"K must be in 1..{N.DR_MAX_K}")
-        for r in reqs:            # the reference treats a negative depth as no steps
-            if r.depth < 0:
-                r.depth = 0
-        cps = np.array([r.checkpoint for r in reqs], dtype=np.uint64).reshape(n)
+        if n and cps.min() < 0:
+            raise OverflowError("negative checkpoint")
         try:
-            a0 = np.array([r.a0 for r in reqs], dtype=np.int64).reshape(n)
-        except OverflowError:
-            raise OverflowError("a0 outside int64") from None
-        try:
-            axis = np.array([v for r in reqs for t in r.axis for v in t] +
-                            [v for r in reqs if r.vec is not None for v in r.vec], dtype=np.int64)
+            axis = np.array(axis_vals + vec_vals, dtype=np.int64)
         except OverflowError:
             raise OverflowError("axis parameter outside int64") from None
-        alen = np.array([4 * len(r.axis) for r in reqs], dtype=np.uint64).reshape(n)
-        vlen = np.array([len(r.vec) if r.vec is not None else 0 for r in reqs], dtype=np.uint64).reshape(n)
         sizes = Ks + np.where(cps > 0, Ks, 0)
         res_off = np.zeros(n, dtype=np.int64)
         if n:
@@ -174,20 +187,18 @@ class _Packed:
         desc = np.zeros(n, dtype=N.WALK_DTYPE)
         desc["program"] = prog
         desc["K"] = Ks
-        desc["depth"] = [r.depth for r in reqs]
+        desc["depth"] = depth
         desc["checkpoint"] = cps
         desc["a0"] = a0
-        desc["flags"] = [(N.DR_WALK_INIT_PCF if r.pcf_init else 0) | (N.DR_WALK_SHADOW if r.shadow else 0)
-                         | (N.DR_WALK_VEC if r.vec is not None else 0) for r in reqs]
-        desc["q_row"] = [r.q_row for r in reqs]
-        desc["p_row"] = [r.p_row for r in reqs]
-        voff = np.zeros(n, dtype=np.uint64)
+        desc["flags"] = flags
+        desc["q_row"] = q_row
+        desc["p_row"] = p_row
+        a_total = int(alen.sum()) if n else 0
+        voff = np.zeros(n, dtype=np.int64)
         if n:
-            voff[:] = int(alen.sum())
             np.cumsum(vlen[:-1], out=voff[1:])
-            voff[1:] += int(alen.sum())
-        desc["vec_offset"] = np.where(vlen > 0, voff, 0)
-        aoff = np.zeros(n, dtype=np.uint64)
+        desc["vec_offset"] = np.where(vlen > 0, voff + a_total, 0)
+        aoff = np.zeros(n, dtype=np.int64)
         if n:
             np.cumsum(alen[:-1], out=aoff[1:])
         desc["axis_offset"] = aoff

@@ -142,8 +142,9 @@ int dr_walk_batch(const dr_walk_desc *walks, int32_t n_walks,
 
 /* ---- prepared batches (inputs resident on the device) -------------------
  * dr_batch_create uploads programs and descriptors once; dr_batch_run runs
- * walk -> CRT -> delta -> top-k entirely on the device (captured in a CUDA
- * graph after the first run); dr_batch_read copies results to the host.     */
+ * walk -> CRT -> delta -> top-k entirely on the device (the first run
+ * launches directly, the second captures a CUDA graph that later runs
+ * replay); dr_batch_read copies results to the host.                        */
 int dr_batch_create(const dr_walk_desc *walks, int32_t n_walks,
                     const uint8_t *blobs, const uint64_t *blob_offsets, int32_t n_programs,
                     const int64_t *axis_params, uint64_t n_axis_params,
@@ -194,7 +195,9 @@ int dr_batch_destroy(int32_t batch);
 /* Autotuner: builds the given walks with candidate depth-chunk lengths and
  * warps per block around the built-in policy, times each as a graph replay
  * (best of three, CUDA events), and returns the fastest in *best (its engine
- * and shadow_buffer_mb fields are inputs).  The choice is remembered for the
+ * and shadow_buffer_mb fields are inputs); a candidate replaces the built-in
+ * policy only when it is at least 2% faster, since shorter chunks cost host
+ * build time on every batch.  The choice is remembered for the
  * workload's shape (per launch class: log2 of the (walk, prime block) count
  * and of their steps, longest walk), so later batches of that shape built
  * with a zero chunk_steps and warps_per_block use it.  No reference
