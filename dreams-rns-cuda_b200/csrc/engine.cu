@@ -67,7 +67,20 @@ int get_plan(const uint8_t* blob, uint64_t size, std::shared_ptr<Plan>* out, std
     if (rc != DR_OK) return rc;
     plan->fcomp = float_companion_shape(*plan);
     plan->blob.assign(key.data(), key.size());
+    std::string code_key(sizeof(uint32_t) + sizeof(Insn) * (plan->ops.size() + plan->dops.size()), '\0');
+    {
+        const uint32_t n_ops = (uint32_t)plan->ops.size();
+        char* q = &code_key[0];
+        std::memcpy(q, &n_ops, sizeof n_ops);
+        if (n_ops) std::memcpy(q + sizeof n_ops, plan->ops.data(), sizeof(Insn) * n_ops);
+        if (!plan->dops.empty())
+            std::memcpy(q + sizeof n_ops + sizeof(Insn) * n_ops, plan->dops.data(), sizeof(Insn) * plan->dops.size());
+    }
     std::lock_guard<std::mutex> lk(g_ctx->mu);
+    if (g_ctx->code_ids.size() > 100000) g_ctx->code_ids.clear();
+    auto ci = g_ctx->code_ids.find(code_key);
+    if (ci == g_ctx->code_ids.end()) ci = g_ctx->code_ids.emplace(std::move(code_key), g_ctx->next_code_id++).first;
+    plan->code_id = ci->second;
     if (g_ctx->plan_cache.size() > 200000) g_ctx->plan_cache.clear();
     g_ctx->plan_cache.emplace(std::string_view(plan->blob), plan);
     *out = plan;
@@ -270,8 +283,11 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     std::vector<DevProgram> dprogs(n_programs);
     std::vector<uint4> code;
     std::vector<int64_t> consts;
-    code.reserve((size_t)n_programs * 24);
+    code.reserve(1024);
     consts.reserve((size_t)n_programs * 8);
+    std::unordered_map<uint32_t, std::pair<uint32_t, uint32_t>> code_at;   // code_id -> (op_off, dop_off)
+    uint32_t last_code_id = 0;
+    std::pair<uint32_t, uint32_t> last_code_at{0, 0};
     for (int32_t i = 0; i < n_programs; ++i) {
         if (blob_offsets[i + 1] < blob_offsets[i]) {
             set_error("blob_offsets not increasing");
@@ -289,13 +305,25 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         d.dim = P.dim;
         d.cls = (engine == DR_ENGINE_AUTO) ? (uint32_t)P.cls : (uint32_t)CLS_INTERP;
         d.degree = P.degree;
-        d.op_off = (uint32_t)code.size();
+        // programs with the same instruction streams share one copy
+        if (P.code_id != last_code_id) {
+            auto at = code_at.find(P.code_id);
+            if (at == code_at.end()) {
+                std::pair<uint32_t, uint32_t> off;
+                off.first = (uint32_t)code.size();
+                for (const Insn& in : P.ops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
+                off.second = (uint32_t)code.size();
+                for (const Insn& in : P.dops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
+                at = code_at.emplace(P.code_id, off).first;
+            }
+            last_code_id = P.code_id;
+            last_code_at = at->second;
+        }
+        d.op_off = last_code_at.first;
         d.n_ops = (uint32_t)P.ops.size();
-        for (const Insn& in : P.ops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
         d.n_regs = P.n_regs;
-        d.dop_off = (uint32_t)code.size();
+        d.dop_off = last_code_at.second;
         d.dn_ops = (uint32_t)P.dops.size();
-        for (const Insn& in : P.dops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
         d.dn_regs = P.dn_regs;
         d.c_off = (uint32_t)consts.size();
         d.n_consts = (uint32_t)P.consts.size();

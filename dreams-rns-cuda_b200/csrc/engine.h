@@ -74,6 +74,10 @@ struct Context {
     std::mutex mu;
     // plan cache keyed by program bytes (views into each Plan's own copy)
     std::unordered_map<std::string_view, std::shared_ptr<Plan>> plan_cache;
+    // interned instruction streams: programs that differ only in their
+    // constants share one copy of device code in a batch
+    std::unordered_map<std::string, uint32_t> code_ids;
+    uint32_t next_code_id = 1;   // never reused, so a cleared table cannot alias
     std::map<int, std::shared_ptr<CrtSet>> crt_std;  // CRT tables of the standard primes
     std::map<std::string, std::pair<uint32_t, uint32_t>> tuned;   // signature -> (chunk, warps/block)
     std::mutex cache_mu;

@@ -533,7 +533,11 @@ int plan_program(const RawProgram& raw, Plan* P, std::string* err) {
 
 double float_bound_log2(const Plan& plan, const int64_t* axis, uint64_t depth) {
     if (plan.has_inv) return INFINITY;
-    std::vector<double> b(DR_MAX_REGS, 0.0);
+    // registers start at 0.0; clear only those the prefix can name
+    uint32_t hi = 0;
+    for (const Insn& in : plan.exec) hi = std::max(hi, std::max(in.a, std::max(in.b, in.c)));
+    double b[DR_MAX_REGS];
+    std::fill(b, b + std::min<uint32_t>(hi + 1, DR_MAX_REGS), 0.0);
     const double last = depth > 0 ? (double)(depth - 1) : 0.0;
     double worst = 0.0;
     for (const Insn& in : plan.exec) {

@@ -37,6 +37,7 @@ struct Plan {
     std::vector<Insn> exec;         // executed prefix, uncompacted (bounds analysis)
     std::vector<int32_t> dirs;
     bool fcomp = false;             // float_companion_shape(*this), set once planned
+    uint32_t code_id = 0;           // equal ids: identical ops and dops (shared device code)
     std::string blob;               // the program bytes (plan cache key storage)
 };
 
