@@ -641,6 +641,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         if (L.kind == 2) {
             const size_t per_warp = (size_t)L.rows_per_warp * 32 * 8;
             const bool coloc = chain_colocate(shadow_list.data() + L.off, L.count, L.m, walk_ns);
+            L.lean = coloc;
             L.block = coloc ? 32 : 32 * kChainWarps;
             L.smem = coloc ? per_warp : std::max(per_warp * kChainWarps, chain_hog_smem());
             if (per_warp * (L.block / 32) > L.smem || L.smem > 227 * 1024) {
@@ -802,7 +803,7 @@ bool chain_colocate(const DevShadowSeg* segs, uint32_t count, uint32_t m, double
     return walk_ns > 0 && 3.0 * (double)longest * chain_step_ns(m) < walk_ns;
 }
 
-int chain_blocks(const DevShadowSeg* segs, uint32_t count, uint32_t m, double walk_ns) {
+int chain_blocks(const DevShadowSeg* segs, uint32_t count, uint32_t m, double walk_ns, int wpb) {
     // segments are sorted longest first; a warp takes 32 of them, so item k
     // lasts as long as segment 32k.  Enough warps that the total chain work
     // spread over them ends with the longest chain, or with the walk kernels
@@ -817,8 +818,8 @@ int chain_blocks(const DevShadowSeg* segs, uint32_t count, uint32_t m, double wa
     const uint32_t items = (count + 31) / 32;
     const double span = std::max((double)longest * kStepNs, walk_ns);
     const uint64_t warps = span > 0 ? (uint64_t)std::ceil((double)total * kStepNs / span) : 1;
-    const uint64_t blocks = (warps + kChainWarps - 1) / kChainWarps + 1;
-    return (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (items + kChainWarps - 1) / kChainWarps));
+    const uint64_t blocks = (warps + wpb - 1) / wpb + 1;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(blocks, (items + wpb - 1) / wpb));
 }
 
 int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs,
@@ -849,8 +850,13 @@ int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevSh
     }
     L.grid = std::max(1, std::min((int)((L.items + wpb - 1) / wpb), occ * sms));
     const bool coloc = whole_sm && chain_colocate(segs, L.count, L.m, walk_ns);
-    L.block2 = coloc ? 32 : 32 * kChainWarps;
-    L.smem2 = shadow_chain_smem(L.m, (L.cls & 1u) != 0) * (L.block2 / 32);
+    L.lean = coloc;
+    // chain warps per block: fewer when their staging buffers would not fit
+    const size_t chain_warp_smem = shadow_chain_smem(L.m, (L.cls & 1u) != 0);
+    int cw = kChainWarps;
+    while (cw > 1 && chain_warp_smem * cw > 227 * 1024) cw /= 2;
+    L.block2 = coloc ? 32 : 32 * cw;
+    L.smem2 = chain_warp_smem * (L.block2 / 32);
     if (whole_sm && !coloc) L.smem2 = std::max(L.smem2, chain_hog_smem());
     e = shadow_chain_dispatch(L.m, L.cls, 0, L.block2, L.smem2, nullptr, sa, &occ);
     if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
@@ -859,7 +865,7 @@ int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevSh
         return DR_ERR_UNSUPPORTED;
     }
     L.grid2 = coloc ? std::min((int)L.items2, occ * sms)
-                    : std::min(chain_blocks(segs, L.count, L.m, walk_ns), occ * sms);
+                    : std::min(chain_blocks(segs, L.count, L.m, walk_ns, cw), occ * sms);
     return DR_OK;
 }
 
@@ -1039,6 +1045,7 @@ static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, Shado
     sa.n_list = L.count;
     sa.rows_regs = L.rows_regs;
     sa.rows_per_warp = L.rows_per_warp;
+    sa.lean = L.lean ? 1u : 0u;
     if (L.kind == 2) {
         sa.n_items = L.items;
         sa.queue = B.queues.as<uint32_t>() + L.queue;

@@ -110,6 +110,9 @@ struct LaunchSpec {
     size_t smem2 = 0;
     int grid2 = 0, block2 = 0;
     bool follow = false;       // runs on the stream of the previous launch (shadow rounds)
+    bool lean = false;         // shadow chains co-located with the walks: exact steps, which
+                               // skip the rescale work on the steps without one (fewest
+                               // instructions, as they share issue slots with the walks)
 };
 
 // Interpreted-shadow launch geometry shared by batches and serving waves:
@@ -128,7 +131,9 @@ constexpr int kChainWarps = 4;
 // walk_ns: expected duration of the walk kernels running beside the chains
 // (0: unknown); the chains get enough SMs to finish within the longer of it
 // and their own longest chain, and no more.
-int chain_blocks(const DevShadowSeg* segs, uint32_t count, uint32_t m, double walk_ns = 0.0);
+// wpb: warps per chain block.
+int chain_blocks(const DevShadowSeg* segs, uint32_t count, uint32_t m, double walk_ns = 0.0,
+                 int wpb = kChainWarps);
 // Whether chains this short next to the walks run best spread over all SMs
 // beside the walk warps (one warp per block, no whole-SM claim): their
 // longest chain, even slowed by sharing issue slots, ends well before the walks.

@@ -82,27 +82,41 @@ cudaError_t walk_dispatch_interp(uint32_t m, int grid, int block, size_t smem, c
                                  const WalkArgs& a, int* occ);
 
 // Launches carry their stream's priority as a launch attribute, so the
-// priority also holds for the kernel nodes of a captured CUDA graph.
+// priority also holds for the kernel nodes of a captured CUDA graph.  With
+// early_start the launch is a programmatic dependent of the previous kernel
+// in the stream: its blocks may become resident while that kernel still
+// runs (once it has executed griddepcontrol.launch_dependents) and must
+// execute griddepcontrol.wait before reading what it wrote.
 template <typename KernelT, typename ArgT>
 inline cudaError_t run_kernel(KernelT k, int grid, int block, size_t smem, cudaStream_t st,
-                              const ArgT& a, int* occ) {
+                              const ArgT& a, int* occ, bool early_start = false) {
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, block, smem);
     int prio = 0;
-    if (st && cudaStreamGetPriority(st, &prio) == cudaSuccess && prio != 0) {
+    const bool has_prio = st && cudaStreamGetPriority(st, &prio) == cudaSuccess && prio != 0;
+    if (has_prio || early_start) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)grid);
         cfg.blockDim = dim3((unsigned)block);
         cfg.dynamicSmemBytes = smem;
         cfg.stream = st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributePriority;
-        attr[0].val.priority = prio;
+        cudaLaunchAttribute attr[2];
+        unsigned n = 0;
+        if (has_prio) {
+            attr[n].id = cudaLaunchAttributePriority;
+            attr[n].val.priority = prio;
+            ++n;
+        }
+        if (early_start) {
+            attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attr[n].val.programmaticStreamSerializationAllowed = 1;
+            ++n;
+        }
         cfg.attrs = attr;
-        cfg.numAttrs = 1;
+        cfg.numAttrs = n;
         return cudaLaunchKernelEx(&cfg, k, a);
     }
     k<<<grid, block, smem, st>>>(a);

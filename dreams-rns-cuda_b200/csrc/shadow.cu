@@ -17,12 +17,17 @@ cudaError_t shadow_eval_dispatch(uint32_t U, int grid, int block, size_t smem, c
 
 cudaError_t shadow_chain_dispatch(uint32_t m, uint32_t flags, int grid, int block, size_t smem,
                                   cudaStream_t st, const ShadowArgs& a, int* occ) {
-    switch (m * 4 + (flags & 3u)) {
+    // flags bit 2: the lean instantiation (exact steps) for co-located chains
+    switch (m * 8 + (flags & 3u) + (a.lean ? 4u : 0u)) {
 #define DR_X(M_, D_) \
-    case M_ * 4: return run_kernel(k_shadow_chain<M_, 0>, grid, block, smem, st, a, occ); \
-    case M_ * 4 + 1: return run_kernel(k_shadow_chain<M_, 1>, grid, block, smem, st, a, occ); \
-    case M_ * 4 + 2: return run_kernel(k_shadow_chain<M_, 2>, grid, block, smem, st, a, occ); \
-    case M_ * 4 + 3: return run_kernel(k_shadow_chain<M_, 3>, grid, block, smem, st, a, occ);
+    case M_ * 8: return run_kernel(k_shadow_chain<M_, 0>, grid, block, smem, st, a, occ, true); \
+    case M_ * 8 + 1: return run_kernel(k_shadow_chain<M_, 1>, grid, block, smem, st, a, occ, true); \
+    case M_ * 8 + 2: return run_kernel(k_shadow_chain<M_, 2>, grid, block, smem, st, a, occ, true); \
+    case M_ * 8 + 3: return run_kernel(k_shadow_chain<M_, 3>, grid, block, smem, st, a, occ, true); \
+    case M_ * 8 + 4: return run_kernel(k_shadow_chain<M_, 4>, grid, block, smem, st, a, occ, true); \
+    case M_ * 8 + 5: return run_kernel(k_shadow_chain<M_, 5>, grid, block, smem, st, a, occ, true); \
+    case M_ * 8 + 6: return run_kernel(k_shadow_chain<M_, 6>, grid, block, smem, st, a, occ, true); \
+    case M_ * 8 + 7: return run_kernel(k_shadow_chain<M_, 7>, grid, block, smem, st, a, occ, true);
         DR_INTERP_INSTANCES(DR_X)
 #undef DR_X
         default: return cudaErrorInvalidValue;
@@ -31,7 +36,7 @@ cudaError_t shadow_chain_dispatch(uint32_t m, uint32_t flags, int grid, int bloc
 
 size_t shadow_chain_smem(uint32_t m, bool comp) {
     const int ne = (int)shadow_entries(m, comp);
-    return 2ull * chain_chunk_steps(ne) * ne * 32 * sizeof(double);
+    return (size_t)chain_buffers(ne) * chain_chunk_steps(ne) * ne * 32 * sizeof(double);
 }
 
 cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block,
@@ -39,7 +44,9 @@ cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, i
     if (cls == CLS_COMPANION) {
         switch (m * 100 + D) {
 #define DR_X(M_, D_) \
-    case M_ * 100 + D_: return run_kernel(k_shadow_intfd<CLS_COMPANION, M_, D_>, grid, block, smem, st, a, occ);
+    case M_ * 100 + D_: \
+        return a.lean ? run_kernel(k_shadow_intfd<CLS_COMPANION, M_, D_, true>, grid, block, smem, st, a, occ) \
+                      : run_kernel(k_shadow_intfd<CLS_COMPANION, M_, D_, false>, grid, block, smem, st, a, occ);
             DR_COMPANION_INSTANCES(DR_X)
 #undef DR_X
             default: return cudaErrorInvalidValue;
@@ -48,7 +55,9 @@ cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, i
     if (cls == CLS_DENSE) {
         switch (m * 100 + D) {
 #define DR_X(M_, D_) \
-    case M_ * 100 + D_: return run_kernel(k_shadow_intfd<CLS_DENSE, M_, D_>, grid, block, smem, st, a, occ);
+    case M_ * 100 + D_: \
+        return a.lean ? run_kernel(k_shadow_intfd<CLS_DENSE, M_, D_, true>, grid, block, smem, st, a, occ) \
+                      : run_kernel(k_shadow_intfd<CLS_DENSE, M_, D_, false>, grid, block, smem, st, a, occ);
             DR_DENSE_INSTANCES(DR_X)
 #undef DR_X
             default: return cudaErrorInvalidValue;

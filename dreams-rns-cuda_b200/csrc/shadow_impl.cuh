@@ -25,7 +25,19 @@
 // Per step the chain's critical path is the product, the max-abs test and,
 // when it fires, one correctly rounded reciprocal plus a three-operation
 // correction per entry; the max / NaN / threshold tests run on the integer
-// pipe so the FP64 pipe only carries the arithmetic.
+// pipe (magnitude keys) so the FP64 pipe only carries the arithmetic.
+//
+// Fast chunks.  The chains run in chunks of steps (the staged chunk of the
+// interpreted mode, 8 steps of the integer mode) on a fast path with no
+// division branch: every lane computes the Markstein quotients and keeps
+// them where it rescales, and records whether it left the Markstein domain.
+// A chunk where any lane of the warp did is run again from its saved start
+// with the exact steps (IEEE division outside the domain) in a function that
+// is not inlined, so that code stays out of the fast loop; both paths give
+// bit-identical results inside the domain.  Chains that share their SMs
+// with the walk kernels (co-located) run the exact steps throughout: they
+// skip the rescale work on steps without one, and issue slots there belong
+// to the walks.
 #pragma once
 #include <stdint.h>
 
@@ -57,6 +69,7 @@ struct ShadowArgs {
     double* state;              // resident chain state [slot][kShadowStateStride]
     uint32_t rows_regs;         // per-warp smem: doubles, 32 per row
     uint32_t rows_per_warp;
+    uint32_t lean;              // chains co-located with walks: exact steps only
 };
 
 constexpr int kShadowStateStride = 72;   // m*m <= 64 entries, then mantissa, exponent, nan flag
@@ -74,39 +87,58 @@ static __device__ __noinline__ double div_slow(double x, double b) { return __dd
 // Biased exponent field of x (0 for zeros and subnormals).
 __device__ __forceinline__ int bexp(double x) { return (__double2hiint(x) >> 20) & 0x7ff; }
 
-// P /= mx entrywise, each quotient rounded to nearest.  The Markstein path
-// (y = RN(1/mx); q0 = RN(x*y); r = x - mx*q0 by FMA; q = RN(q0 + r*y);
-// P. Markstein, IBM J. Res. Dev. 34(1), 1990) is exact when y, q and the
-// residual r are normal numbers: y is normal for mx < 2^1022 (biased exponent
-// em < 2045); r ~ 2^-52 |x| is normal for a biased exponent ex >= 60 of x;
-// q is normal when ex >= em - 1000 (|x/mx| > 2^(ex - em - 1)).  Entries outside
-// these ranges (and an infinite mx) take the IEEE division.  The test reads
-// only exponent bits of the inputs, so it completes on the integer pipe
-// while the reciprocal is in flight.  q takes the sign of x, which keeps the
-// sign of a zero.
+// Magnitude key: |x| as an integer with the order of |x| (the sign bit
+// cleared).  For non-NaN x the key order is the order of |x|; NaN keys exceed
+// kInfKey, so the max key of a set of entries also tells whether any is NaN.
+__device__ __forceinline__ unsigned long long mag_key(double x) {
+    return (unsigned long long)__double_as_longlong(x) & 0x7fffffffffffffffull;
+}
+constexpr unsigned long long kInfKey = 0x7ff0000000000000ull;
+constexpr unsigned long long kRescaleKey = 0x4202a05f20000000ull;   // key of 1e10
+
+// Markstein quotient q = RN(x / mx) from y = RN(1/mx) (P. Markstein, IBM J.
+// Res. Dev. 34(1), 1990): q0 = RN(x*y); the residual x - q0*mx is exact by
+// FMA; q = RN(q0 + residual*y).  Written with the residual negated,
+// rn = q0*mx - x and q = RN(q0 - rn*y), which equals the above for every x
+// and also gives a zero x its own sign (q0 = +-0, rn = +0, -rn*y + q0 keeps
+// q0's sign) -- numpy's 0/mx.
+__device__ __forceinline__ double markstein_q(double x, double y, double mx) {
+    const double q0 = __dmul_rn(x, y);
+    const double rn = __fma_rn(q0, mx, -x);
+    return __fma_rn(-rn, y, q0);
+}
+
+// Whether every quotient x/mx of the entries is exact by markstein_q: y, the
+// residual and q are normal numbers when mx < 2^1022 (biased exponent
+// em < 2045), the biased exponent ex of x is >= 60 (residual ~ 2^-52 |x|)
+// and ex >= em - 1000 (|x/mx| > 2^(ex - em - 1)); zero entries are exact.
+// Only exponent bits are read, on the integer pipe.
 template <int N_>
-__device__ __forceinline__ void rescale_n(double (&P)[N_], double mx) {
-    const double y = __drcp_rn(mx);
+__device__ __forceinline__ bool markstein_domain(const double (&P)[N_], double mx) {
     const int em = bexp(mx);
     const int t_hi = max(60, em - 1000) << 20;
-    bool slow = em >= 2045;
+    bool out = em >= 2045;
 #pragma unroll
     for (int i = 0; i < N_; ++i) {
         const int ahi = __double2hiint(P[i]) & 0x7fffffff;
-        slow |= (ahi < t_hi) & ((ahi | __double2loint(P[i])) != 0);
+        out |= (ahi < t_hi) & ((ahi | __double2loint(P[i])) != 0);
     }
-    if (__builtin_expect(slow, 0)) {
+    return !out;
+}
+
+// Exact rescale: P /= mx entrywise, each quotient rounded to nearest; the
+// Markstein quotient inside its domain, the IEEE division outside it (and for
+// an infinite mx).
+template <int N_>
+__device__ __forceinline__ void rescale_n(double (&P)[N_], double mx) {
+    const double y = __drcp_rn(mx);
+    if (__builtin_expect(!markstein_domain<N_>(P, mx), 0)) {
 #pragma unroll
         for (int i = 0; i < N_; ++i) P[i] = div_slow(P[i], mx);
         return;
     }
 #pragma unroll
-    for (int i = 0; i < N_; ++i) {
-        const double x = P[i];
-        const double q0 = __dmul_rn(x, y);
-        const double r = __fma_rn(-q0, mx, x);
-        P[i] = copysign(__fma_rn(r, y, q0), x);
-    }
+    for (int i = 0; i < N_; ++i) P[i] = markstein_q(P[i], y, mx);
 }
 
 template <int M_>
@@ -122,6 +154,41 @@ __device__ __forceinline__ void scale_acc(double& sc_m, int& sc_e, double mx) {
     const bool inf = (hi & 0x7ff00000) == 0x7ff00000;
     sc_e += inf ? 0 : ((hi >> 20) & 0x7ff) - 1022;
     sc_m = inf ? p : __hiloint2double((hi & 0x800fffff) | 0x3fe00000, __double2loint(p));
+}
+
+// sc_m * 2^sc_e as the same value with sc_m in [0.5, 1) (exact: only the
+// exponent moves; an infinite sc_m stays as it is).
+__device__ __forceinline__ void scale_norm(double& sc_m, int& sc_e) {
+    const int hi = __double2hiint(sc_m);
+    const int e = (hi >> 20) & 0x7ff;
+    if (e == 0x7ff) return;
+    sc_e += e - 1022;
+    sc_m = __hiloint2double((hi & 0x800fffff) | 0x3fe00000, __double2loint(sc_m));
+}
+
+// Fast rescale of the chunked chains.  Every lane computes the Markstein
+// quotients and keeps them where it rescales (rs), with no branch; the scale
+// takes the significand of mx in [1, 2) and its exponent separately
+// (sc_m * significand rounds to the same significand as sc_m * mx, since the
+// two differ by a power of two; scale_norm after at most a chunk of steps
+// keeps sc_m finite).  Returns whether this lane rescaled outside the
+// Markstein domain: the caller then redoes the chunk with the exact steps.
+template <int N_>
+__device__ __forceinline__ bool rescale_fast(double (&P)[N_], bool rs, double mx, double& sc_m, int& sc_e) {
+    // lanes that do not rescale (their quotients are discarded) take the
+    // reciprocal of 2: a tiny, zero or subnormal max would send the
+    // reciprocal down its slow special-case path on every step
+    const double y = __drcp_rn(rs ? mx : 2.0);
+    const bool out = rs & !markstein_domain<N_>(P, mx);
+#pragma unroll
+    for (int i = 0; i < N_; ++i) {
+        const double q = markstein_q(P[i], y, mx);
+        P[i] = rs ? q : P[i];
+    }
+    const int hi = __double2hiint(mx);
+    sc_e += rs ? ((hi >> 20) & 0x7ff) - 1023 : 0;
+    sc_m = rs ? __dmul_rn(sc_m, __hiloint2double((hi & 0x000fffff) | 0x3ff00000, __double2loint(mx))) : sc_m;
+    return out;
 }
 
 template <int M_>
@@ -141,14 +208,11 @@ struct FChain {
         sc_e = 0;
         nan_seen = false;
     }
-    // P <- P @ X with numpy's rounding, then the max-abs rescale.  A NaN
-    // anywhere in P makes its whole row NaN in the product (NaN * x is NaN
-    // for every x), so the new entries alone decide the reference's
-    // "max(|P|) is NaN" case.
-    __device__ __forceinline__ void step(const double (&X)[M_][M_]) {
+    // P <- P @ X with numpy's rounding; returns the max magnitude key of the
+    // new entries (above kInfKey when one is NaN, numpy's NaN max).
+    __device__ __forceinline__ unsigned long long product(const double (&X)[M_][M_]) {
         double C[M_][M_];
-        double mx = 0.0;
-        bool has_nan = false;
+        unsigned long long mb = 0;
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
@@ -157,29 +221,23 @@ struct FChain {
 #pragma unroll
                 for (int k = 1; k < M_; ++k) c = __fma_rn(P[i][k], X[k][j], c);
                 C[i][j] = c;
-                has_nan |= c != c;
-                mx = fmax(mx, fabs(c));
+                mb = max(mb, mag_key(c));
             }
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
             for (int j = 0; j < M_; ++j) P[i][j] = C[i][j];
-        if (!has_nan && mx > 1e10) {
-            rescale<M_>(P, mx);
-            scale_acc(sc_m, sc_e, mx);
-        }
-        nan_seen |= has_nan;
+        return mb;
     }
-    // companion step: P @ X with X's first m-1 columns the shifted identity
-    // and its last column c.  The shifted entries use the dense product's
-    // own operations with the exact 0 and 1 (so signed zeros, infinities and
-    // NaNs come out as numpy's); they depend only on the old P and stay off
-    // the dependency chain.  A NaN in row i of P always reaches the new
-    // last[i], so the new column decides the NaN case.
-    __device__ __forceinline__ void step_companion(const double (&c)[M_]) {
+    // companion product: X's first m-1 columns are the shifted identity and
+    // its last column is c.  The shifted entries use the dense product's own
+    // operations with the exact 0 and 1 (so signed zeros, infinities and NaNs
+    // come out as numpy's, inf * 0 included); they depend only on the old P
+    // and stay off the dependency chain.
+    __device__ __forceinline__ unsigned long long product_companion(const double (&c)[M_]) {
         double last[M_];
         double sh[M_][M_ > 1 ? M_ - 1 : 1];
-        double mxs = 0.0;
+        unsigned long long mb = 0;
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
@@ -188,7 +246,7 @@ struct FChain {
 #pragma unroll
                 for (int k = 1; k < M_; ++k) v = __fma_rn(P[i][k], k == j + 1 ? 1.0 : 0.0, v);
                 sh[i][j] = v;
-                mxs = fmax(mxs, fabs(v));
+                mb = max(mb, mag_key(v));
             }
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
@@ -196,23 +254,42 @@ struct FChain {
 #pragma unroll
             for (int k = 1; k < M_; ++k) v = __fma_rn(P[i][k], c[k], v);
             last[i] = v;
+            mb = max(mb, mag_key(v));
         }
-        bool has_nan = false;
-        double mx = mxs;
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
 #pragma unroll
             for (int j = 0; j + 1 < M_; ++j) P[i][j] = sh[i][j];
             P[i][M_ - 1] = last[i];
-            has_nan |= last[i] != last[i];
-            mx = fmax(mx, fabs(last[i]));
         }
-        if (!has_nan && mx > 1e10) {
+        return mb;
+    }
+    // the max-abs rescale after a product, exactly (IEEE division outside the
+    // Markstein domain); sc_m stays in [0.5, 1)
+    __device__ __forceinline__ void finish(unsigned long long mb) {
+        const bool nan = mb > kInfKey;
+        if (!nan && mb > kRescaleKey) {
+            const double mx = __longlong_as_double((long long)mb);
             rescale<M_>(P, mx);
             scale_acc(sc_m, sc_e, mx);
         }
-        nan_seen |= has_nan;
+        nan_seen |= nan;
     }
+    // the same on the fast path (rescale_fast); out |= this lane left the
+    // Markstein domain
+    __device__ __forceinline__ void finish_fast(unsigned long long mb, bool& out) {
+        const bool nan = mb > kInfKey;
+        out |= rescale_fast<M_ * M_>(reinterpret_cast<double (&)[M_ * M_]>(P), !nan && mb > kRescaleKey,
+                                     __longlong_as_double((long long)mb), sc_m, sc_e);
+        nan_seen |= nan;
+    }
+    __device__ __forceinline__ void step(const double (&X)[M_][M_]) { finish(product(X)); }
+    __device__ __forceinline__ void step_companion(const double (&c)[M_]) { finish(product_companion(c)); }
+    __device__ __forceinline__ void step_fast(const double (&X)[M_][M_], bool& out) { finish_fast(product(X), out); }
+    __device__ __forceinline__ void step_companion_fast(const double (&c)[M_], bool& out) {
+        finish_fast(product_companion(c), out);
+    }
+    __device__ __forceinline__ void renorm() { scale_norm(sc_m, sc_e); }
     __device__ __forceinline__ void load(const double* st) {
 #pragma unroll
         for (int i = 0; i < M_; ++i)
@@ -227,8 +304,11 @@ struct FChain {
         for (int i = 0; i < M_; ++i)
 #pragma unroll
             for (int j = 0; j < M_; ++j) st[i * M_ + j] = P[i][j];
-        st[64] = sc_m;
-        st[65] = (double)sc_e;
+        double m = sc_m;
+        int e = sc_e;
+        scale_norm(m, e);
+        st[64] = m;
+        st[65] = (double)e;
         st[66] = nan_seen ? 1.0 : 0.0;
     }
     // start of a segment: the walk's initial matrix at step 0, else the state
@@ -254,9 +334,12 @@ struct FChain {
             if ((uint32_t)i == W.p_row) p = P[i][M_ - 1];
             if ((uint32_t)i == W.q_row) q = P[i][M_ - 1];
         }
+        double m = sc_m;
+        int e = sc_e;
+        scale_norm(m, e);
         out[0] = p;
         out[1] = q;
-        out[2] = __dadd_rn(log(sc_m), (double)sc_e * 0.69314718055994530942);
+        out[2] = __dadd_rn(log(m), (double)e * 0.69314718055994530942);
     }
 };
 
@@ -296,34 +379,50 @@ struct FVec {
         for (int k = 1; k < M_; ++k) c = __fma_rn(a[k], x[k], c);
         return c;
     }
-    __device__ __forceinline__ void step(const double (&X)[M_][M_]) {
+    // v <- X @ v; returns the max magnitude key of the new entries
+    __device__ __forceinline__ unsigned long long product(const double (&X)[M_][M_]) {
         double w[M_];
-        double mx = 0.0;
-        bool has_nan = false;
+        unsigned long long mb = 0;
 #pragma unroll
         for (int i = 0; i < M_; ++i) {
             w[i] = dot(X[i], v);
-            has_nan |= w[i] != w[i];
-            mx = fmax(mx, fabs(w[i]));
+            mb = max(mb, mag_key(w[i]));
         }
 #pragma unroll
         for (int i = 0; i < M_; ++i) v[i] = w[i];
-        if (!has_nan && mx > 1e10) {
-            rescale_n<M_>(v, mx);
-            scale_acc(sc_m, sc_e, mx);
-        }
-        nan_seen |= has_nan;
+        return mb;
     }
     // companion-shaped step matrix from its last column: the dense product
     // with the exact 0 and 1 entries
-    __device__ __forceinline__ void step_companion(const double (&c)[M_]) {
+    __device__ __forceinline__ unsigned long long product_companion(const double (&c)[M_]) {
         double X[M_][M_];
 #pragma unroll
         for (int i = 0; i < M_; ++i)
 #pragma unroll
             for (int j = 0; j < M_; ++j) X[i][j] = (j == M_ - 1) ? c[i] : (i == j + 1 ? 1.0 : 0.0);
-        step(X);
+        return product(X);
     }
+    __device__ __forceinline__ void finish(unsigned long long mb) {
+        const bool nan = mb > kInfKey;
+        if (!nan && mb > kRescaleKey) {
+            const double mx = __longlong_as_double((long long)mb);
+            rescale_n<M_>(v, mx);
+            scale_acc(sc_m, sc_e, mx);
+        }
+        nan_seen |= nan;
+    }
+    __device__ __forceinline__ void finish_fast(unsigned long long mb, bool& out) {
+        const bool nan = mb > kInfKey;
+        out |= rescale_fast<M_>(v, !nan && mb > kRescaleKey, __longlong_as_double((long long)mb), sc_m, sc_e);
+        nan_seen |= nan;
+    }
+    __device__ __forceinline__ void step(const double (&X)[M_][M_]) { finish(product(X)); }
+    __device__ __forceinline__ void step_companion(const double (&c)[M_]) { finish(product_companion(c)); }
+    __device__ __forceinline__ void step_fast(const double (&X)[M_][M_], bool& out) { finish_fast(product(X), out); }
+    __device__ __forceinline__ void step_companion_fast(const double (&c)[M_], bool& out) {
+        finish_fast(product_companion(c), out);
+    }
+    __device__ __forceinline__ void renorm() { scale_norm(sc_m, sc_e); }
     __device__ __forceinline__ void load(const double* st) {
 #pragma unroll
         for (int i = 0; i < M_; ++i) v[i] = st[i];
@@ -334,8 +433,11 @@ struct FVec {
     __device__ __forceinline__ void store(double* st) const {
 #pragma unroll
         for (int i = 0; i < M_; ++i) st[i] = v[i];
-        st[64] = sc_m;
-        st[65] = (double)sc_e;
+        double m = sc_m;
+        int e = sc_e;
+        scale_norm(m, e);
+        st[64] = m;
+        st[65] = (double)e;
         st[66] = nan_seen ? 1.0 : 0.0;
     }
     __device__ __forceinline__ void begin(const DevWalk& W, const DevShadowSeg& g, const double* state,
@@ -350,9 +452,12 @@ struct FVec {
             if ((uint32_t)i == W.p_row) p = v[i];
             if ((uint32_t)i == W.q_row) q = v[i];
         }
+        double m = sc_m;
+        int e = sc_e;
+        scale_norm(m, e);
         out[0] = p;
         out[1] = q;
-        out[2] = __dadd_rn(log(sc_m), (double)sc_e * 0.69314718055994530942);
+        out[2] = __dadd_rn(log(m), (double)e * 0.69314718055994530942);
     }
     __device__ __forceinline__ void end(const DevWalk& W, const DevShadowSeg& g, double* state,
                                         double* shadow, uint32_t* status, uint32_t w) const {
@@ -388,6 +493,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // thousands of cycles, far more than the copy of the next one, so small
 // buffers suffice (longer chunks measured slower).
 __host__ __device__ constexpr int chain_chunk_steps(int ne) { return ne >= 8 ? 2 : 16 / ne; }
+// Staging buffers per chain warp (double buffering: one chunk in flight while
+// one is consumed; deeper pipelines measured slower).
+__host__ __device__ constexpr int chain_buffers(int /*ne*/) { return 2; }
 
 // Evaluation: each warp takes items of kEvalSteps steps of one segment and
 // runs the float interpreter on U sub-blocks of 32 steps at a time.  The
@@ -396,6 +504,9 @@ __host__ __device__ constexpr int chain_chunk_steps(int ne) { return ne >= 8 ? 2
 // column, so no warp synchronisation is needed.
 template <int U>
 __global__ void __launch_bounds__(128) k_shadow_eval(const ShadowArgs A) {
+    // the chain launch that follows may place its blocks from now on; it
+    // waits for this grid's completion before it reads the step matrices
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     extern __shared__ double dsm[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -463,6 +574,56 @@ __device__ __forceinline__ void chain_step(Chain& ch, const double (&X)[COMP ? M
     }
 }
 
+template <int M_, bool COMP, class Chain>
+__device__ __forceinline__ void chain_step_fast(Chain& ch, const double (&X)[COMP ? M_ : M_ * M_], bool& out) {
+    if (COMP) {
+        double cv[M_];
+#pragma unroll
+        for (int i = 0; i < M_; ++i) cv[i] = X[i];
+        ch.step_companion_fast(cv, out);
+    } else {
+        double Xm[M_][M_];
+#pragma unroll
+        for (int e = 0; e < M_ * M_; ++e) Xm[e / M_][e % M_] = X[e];
+        ch.step_fast(Xm, out);
+    }
+}
+
+// The exact steps of one staged chunk (rarely run: only when a lane of the
+// warp left the Markstein domain on the fast path).  Not inlined, and taking
+// and returning the chain by value, so that its IEEE division code stays out
+// of the fast loop's registers and schedule.
+template <int M_, bool COMP, class Chain, int CS>
+__device__ __noinline__ Chain chain_chunk_exact(Chain ch, const double* buf, int lane) {
+    constexpr int NE = COMP ? M_ : M_ * M_;
+#pragma unroll 1
+    for (int t = 0; t < CS; ++t) {
+        double X[NE];
+#pragma unroll
+        for (int e = 0; e < NE; ++e) X[e] = buf[(t * NE + e) * 32 + lane];
+        chain_step<M_, COMP, Chain>(ch, X);
+    }
+    return ch;
+}
+
+template <int M_, bool COMP, class Chain, int CS>
+__device__ __noinline__ Chain chain_chunk_partial(Chain ch, const double* buf, int lane, uint64_t base, uint64_t len,
+                                                  uint64_t cp_rel, double* cp_out, const DevWalk* Wp) {
+    constexpr int NE = COMP ? M_ : M_ * M_;
+#pragma unroll 1
+    for (int t = 0; t < CS; ++t) {
+        const uint64_t rel = base + t;
+        if (rel < len) {
+            double X[NE];
+#pragma unroll
+            for (int e = 0; e < NE; ++e) X[e] = buf[(t * NE + e) * 32 + lane];
+            chain_step<M_, COMP, Chain>(ch, X);
+            if (rel == cp_rel) ch.write(cp_out, *Wp);
+        }
+    }
+    return ch;
+}
+
 // Chain: lane = segment, 32 segments per warp, every warp of the block on
 // its own items.  The
 // warp's entries for the next chunk of steps are copied into shared memory
@@ -470,17 +631,26 @@ __device__ __forceinline__ void chain_step(Chain& ch, const double (&X)[COMP ? M
 // reads what it copied itself, so the per-thread cp.async group wait is the
 // only synchronisation.
 // FLAGS: bit 0 the float step matrix has the companion shape (only its last
-// column is stored), bit 1 state-vector walks.
+// column is stored), bit 1 state-vector walks, bit 2 lean: chains co-located
+// with walk kernels run the exact steps, which skip the rescale work on
+// steps without one (fewest instructions, as they share issue slots with the
+// walks); the others run the fast chunks.
 template <int M_, int FLAGS>
 __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
     constexpr bool COMP = (FLAGS & 1) != 0;
     constexpr bool VEC = (FLAGS & 2) != 0;
+    constexpr bool LEAN = (FLAGS & 4) != 0;
     using Chain = typename std::conditional<VEC, FVec<M_>, FChain<M_>>::type;
     constexpr int NE = COMP ? M_ : M_ * M_;
     constexpr int CS = chain_chunk_steps(NE);
     extern __shared__ double dsm_all[];
     const int lane = threadIdx.x & 31;
-    double* dsm = dsm_all + (size_t)(threadIdx.x >> 5) * 2 * CS * NE * 32;
+    constexpr int NB = chain_buffers(NE);
+    double* dsm = dsm_all + (size_t)(threadIdx.x >> 5) * NB * CS * NE * 32;
+    // launched as a programmatic dependent of the evaluation kernel: wait for
+    // that grid to complete (and its step matrices to be visible); returns at
+    // once when there is no such prerequisite
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     stamp_begin(A.tstamp);
     for (;;) {
         uint32_t it = 0;
@@ -495,6 +665,10 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
         Chain ch;
         ch.begin(W, g, A.state, A.axis);
         const uint64_t len = active ? g.s1 - g.s0 : 0;
+        // lanes past the item's segments stream lane 0's step matrices (their
+        // results are dropped): stale shared memory could hold values that
+        // take slow special-case paths and hold up the whole warp
+        const uint64_t load_len = g.s1 - g.s0;
         const double* src = A.mf + g.mf_off;
         unsigned long long mlen = len;
         // chunks every lane runs in full, and the chunk holding any lane's
@@ -510,25 +684,32 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
                                     ? W.checkpoint - g.s0 - 1 : ~0ull;
         const uint64_t nch = (mlen + CS - 1) / CS;
         auto issue = [&](uint64_t c) {
-            double* buf = dsm + (size_t)(c & 1) * CS * NE * 32;
+            double* buf = dsm + (size_t)(c % NB) * CS * NE * 32;
 #pragma unroll 1
             for (int t = 0; t < CS; ++t) {
                 const uint64_t rel = c * CS + t;
-                if (rel < len)
+                if (rel < load_len)
 #pragma unroll
                     for (int e = 0; e < NE; ++e) cp_async8(buf + (t * NE + e) * 32 + lane, src + rel * NE + e);
             }
         };
-        if (nch) issue(0);
-        cp_async_commit();
-        for (uint64_t c = 0; c < nch; ++c) {
-            if (c + 1 < nch) issue(c + 1);
+        // chunk c goes to buffer c % NB, one commit group per chunk (empty
+        // past the end), so waiting until NB - 1 groups are pending means
+        // chunk c has landed; chunk c + NB - 1 is issued into the buffer
+        // chunk c - 1 has left
+#pragma unroll 1
+        for (int c0 = 0; c0 + 1 < NB; ++c0) {
+            if ((uint64_t)c0 < nch) issue(c0);
             cp_async_commit();
-            cp_async_wait<1>();
-            const double* buf = dsm + (size_t)(c & 1) * CS * NE * 32;
+        }
+        for (uint64_t c = 0; c < nch; ++c) {
+            if (c + NB - 1 < nch) issue(c + NB - 1);
+            cp_async_commit();
+            cp_async_wait<NB - 1>();
+            const double* buf = dsm + (size_t)(c % NB) * CS * NE * 32;
             const uint64_t base = c * CS;
             const bool cp_here = __any_sync(0xffffffffu, cp_rel >= base && cp_rel < base + CS);
-            if (base + CS <= minlen && !cp_here) {
+            if (LEAN && base + CS <= minlen && !cp_here) {
                 double X[NE];
 #pragma unroll
                 for (int e = 0; e < NE; ++e) X[e] = buf[e * 32 + lane];
@@ -542,18 +723,30 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
 #pragma unroll
                     for (int e = 0; e < NE; ++e) X[e] = Y[e];
                 }
-            } else {
-#pragma unroll 1
-                for (int t = 0; t < CS; ++t) {
-                    const uint64_t rel = base + t;
-                    if (rel < len) {
-                        double X[NE];
+            } else if (!LEAN && base + CS <= minlen && !cp_here) {
+                // fast steps (no division branch); a chunk where any lane
+                // rescaled outside the Markstein domain runs again exactly
+                // from its saved start
+                const Chain saved = ch;
+                bool out = false;
+                double X[NE];
 #pragma unroll
-                        for (int e = 0; e < NE; ++e) X[e] = buf[(t * NE + e) * 32 + lane];
-                        chain_step<M_, COMP, Chain>(ch, X);
-                        if (rel == cp_rel) ch.write(A.shadow + 3 * ((size_t)A.n_walks + g.walk), W);
-                    }
+                for (int e = 0; e < NE; ++e) X[e] = buf[e * 32 + lane];
+#pragma unroll 2
+                for (int t = 0; t < CS; ++t) {
+                    double Y[NE];
+                    const int tn = t + 1 < CS ? t + 1 : t;
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) Y[e] = buf[(tn * NE + e) * 32 + lane];
+                    chain_step_fast<M_, COMP, Chain>(ch, X, out);
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) X[e] = Y[e];
                 }
+                ch.renorm();
+                if (__any_sync(0xffffffffu, out && active)) ch = chain_chunk_exact<M_, COMP, Chain, CS>(saved, buf, lane);
+            } else {
+                ch = chain_chunk_partial<M_, COMP, Chain, CS>(ch, buf, lane, base, len, cp_rel,
+                                                               A.shadow + 3 * ((size_t)A.n_walks + g.walk), A.walks + g.walk);
             }
         }
         cp_async_wait<0>();
@@ -562,8 +755,46 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
     stamp_end(A.tstamp);
 }
 
+// Chain state and difference table of one integer-difference shadow lane.
+template <int M_, int NS, int D>
+struct FdChain {
+    FChain<M_> ch;
+    int64_t fd[NS][D + 1];
+};
+
+// n exact steps of the integer-difference shadow, with the checkpoint write
+// when step s0 + t + 1 is the checkpoint.  Rarely run (segment ends,
+// checkpoints, chunks that left the Markstein domain); not inlined and by
+// value so that the IEEE division code stays out of the fast loop.
+template <int CLS, int M_, int NS, int D>
+__device__ __noinline__ FdChain<M_, NS, D> intfd_exact(FdChain<M_, NS, D> st, int n, uint64_t s0,
+                                                       uint64_t checkpoint, double* cp_out, const DevWalk* Wp) {
+#pragma unroll 1
+    for (int t = 0; t < n; ++t) {
+        if (CLS == CLS_COMPANION) {
+            double c[M_];
+#pragma unroll
+            for (int i = 0; i < M_; ++i) c[i] = __ll2double_rn(st.fd[i][0]);
+            st.ch.step_companion(c);
+        } else {
+            double X[M_][M_];
+#pragma unroll
+            for (int e = 0; e < M_ * M_; ++e) X[e / M_][e % M_] = __ll2double_rn(st.fd[e][0]);
+            st.ch.step(X);
+        }
+#pragma unroll
+        for (int i = 0; i < NS; ++i)
+#pragma unroll
+            for (int j = 0; j < D; ++j) st.fd[i][j] += st.fd[i][j + 1];
+        if (checkpoint && s0 + t + 1 == checkpoint) st.ch.write(cp_out, *Wp);
+    }
+    return st;
+}
+
 // Integer-difference shadow: NS streams of depth D per walk, lane = walk.
-template <int CLS, int M_, int D>
+// LEAN: co-located with walk kernels, the exact steps inline (they skip the
+// rescale work on steps without one); otherwise fast chunks.
+template <int CLS, int M_, int D, bool LEAN>
 __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
     constexpr int NS = (CLS == CLS_COMPANION) ? M_ : M_ * M_;
     extern __shared__ double dsm[];
@@ -604,39 +835,85 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
         const uint32_t wi = g.walk;
         const DevWalk W = A.walks[wi];
         const DevProgram G = A.progs[W.prog];
-        int64_t fd[NS][D + 1];
+        FdChain<M_, NS, D> st;
 #pragma unroll
         for (int j = 0; j <= D; ++j)
 #pragma unroll
-            for (int i = 0; i < NS; ++i) fd[i][j] = ((uint32_t)j <= G.degree && active) ? stage[(j * NS + i) * 32 + lane] : 0;
+            for (int i = 0; i < NS; ++i) st.fd[i][j] = ((uint32_t)j <= G.degree && active) ? stage[(j * NS + i) * 32 + lane] : 0;
 #pragma unroll
         for (int lvl = 1; lvl <= D; ++lvl)
 #pragma unroll
             for (int j = D; j >= lvl; --j)
                 if ((uint32_t)j <= G.degree)
 #pragma unroll
-                    for (int i = 0; i < NS; ++i) fd[i][j] -= fd[i][j - 1];
-        FChain<M_> ch;
-        ch.begin(W, g, A.state, A.axis);
+                    for (int i = 0; i < NS; ++i) st.fd[i][j] -= st.fd[i][j - 1];
+        st.ch.begin(W, g, A.state, A.axis);
         const uint64_t s_end = active ? g.s1 : g.s0;
-        for (uint64_t s = g.s0; s < s_end; ++s) {
-            if (CLS == CLS_COMPANION) {
-                double c[M_];
+        double* cp_out = A.shadow + 3 * ((size_t)A.n_walks + wi);
+        // Chunks of kFdChunk fast steps while every lane that still has steps
+        // has a whole chunk left with no checkpoint inside it; a chunk where a
+        // lane rescaled outside the Markstein domain runs again exactly from
+        // its saved start.  Other steps (segment ends, checkpoints) run exactly.
+        constexpr int kFdChunk = 8;
+        uint64_t s = g.s0;
+        if (LEAN) {
+            for (; s < s_end; ++s) {
+                if (CLS == CLS_COMPANION) {
+                    double c[M_];
 #pragma unroll
-                for (int i = 0; i < M_; ++i) c[i] = __ll2double_rn(fd[i][0]);
-                ch.step_companion(c);
-            } else {
-                double X[M_][M_];
+                    for (int i = 0; i < M_; ++i) c[i] = __ll2double_rn(st.fd[i][0]);
+                    st.ch.step_companion(c);
+                } else {
+                    double X[M_][M_];
 #pragma unroll
-                for (int e = 0; e < M_ * M_; ++e) X[e / M_][e % M_] = __ll2double_rn(fd[e][0]);
-                ch.step(X);
+                    for (int e = 0; e < M_ * M_; ++e) X[e / M_][e % M_] = __ll2double_rn(st.fd[e][0]);
+                    st.ch.step(X);
+                }
+#pragma unroll
+                for (int i = 0; i < NS; ++i)
+#pragma unroll
+                    for (int j = 0; j < D; ++j) st.fd[i][j] += st.fd[i][j + 1];
+                if (W.checkpoint && s + 1 == W.checkpoint) st.ch.write(cp_out, W);
             }
-#pragma unroll
-            for (int i = 0; i < NS; ++i)
-#pragma unroll
-                for (int j = 0; j < D; ++j) fd[i][j] += fd[i][j + 1];
-            if (W.checkpoint && s + 1 == W.checkpoint) ch.write(A.shadow + 3 * ((size_t)A.n_walks + wi), W);
         }
+        if (!LEAN) {
+            for (;;) {
+                const bool left = s < s_end;
+                if (!__any_sync(0xffffffffu, left)) break;
+                const bool cp_in = W.checkpoint > s && W.checkpoint <= s + kFdChunk;
+                if (__all_sync(0xffffffffu, !left || (s + kFdChunk <= s_end && !cp_in))) {
+                    const FdChain<M_, NS, D> saved = st;
+                    bool out = false;
+#pragma unroll 2
+                    for (int t = 0; t < kFdChunk; ++t) {
+                        if (CLS == CLS_COMPANION) {
+                            double c[M_];
+#pragma unroll
+                            for (int i = 0; i < M_; ++i) c[i] = __ll2double_rn(st.fd[i][0]);
+                            st.ch.step_companion_fast(c, out);
+                        } else {
+                            double X[M_][M_];
+#pragma unroll
+                            for (int e = 0; e < M_ * M_; ++e) X[e / M_][e % M_] = __ll2double_rn(st.fd[e][0]);
+                            st.ch.step_fast(X, out);
+                        }
+#pragma unroll
+                        for (int i = 0; i < NS; ++i)
+#pragma unroll
+                            for (int j = 0; j < D; ++j) st.fd[i][j] += st.fd[i][j + 1];
+                    }
+                    st.ch.renorm();
+                    if (__any_sync(0xffffffffu, out && left))
+                        st = intfd_exact<CLS, M_, NS, D>(saved, kFdChunk, s, 0, cp_out, A.walks + wi);
+                    if (left) s += kFdChunk;
+                    else st = saved;      // lanes without steps keep their state
+                } else if (left) {
+                    st = intfd_exact<CLS, M_, NS, D>(st, 1, s, W.checkpoint, cp_out, A.walks + wi);
+                    ++s;
+                }
+            }
+        }
+        const FChain<M_>& ch = st.ch;
         if (active) ch.end(W, g, A.state, A.shadow, A.status, wi);
         __syncwarp();
     }
