@@ -53,7 +53,7 @@ int get_plan(const uint8_t* blob, uint64_t size, std::shared_ptr<Plan>* out, std
     // the cache is keyed by the blob's bytes; lookups hash them in place
     const std::string_view key(reinterpret_cast<const char*>(blob), (size_t)size);
     {
-        std::lock_guard<std::mutex> lk(g_ctx->mu);
+        std::shared_lock<std::shared_mutex> lk(g_ctx->plan_mu);
         auto it = g_ctx->plan_cache.find(key);
         if (it != g_ctx->plan_cache.end()) {
             *out = it->second;
@@ -76,7 +76,7 @@ int get_plan(const uint8_t* blob, uint64_t size, std::shared_ptr<Plan>* out, std
         if (!plan->dops.empty())
             std::memcpy(q + sizeof n_ops + sizeof(Insn) * n_ops, plan->dops.data(), sizeof(Insn) * plan->dops.size());
     }
-    std::lock_guard<std::mutex> lk(g_ctx->mu);
+    std::unique_lock<std::shared_mutex> lk(g_ctx->plan_mu);
     if (g_ctx->code_ids.size() > 100000) g_ctx->code_ids.clear();
     auto ci = g_ctx->code_ids.find(code_key);
     if (ci == g_ctx->code_ids.end()) ci = g_ctx->code_ids.emplace(std::move(code_key), g_ctx->next_code_id++).first;
@@ -85,6 +85,77 @@ int get_plan(const uint8_t* blob, uint64_t size, std::shared_ptr<Plan>* out, std
     g_ctx->plan_cache.emplace(std::string_view(plan->blob), plan);
     *out = plan;
     return DR_OK;
+}
+
+HostPool::HostPool(int workers) {
+    for (int i = 0; i < workers; ++i) threads_.emplace_back([this] { worker(); });
+}
+
+HostPool::~HostPool() {
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : threads_) t.join();
+}
+
+void HostPool::take_parts(const std::function<void(int, size_t, size_t)>* fn, int parts, size_t n) {
+    for (;;) {
+        const int p = next_.fetch_add(1);
+        if (p >= parts) return;
+        (*fn)(p, n * (size_t)p / (size_t)parts, n * (size_t)(p + 1) / (size_t)parts);
+        std::lock_guard<std::mutex> lk(mu_);
+        if (++done_ == parts) done_cv_.notify_all();
+    }
+}
+
+void HostPool::worker() {
+    uint64_t seen = 0;
+    for (;;) {
+        const std::function<void(int, size_t, size_t)>* fn;
+        int parts;
+        size_t n;
+        {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+            if (stop_) return;
+            seen = gen_;
+            // the job's fields stay as read here until active_ returns to 0
+            fn = fn_;
+            parts = fn ? parts_ : 0;
+            n = n_;
+            ++active_;
+        }
+        // a worker that woke after the job ended holds no job: it must not
+        // touch the part counter, which the next job may already use
+        if (fn) take_parts(fn, parts, n);
+        std::lock_guard<std::mutex> lk(mu_);
+        if (--active_ == 0) done_cv_.notify_all();
+    }
+}
+
+void HostPool::run(int parts, size_t n, const std::function<void(int, size_t, size_t)>& fn) {
+    std::lock_guard<std::mutex> one(run_mu_);
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        fn_ = &fn;
+        parts_ = parts;
+        n_ = n;
+        next_.store(0);
+        done_ = 0;
+        ++gen_;
+    }
+    cv_.notify_all();
+    take_parts(&fn, parts, n);
+    std::unique_lock<std::mutex> lk(mu_);
+    done_cv_.wait(lk, [&] { return done_ == parts && active_ == 0; });
+    fn_ = nullptr;
+}
+
+HostPool& host_pool() {
+    static HostPool pool(std::max(1, std::min(7, (int)std::thread::hardware_concurrency() / 2 - 1)));
+    return pool;
 }
 
 int crt_limbs_for(int K) { return (31 * K + 31) / 32 + 2; }
@@ -262,6 +333,28 @@ static void build_mark(int i) {
     else g_build_ms[i - 1] = std::chrono::duration<double, std::milli>(t - g_build_t0).count();
 }
 
+// Host-pool use in batch construction: parts for n items (one part below
+// kPoolMin items; about kPoolGrain items per part otherwise).
+constexpr size_t kPoolMin = 1024, kPoolGrain = 512;
+static int build_parts(size_t n) {
+    if (n < kPoolMin) return 1;
+    return (int)std::min<size_t>((size_t)host_pool().threads() * 2, (n + kPoolGrain - 1) / kPoolGrain);
+}
+// First error of a part (item index, status, message); the lowest index wins.
+struct BuildErr {
+    int64_t at = -1;
+    int rc = DR_OK;
+    std::string msg;
+};
+static int first_error(const std::vector<BuildErr>& e) {
+    const BuildErr* best = nullptr;
+    for (const BuildErr& x : e)
+        if (x.at >= 0 && (!best || x.at < best->at)) best = &x;
+    if (!best) return DR_OK;
+    set_error(best->msg);
+    return best->rc;
+}
+
 int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs,
                 const uint64_t* blob_offsets, int32_t n_programs, const int64_t* axis,
                 uint64_t n_axis, const dr_tune* tune, uint64_t n_res, std::unique_ptr<Batch>* out) {
@@ -283,37 +376,64 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     std::vector<DevProgram> dprogs(n_programs);
     std::vector<uint4> code;
     std::vector<int64_t> consts;
-    code.reserve(1024);
-    consts.reserve((size_t)n_programs * 8);
+
     std::unordered_map<uint32_t, std::pair<uint32_t, uint32_t>> code_at;   // code_id -> (op_off, dop_off)
     uint32_t last_code_id = 0;
     std::pair<uint32_t, uint32_t> last_code_at{0, 0};
+    // plans on the host pool (parts in program order; the first failing
+    // program is reported, as a serial pass would)
+    {
+        const int parts = build_parts(n_programs);
+        std::vector<BuildErr> perr(parts);
+        auto plan_range = [&](int part, size_t lo, size_t hi) {
+            for (size_t i = lo; i < hi; ++i)
+                if (blob_offsets[i + 1] < blob_offsets[i]) {
+                    perr[part] = {(int64_t)i, DR_ERR_ARG, "blob_offsets not increasing"};
+                    hi = i;
+                    break;
+                }
+            {
+                // cached plans under one shared lock per part
+                std::shared_lock<std::shared_mutex> lk(C.plan_mu);
+                for (size_t i = lo; i < hi; ++i) {
+                    const std::string_view key(reinterpret_cast<const char*>(blobs + blob_offsets[i]),
+                                               (size_t)(blob_offsets[i + 1] - blob_offsets[i]));
+                    auto it = C.plan_cache.find(key);
+                    if (it != C.plan_cache.end()) plans[i] = it->second;
+                }
+            }
+            for (size_t i = lo; i < hi; ++i) {
+                if (plans[i]) continue;
+                std::string err;
+                const int r = get_plan(blobs + blob_offsets[i], blob_offsets[i + 1] - blob_offsets[i], &plans[i], &err);
+                if (r) {
+                    if (perr[part].at < 0 || (int64_t)i < perr[part].at)
+                        perr[part] = {(int64_t)i, r, "program " + std::to_string(i) + ": " + err};
+                    return;
+                }
+            }
+        };
+        if (parts > 1) host_pool().run(parts, (size_t)n_programs, plan_range);
+        else plan_range(0, 0, (size_t)n_programs);
+        if ((rc = first_error(perr))) return rc;
+    }
+    // descriptors and offsets (serial, cheap); programs with the same
+    // instruction streams share one copy of them
+    std::vector<uint8_t> copy_code(n_programs, 0);     // first program of its code_id
+    size_t code_total = 0, consts_total = 0;
     for (int32_t i = 0; i < n_programs; ++i) {
-        if (blob_offsets[i + 1] < blob_offsets[i]) {
-            set_error("blob_offsets not increasing");
-            return DR_ERR_ARG;
-        }
-        std::string err;
-        rc = get_plan(blobs + blob_offsets[i], blob_offsets[i + 1] - blob_offsets[i], &plans[i], &err);
-        if (rc) {
-            set_error("program " + std::to_string(i) + ": " + err);
-            return rc;
-        }
         const Plan& P = *plans[i];
         DevProgram d{};
         d.m = P.m;
         d.dim = P.dim;
         d.cls = (engine == DR_ENGINE_AUTO) ? (uint32_t)P.cls : (uint32_t)CLS_INTERP;
         d.degree = P.degree;
-        // programs with the same instruction streams share one copy
         if (P.code_id != last_code_id) {
             auto at = code_at.find(P.code_id);
             if (at == code_at.end()) {
-                std::pair<uint32_t, uint32_t> off;
-                off.first = (uint32_t)code.size();
-                for (const Insn& in : P.ops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
-                off.second = (uint32_t)code.size();
-                for (const Insn& in : P.dops) code.push_back(make_uint4(in.op, in.a, in.b, in.c));
+                std::pair<uint32_t, uint32_t> off((uint32_t)code_total, (uint32_t)(code_total + P.ops.size()));
+                code_total += P.ops.size() + P.dops.size();
+                copy_code[i] = 1;
                 at = code_at.emplace(P.code_id, off).first;
             }
             last_code_id = P.code_id;
@@ -325,91 +445,134 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         d.dop_off = last_code_at.second;
         d.dn_ops = (uint32_t)P.dops.size();
         d.dn_regs = P.dn_regs;
-        d.c_off = (uint32_t)consts.size();
+        d.c_off = (uint32_t)consts_total;
         d.n_consts = (uint32_t)P.consts.size();
-        consts.insert(consts.end(), P.consts.begin(), P.consts.end());
+        consts_total += P.consts.size();
         d.n_streams = P.n_streams;
         d.zero_reg = P.zero_reg;
         d.shadow_fd = (!P.has_inv && (P.cls == CLS_COMPANION || P.cls == CLS_DENSE)) ? 1u : 0u;
         d.fcomp = P.fcomp ? 1u : 0u;
         dprogs[i] = d;
     }
+    if (code_total > UINT32_MAX || consts_total > UINT32_MAX) {
+        set_error("programs too large: more than 2^32 instructions or constants");
+        return DR_ERR_UNSUPPORTED;
+    }
+    // the instruction streams (Insn and uint4 are both four 32-bit words) and
+    // constants, copied on the host pool
+    static_assert(sizeof(Insn) == sizeof(uint4), "instruction layout");
+    code.resize(std::max<size_t>(code_total, 1));
+    consts.resize(std::max<size_t>(consts_total, 1));
+    {
+        auto copy_range = [&](int, size_t lo, size_t hi) {
+            for (size_t i = lo; i < hi; ++i) {
+                const Plan& P = *plans[i];
+                const DevProgram& d = dprogs[i];
+                if (copy_code[i]) {
+                    if (!P.ops.empty()) std::memcpy(&code[d.op_off], P.ops.data(), sizeof(Insn) * P.ops.size());
+                    if (!P.dops.empty()) std::memcpy(&code[d.dop_off], P.dops.data(), sizeof(Insn) * P.dops.size());
+                }
+                if (!P.consts.empty()) std::memcpy(&consts[d.c_off], P.consts.data(), sizeof(int64_t) * P.consts.size());
+            }
+        };
+        const int parts = build_parts(n_programs);
+        if (parts > 1) host_pool().run(parts, (size_t)n_programs, copy_range);
+        else copy_range(0, 0, (size_t)n_programs);
+    }
 
     build_mark(1);
     // ---- walks
     std::vector<DevWalk> dwalks(n_walks);
     uint64_t total_group_steps = 0, n_groups = 0;
-    for (int32_t w = 0; w < n_walks; ++w) {
-        const dr_walk_desc& W = walks[w];
-        if (W.program >= (uint32_t)n_programs) { set_error("walk program index out of range"); return DR_ERR_ARG; }
-        const DevProgram& G = dprogs[W.program];
-        if (W.K < 1 || W.K > DR_MAX_K) { set_error("K outside 1..DR_MAX_K"); return DR_ERR_UNSUPPORTED; }
-        if (W.q_row >= G.m || W.p_row >= G.m) { set_error("p_row or q_row >= m"); return DR_ERR_ARG; }
-        if (W.flags & DR_WALK_VEC) {
-            if (W.flags & DR_WALK_INIT_PCF) {
-                set_error("a state-vector walk starts from v(0), not the PCF initial matrix");
-                return DR_ERR_ARG;
+    {
+        // validation and device descriptors on the host pool; per-part sums
+        struct WalkAcc {
+            uint64_t group_steps = 0, groups = 0, prime_steps = 0;
+            bool shadow = false;
+        };
+        const int parts = build_parts((size_t)n_walks);
+        std::vector<BuildErr> perr(parts);
+        std::vector<WalkAcc> accs(parts);
+        auto walk_range = [&](int part, size_t w_lo, size_t w_hi) {
+            WalkAcc& acc = accs[part];
+            for (size_t wi = w_lo; wi < w_hi; ++wi) {
+                const int32_t w = (int32_t)wi;
+                const dr_walk_desc& W = walks[w];
+                if (W.program >= (uint32_t)n_programs) { perr[part] = {(int64_t)w, DR_ERR_ARG, "walk program index out of range"}; return; }
+                const DevProgram& G = dprogs[W.program];
+                if (W.K < 1 || W.K > DR_MAX_K) { perr[part] = {(int64_t)w, DR_ERR_UNSUPPORTED, "K outside 1..DR_MAX_K"}; return; }
+                if (W.q_row >= G.m || W.p_row >= G.m) { perr[part] = {(int64_t)w, DR_ERR_ARG, "p_row or q_row >= m"}; return; }
+                if (W.flags & DR_WALK_VEC) {
+                    if (W.flags & DR_WALK_INIT_PCF) {
+                        perr[part] = {(int64_t)w, DR_ERR_ARG, "a state-vector walk starts from v(0), not the PCF initial matrix"}; return;
+                    }
+                    if (W.checkpoint) { perr[part] = {(int64_t)w, DR_ERR_UNSUPPORTED, "state-vector walks have no checkpoint"}; return; }
+                    if (W.vec_offset + (uint64_t)G.m * W.K + G.m > n_axis) {
+                        perr[part] = {(int64_t)w, DR_ERR_ARG, "state-vector initial values out of range of the axis parameters"}; return;
+                    }
+                }
+                if (W.checkpoint && W.checkpoint >= W.depth) { perr[part] = {(int64_t)w, DR_ERR_ARG, "checkpoint must be < depth"}; return; }
+                if ((W.flags & DR_WALK_INIT_PCF) && G.m < 2) { perr[part] = {(int64_t)w, DR_ERR_ARG, "PCF initial matrix needs m >= 2"}; return; }
+                if (W.res_offset + W.K > n_res || (W.checkpoint && W.cp_res_offset + W.K > n_res)) {
+                    perr[part] = {(int64_t)w, DR_ERR_ARG, "residue output offset out of range"}; return;
+                }
+                if (W.axis_offset + 4ull * G.dim > n_axis) { perr[part] = {(int64_t)w, DR_ERR_ARG, "axis parameters out of range"}; return; }
+                if (W.depth > (1ull << 40)) { perr[part] = {(int64_t)w, DR_ERR_UNSUPPORTED, "depth above 2^40"}; return; }
+                for (uint32_t a = 0; a < G.dim; ++a) {
+                    const int64_t* ax = axis + W.axis_offset + 4 * a;
+                    if (ax[1] == 0 || ax[3] == 0) {
+                        // the reference divides by float(sd*td) (cmf_walk.py:281): ZeroDivisionError
+                        perr[part] = {(int64_t)w, DR_ERR_ARG, "zero shift or trajectory denominator"}; return;
+                    }
+                    const __int128 hi = (__int128)ax[0] * ax[3];
+                    const __int128 st = (__int128)ax[2] * ax[1];
+                    const __int128 lim = (__int128)1 << 62;
+                    const __int128 span = st * (__int128)(W.depth + 64);
+                    if (hi > lim || hi < -lim || span > lim || span < -lim || (__int128)ax[1] * ax[3] > lim ||
+                        (__int128)ax[1] * ax[3] < -lim) {
+                        perr[part] = {(int64_t)w, DR_ERR_UNSUPPORTED, "axis numerators exceed 2^62 over the walk"}; return;
+                    }
+                }
+                DevWalk d{};
+                d.prog = W.program;
+                d.K = W.K;
+                d.flags = W.flags;
+                d.q_row = W.q_row;
+                d.a0 = W.a0;
+                d.depth = W.depth;
+                d.checkpoint = W.checkpoint;
+                d.axis_off = W.axis_offset;
+                d.res_off = W.res_offset;
+                d.cp_res_off = W.cp_res_offset;
+                d.p_row = W.p_row;
+                d.vec_off = W.vec_offset;
+                d.shadow_mode = SHADOW_NONE;
+                if (W.flags & DR_WALK_SHADOW) {
+                    d.shadow_mode = SHADOW_INTERP;
+                    const Plan& P = *plans[W.program];
+                    const int Dt = template_degree(P.cls, P.m, P.degree);
+                    if (G.shadow_fd && G.cls != CLS_INTERP && Dt > 0 && !(W.flags & DR_WALK_VEC)) {
+                        const double b = float_bound_log2(P, axis + W.axis_offset, W.depth + 1);
+                        if (b < 53.0 && b + Dt < 61.0) d.shadow_mode = SHADOW_INTFD;
+                    }
+                    acc.shadow = true;
+                }
+                dwalks[w] = d;
+                const uint64_t nb = (W.K + 31) / 32;
+                acc.group_steps += nb * std::max<uint64_t>(W.depth, 1);
+                acc.groups += nb;
+                acc.prime_steps += (uint64_t)W.K * W.depth;
             }
-            if (W.checkpoint) { set_error("state-vector walks have no checkpoint"); return DR_ERR_UNSUPPORTED; }
-            if (W.vec_offset + (uint64_t)G.m * W.K + G.m > n_axis) {
-                set_error("state-vector initial values out of range of the axis parameters");
-                return DR_ERR_ARG;
-            }
+        };
+        if (parts > 1) host_pool().run(parts, (size_t)n_walks, walk_range);
+        else walk_range(0, 0, (size_t)n_walks);
+        if ((rc = first_error(perr))) return rc;
+        for (const WalkAcc& a : accs) {
+            total_group_steps += a.group_steps;
+            n_groups += a.groups;
+            B->prime_steps += a.prime_steps;
+            B->has_shadow |= a.shadow;
         }
-        if (W.checkpoint && W.checkpoint >= W.depth) { set_error("checkpoint must be < depth"); return DR_ERR_ARG; }
-        if ((W.flags & DR_WALK_INIT_PCF) && G.m < 2) { set_error("PCF initial matrix needs m >= 2"); return DR_ERR_ARG; }
-        if (W.res_offset + W.K > n_res || (W.checkpoint && W.cp_res_offset + W.K > n_res)) {
-            set_error("residue output offset out of range");
-            return DR_ERR_ARG;
-        }
-        if (W.axis_offset + 4ull * G.dim > n_axis) { set_error("axis parameters out of range"); return DR_ERR_ARG; }
-        if (W.depth > (1ull << 40)) { set_error("depth above 2^40"); return DR_ERR_UNSUPPORTED; }
-        for (uint32_t a = 0; a < G.dim; ++a) {
-            const int64_t* ax = axis + W.axis_offset + 4 * a;
-            if (ax[1] == 0 || ax[3] == 0) {
-                // the reference divides by float(sd*td) (cmf_walk.py:281): ZeroDivisionError
-                set_error("zero shift or trajectory denominator");
-                return DR_ERR_ARG;
-            }
-            const __int128 hi = (__int128)ax[0] * ax[3];
-            const __int128 st = (__int128)ax[2] * ax[1];
-            const __int128 lim = (__int128)1 << 62;
-            const __int128 span = st * (__int128)(W.depth + 64);
-            if (hi > lim || hi < -lim || span > lim || span < -lim || (__int128)ax[1] * ax[3] > lim ||
-                (__int128)ax[1] * ax[3] < -lim) {
-                set_error("axis numerators exceed 2^62 over the walk");
-                return DR_ERR_UNSUPPORTED;
-            }
-        }
-        DevWalk d{};
-        d.prog = W.program;
-        d.K = W.K;
-        d.flags = W.flags;
-        d.q_row = W.q_row;
-        d.a0 = W.a0;
-        d.depth = W.depth;
-        d.checkpoint = W.checkpoint;
-        d.axis_off = W.axis_offset;
-        d.res_off = W.res_offset;
-        d.cp_res_off = W.cp_res_offset;
-        d.p_row = W.p_row;
-        d.vec_off = W.vec_offset;
-        d.shadow_mode = SHADOW_NONE;
-        if (W.flags & DR_WALK_SHADOW) {
-            d.shadow_mode = SHADOW_INTERP;
-            const Plan& P = *plans[W.program];
-            const int Dt = template_degree(P.cls, P.m, P.degree);
-            if (G.shadow_fd && G.cls != CLS_INTERP && Dt > 0 && !(W.flags & DR_WALK_VEC)) {
-                const double b = float_bound_log2(P, axis + W.axis_offset, W.depth + 1);
-                if (b < 53.0 && b + Dt < 61.0) d.shadow_mode = SHADOW_INTFD;
-            }
-            B->has_shadow = true;
-        }
-        dwalks[w] = d;
-        const uint64_t nb = (W.K + 31) / 32;
-        total_group_steps += nb * std::max<uint64_t>(W.depth, 1);
-        n_groups += nb;
-        B->prime_steps += (uint64_t)W.K * W.depth;
     }
 
     build_mark(2);
@@ -420,15 +583,21 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     {
         std::map<LaunchKey, std::pair<uint64_t, uint64_t>> shape;
         uint64_t longest = 0;
+        LaunchKey prev{-1, 0, 0, 0};
+        std::pair<uint64_t, uint64_t>* cur = nullptr;   // shape entry of prev
         for (int32_t w = 0; w < n_walks; ++w) {
             const DevWalk& W = dwalks[w];
             const DevProgram& G = dprogs[W.prog];
             const Plan& P = *plans[W.prog];
             LaunchKey key{0, G.cls, G.m, 0};
             if (G.cls != CLS_INTERP) key.D = (uint32_t)template_degree(P.cls, P.m, P.degree);
+            if (!cur || key < prev || prev < key) {
+                cur = &shape[key];
+                prev = key;
+            }
             const uint64_t nb = (W.K + 31) / 32;
-            shape[key].first += nb;
-            shape[key].second += nb * W.depth;
+            cur->first += nb;
+            cur->second += nb * W.depth;
             longest = std::max<uint64_t>(longest, W.depth);
         }
         auto lg = [](uint64_t v) { int b = 0; while (v > 1) { v >>= 1; ++b; } return b; };
@@ -450,72 +619,149 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
                          : tuned_chunk ? tuned_chunk
                          : chunk_policy(total_group_steps, n_groups, C.sms, tune);
     B->chunk_used = chunk;
-    std::map<LaunchKey, std::vector<DevTile>> tile_sets;
-    std::vector<DevGroup> groups;
-    groups.reserve(n_groups);
-    uint32_t slots = 0;
-    std::vector<std::pair<uint64_t, uint64_t>> ranges;
-    LaunchKey prev_key{-1, 0, 0, 0};
-    std::vector<DevTile>* vec = nullptr;     // tile set of prev_key
-    size_t n_tiles_est = 0;                  // upper bound: chunks of each part, per prime block
-    for (int32_t w = 0; w < n_walks; ++w) {
-        const DevWalk& W = dwalks[w];
-        const uint64_t a = W.checkpoint, b = W.depth - W.checkpoint;
-        n_tiles_est += ((W.K + 31) / 32) * (2 + a / chunk + b / chunk);
-    }
-    for (int32_t w = 0; w < n_walks; ++w) {
-        const DevWalk& W = dwalks[w];
+    // Tiles and combine groups in walk order, on the host pool: a counting
+    // pass gives every part its offsets in the tile set of each launch class,
+    // in the group array and in the chunk slots, so each part writes its
+    // tiles in place with their final indices (the arrays one pass over the
+    // walks would give).
+    auto walk_key = [&](const DevWalk& W) {
         const DevProgram& G = dprogs[W.prog];
         const Plan& P = *plans[W.prog];
         LaunchKey key{0, G.cls, G.m, 0};
         if (G.cls != CLS_INTERP) key.D = (uint32_t)template_degree(P.cls, P.m, P.degree);
-        if (!vec || key < prev_key || prev_key < key) {
-            vec = &tile_sets[key];
-            prev_key = key;
-            // one launch class is the common case: the first gets the whole estimate
-            if (tile_sets.size() == 1 && vec->capacity() == 0) vec->reserve(n_tiles_est);
+        return key;
+    };
+    auto n_chunks_of = [&](const DevWalk& W) -> uint64_t {   // the ranges split() makes
+        auto nc = [&](uint64_t len) { return std::max<uint64_t>(1, (len + chunk - 1) / chunk); };
+        if (W.depth == 0) return 1;
+        if (W.checkpoint) return nc(W.checkpoint) + nc(W.depth - W.checkpoint);
+        return nc(W.depth);
+    };
+    struct TileCount {
+        std::map<LaunchKey, size_t> tiles;   // count, then this part's first index in the set
+        std::map<LaunchKey, std::pair<uint32_t, uint32_t>> rows;   // max registers, constants
+        uint64_t groups = 0, slots = 0;      // count, then this part's first group / slot
+    };
+    const int tparts = build_parts((size_t)n_walks);
+    std::vector<TileCount> tcount(tparts);
+    auto count_range = [&](int part, size_t w_lo, size_t w_hi) {
+        TileCount& T = tcount[part];
+        LaunchKey prev{-1, 0, 0, 0};
+        size_t* cur = nullptr;
+        std::pair<uint32_t, uint32_t>* rows = nullptr;
+        for (size_t w = w_lo; w < w_hi; ++w) {
+            const DevWalk& W = dwalks[w];
+            const LaunchKey key = walk_key(W);
+            if (!cur || key < prev || prev < key) {
+                cur = &T.tiles[key];
+                rows = &T.rows.emplace(key, std::make_pair(1u, 1u)).first->second;
+                prev = key;
+            }
+            const DevProgram& G = dprogs[W.prog];
+            rows->first = std::max(rows->first, std::max(G.n_regs, G.dn_regs));
+            rows->second = std::max(rows->second, G.n_consts);
+            const uint64_t nb = (W.K + 31) / 32, nc = n_chunks_of(W);
+            *cur += nb * nc;
+            T.groups += nb;
+            if (nc > 1) T.slots += nb * nc;
         }
-        // chunk boundaries; a checkpoint always ends a chunk
-        ranges.clear();
-        auto split = [&](uint64_t a, uint64_t b) {
-            const uint64_t len = b - a;
-            const uint64_t nc = std::max<uint64_t>(1, (len + chunk - 1) / chunk);
-            for (uint64_t c = 0; c < nc; ++c)
-                ranges.emplace_back(a + len * c / nc, a + len * (c + 1) / nc);
-        };
-        if (W.depth == 0) ranges.emplace_back(0, 0);
-        else if (W.checkpoint) { split(0, W.checkpoint); split(W.checkpoint, W.depth); }
-        else split(0, W.depth);
-        uint32_t cp_chunks = 0;
-        if (W.checkpoint)
-            for (auto& r : ranges) cp_chunks += r.second <= W.checkpoint;
-        for (uint32_t p0 = 0; p0 < W.K; p0 += 32) {
-            DevGroup g{};
-            g.walk = (uint32_t)w;
-            g.prime0 = p0;
-            g.nprimes = std::min<uint32_t>(32, W.K - p0);
-            g.n_chunks = (uint32_t)ranges.size();
-            g.cp_chunks = cp_chunks;
-            g.slot0 = g.n_chunks > 1 ? slots : 0;
-            g.state = kNoState;
-            g.flags = 0;
-            if (g.n_chunks > 1) slots += g.n_chunks;
-            const uint32_t gi = (uint32_t)groups.size();
-            groups.push_back(g);
-            for (uint32_t c = 0; c < g.n_chunks; ++c) {
-                DevTile t{};
-                t.walk = (uint32_t)w;
-                t.group = gi;
-                t.prime0 = p0;
-                t.nprimes = g.nprimes;
-                t.chunk = c;
-                t.slot = g.slot0 + c;
-                t.s0 = ranges[c].first;
-                t.s1 = ranges[c].second;
-                vec->push_back(t);
+    };
+    if (tparts > 1) host_pool().run(tparts, (size_t)n_walks, count_range);
+    else count_range(0, 0, (size_t)n_walks);
+    std::map<LaunchKey, std::vector<DevTile>> tile_sets;
+    std::map<LaunchKey, std::pair<uint32_t, uint32_t>> key_rows;   // max registers, constants
+    uint64_t n_group_total = 0, slots64 = 0;
+    {
+        std::map<LaunchKey, size_t> total;
+        for (const TileCount& T : tcount)
+            for (const auto& kv : T.rows) {
+                auto& r = key_rows.emplace(kv.first, std::make_pair(1u, 1u)).first->second;
+                r.first = std::max(r.first, kv.second.first);
+                r.second = std::max(r.second, kv.second.second);
+            }
+        for (TileCount& T : tcount) {
+            for (auto& kv : T.tiles) {
+                const size_t c = kv.second;
+                kv.second = total[kv.first];
+                total[kv.first] += c;
+            }
+            const uint64_t g = T.groups, sl = T.slots;
+            T.groups = n_group_total;
+            T.slots = slots64;
+            n_group_total += g;
+            slots64 += sl;
+        }
+        for (const auto& kv : total) tile_sets[kv.first].resize(kv.second);
+    }
+    if (slots64 > UINT32_MAX || n_group_total > UINT32_MAX) {
+        set_error("batch too large: more than 2^32 chunk slots or groups");
+        return DR_ERR_UNSUPPORTED;
+    }
+    std::vector<DevGroup> groups(n_group_total);
+    const uint32_t slots = (uint32_t)slots64;
+    auto fill_range = [&](int part, size_t w_lo, size_t w_hi) {
+        TileCount& T = tcount[part];
+        std::vector<std::pair<uint64_t, uint64_t>> ranges;
+        LaunchKey prev{-1, 0, 0, 0};
+        DevTile* out = nullptr;      // next tile of prev's set
+        size_t* cursor = nullptr;
+        uint32_t gi = (uint32_t)T.groups, slot = (uint32_t)T.slots;
+        for (size_t w = w_lo; w < w_hi; ++w) {
+            const DevWalk& W = dwalks[w];
+            const LaunchKey key = walk_key(W);
+            if (!cursor || key < prev || prev < key) {
+                // find (not operator[]) on the shared map: safe beside the other parts
+                if (cursor) *cursor = (size_t)(out - tile_sets.find(prev)->second.data());
+                cursor = &T.tiles.find(key)->second;
+                out = tile_sets.find(key)->second.data() + *cursor;
+                prev = key;
+            }
+            // chunk boundaries; a checkpoint always ends a chunk
+            ranges.clear();
+            auto split = [&](uint64_t a, uint64_t b) {
+                const uint64_t len = b - a;
+                const uint64_t nc = std::max<uint64_t>(1, (len + chunk - 1) / chunk);
+                for (uint64_t c = 0; c < nc; ++c)
+                    ranges.emplace_back(a + len * c / nc, a + len * (c + 1) / nc);
+            };
+            if (W.depth == 0) ranges.emplace_back(0, 0);
+            else if (W.checkpoint) { split(0, W.checkpoint); split(W.checkpoint, W.depth); }
+            else split(0, W.depth);
+            uint32_t cp_chunks = 0;
+            if (W.checkpoint)
+                for (auto& r : ranges) cp_chunks += r.second <= W.checkpoint;
+            for (uint32_t p0 = 0; p0 < W.K; p0 += 32) {
+                DevGroup g{};
+                g.walk = (uint32_t)w;
+                g.prime0 = p0;
+                g.nprimes = std::min<uint32_t>(32, W.K - p0);
+                g.n_chunks = (uint32_t)ranges.size();
+                g.cp_chunks = cp_chunks;
+                g.slot0 = g.n_chunks > 1 ? slot : 0;
+                g.state = kNoState;
+                g.flags = 0;
+                if (g.n_chunks > 1) slot += g.n_chunks;
+                groups[gi] = g;
+                for (uint32_t c = 0; c < g.n_chunks; ++c) {
+                    DevTile& t = *out++;
+                    t = DevTile{};
+                    t.walk = (uint32_t)w;
+                    t.group = gi;
+                    t.prime0 = p0;
+                    t.nprimes = g.nprimes;
+                    t.chunk = c;
+                    t.slot = g.slot0 + c;
+                    t.s0 = ranges[c].first;
+                    t.s1 = ranges[c].second;
+                }
+                ++gi;
             }
         }
-    }
+    };
+    if (tparts > 1) host_pool().run(tparts, (size_t)n_walks, fill_range);
+    else fill_range(0, 0, (size_t)n_walks);
+    size_t n_tiles_est = 0;
+    for (auto& kv : tile_sets) n_tiles_est += kv.second.size();
     std::vector<DevTile> tiles;
     tiles.reserve(n_tiles_est);
     for (auto& kv : tile_sets) {
@@ -528,12 +774,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         L.off = (uint32_t)tiles.size();
         L.count = (uint32_t)v.size();
         L.items = L.count;
-        uint32_t rr = 1, rc_ = 1;
-        for (const DevTile& t : v) {
-            const DevProgram& G = dprogs[dwalks[t.walk].prog];
-            rr = std::max(rr, std::max(G.n_regs, G.dn_regs));
-            rc_ = std::max(rc_, G.n_consts);
-        }
+        const uint32_t rr = key_rows[kv.first].first, rc_ = key_rows[kv.first].second;
         const uint32_t ns = (uint32_t)std::max(streams_for(L.cls, L.m), 0);
         L.rows_regs = rr;
         L.rows_consts = rc_;
@@ -548,15 +789,23 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     build_mark(3);
     // ---- shadow work lists
     std::map<LaunchKey, std::vector<uint32_t>> shadow_sets;
-    for (int32_t w = 0; w < n_walks; ++w) {
-        const DevWalk& W = dwalks[w];
-        if (W.shadow_mode == SHADOW_NONE) continue;
-        const DevProgram& G = dprogs[W.prog];
-        const Plan& P = *plans[W.prog];
-        if (W.shadow_mode == SHADOW_INTFD)
-            shadow_sets[LaunchKey{2, P.cls, P.m, (uint32_t)template_degree(P.cls, P.m, P.degree)}].push_back(w);
-        else
-            shadow_sets[LaunchKey{1, G.fcomp | ((W.flags & DR_WALK_VEC) ? 2u : 0u), G.m, 0}].push_back(w);
+    {
+        LaunchKey prev{-1, 0, 0, 0};
+        std::vector<uint32_t>* set = nullptr;   // shadow set of prev
+        for (int32_t w = 0; w < n_walks; ++w) {
+            const DevWalk& W = dwalks[w];
+            if (W.shadow_mode == SHADOW_NONE) continue;
+            const DevProgram& G = dprogs[W.prog];
+            const Plan& P = *plans[W.prog];
+            const LaunchKey key = W.shadow_mode == SHADOW_INTFD
+                ? LaunchKey{2, P.cls, P.m, (uint32_t)template_degree(P.cls, P.m, P.degree)}
+                : LaunchKey{1, G.fcomp | ((W.flags & DR_WALK_VEC) ? 2u : 0u), G.m, 0};
+            if (!set || key < prev || prev < key) {
+                set = &shadow_sets[key];
+                prev = key;
+            }
+            set->push_back((uint32_t)w);
+        }
     }
     std::vector<DevShadowSeg> shadow_list;
     std::vector<uint32_t> eval_items;

@@ -2,12 +2,17 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
+#include <condition_variable>
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <string_view>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -59,6 +64,38 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Host worker threads for batch construction.  run(parts, n, fn) splits
+// [0, n) into `parts` contiguous ranges in order and calls fn(part, lo, hi)
+// once for each, on the workers and the calling thread; it returns when all
+// are done.  One job at a time.
+class HostPool {
+  public:
+    explicit HostPool(int workers);
+    ~HostPool();
+    HostPool(const HostPool&) = delete;
+    HostPool& operator=(const HostPool&) = delete;
+    void run(int parts, size_t n, const std::function<void(int, size_t, size_t)>& fn);
+    int threads() const { return (int)threads_.size() + 1; }
+
+  private:
+    void worker();
+    void take_parts(const std::function<void(int, size_t, size_t)>* fn, int parts, size_t n);
+    std::vector<std::thread> threads_;
+    std::mutex run_mu_;
+    std::mutex mu_;
+    std::condition_variable cv_, done_cv_;
+    const std::function<void(int, size_t, size_t)>* fn_ = nullptr;
+    int parts_ = 0;
+    size_t n_ = 0;
+    std::atomic<int> next_{0};
+    int done_ = 0, active_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
+// The context's pool (created on first use).
+HostPool& host_pool();
+
 struct CrtSet {
     int K = 0, L = 0;
     DevBuf moduli, pinv, r2, ginv, Mlimbs, Mtotal;
@@ -72,7 +109,9 @@ struct Context {
     std::vector<cudaStream_t> hpool;  // high-priority streams for the FP64 shadow launches
     DevBuf primes, pinv, r2;   // DR_MAX_K-entry prime table
     std::mutex mu;
-    // plan cache keyed by program bytes (views into each Plan's own copy)
+    // plan cache keyed by program bytes (views into each Plan's own copy);
+    // plan_mu guards it and code_ids (lookups shared, inserts exclusive)
+    std::shared_mutex plan_mu;
     std::unordered_map<std::string_view, std::shared_ptr<Plan>> plan_cache;
     // interned instruction streams: programs that differ only in their
     // constants share one copy of device code in a batch

@@ -365,6 +365,32 @@ def test_autotune_keeps_results():
         assert x["p_float"] == y["p_float"]
 
 
+def test_large_batch_build_matches_small_batches():
+    """Batches of 1024 walks or more are built by several host threads whose
+    groups and chunk slots are merged in walk order; the same walks built as
+    small batches (one thread) must give identical residues and shadows."""
+    rng = random.Random(41)
+    progs = [dr.compile_pcf(w.a, w.b) for w in dr.synth.uniform_pcfs(40, seed=41, depth=10, limit_depth=10)]
+    rat = [dr.compile_pcf(w.a, w.b) for w in dr.synth.rational_pcfs(12, seed=42, depth_range=(100, 400))]
+    reqs = []
+    for i in range(2400):
+        prog = rat[i % len(rat)] if i % 5 == 0 else progs[i % len(progs)]
+        depth = rng.randrange(1, 3000)
+        cp = rng.randrange(1, depth) if depth > 2 and i % 3 == 0 else 0
+        reqs.append(pcf_request(prog, rng.randrange(-3, 4), depth, rng.choice([16, 32, 64, 96]), checkpoint=cp))
+    whole = run_walks(reqs)
+    parts = []
+    for i in range(0, len(reqs), 600):
+        parts += run_walks(reqs[i:i + 600])
+    for req, x, y in zip(reqs, whole, parts):
+        assert list(x["p_residues"]) == list(y["p_residues"])
+        assert list(x["q_residues"]) == list(y["q_residues"])
+        for k in ("p_float", "q_float", "log_scale"):
+            assert x[k] == y[k] or (math.isnan(x[k]) and math.isnan(y[k])), k
+        if req.checkpoint:
+            assert list(x["checkpoint"]["p_residues"]) == list(y["checkpoint"]["p_residues"])
+
+
 def test_vec_walk_golden(golden):
     """run_cmf_walk_vec against the reference's own output (fixture)."""
     from fractions import Fraction
