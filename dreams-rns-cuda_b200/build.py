@@ -5,6 +5,8 @@
 Each translation unit under csrc/ is compiled by nvcc in parallel into
 _build/, then linked into dreams_rns/_native/libdreams_b200.so (the CUDA
 runtime is linked statically, so the library only needs the driver).
+csrc/pack.c (request packing, CPython API) is compiled by the C compiler
+into dreams_rns/_pack.*.so.
 Rebuilds a unit when it or any header in csrc/ or include/ is newer than its
 object file.
 """
@@ -16,6 +18,7 @@ import glob
 import os
 import subprocess
 import sys
+import sysconfig
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -75,7 +78,28 @@ def build(force: bool = False, jobs: int = 0, verbose_ptxas: bool = False) -> st
             sys.stderr.write(res.stdout + res.stderr)
             raise RuntimeError("link failed")
         os.replace(LIB + ".tmp", LIB)
+    build_pack(force)
     return LIB
+
+
+PACK_SRC = os.path.join(SRC, "pack.c")
+PACK = os.path.join(HERE, "dreams_rns", "_pack" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+
+
+def build_pack(force: bool = False) -> str:
+    """The request-packing extension (plain C against the CPython API)."""
+    newest = max(os.path.getmtime(PACK_SRC), os.path.getmtime(os.path.join(REPO, "include", "dreams_b200.h")))
+    if not force and os.path.exists(PACK) and os.path.getmtime(PACK) >= newest:
+        return PACK
+    cc = os.environ.get("CC", "gcc")
+    cmd = [cc, "-O2", "-shared", "-fPIC", "-Wall", "-I", sysconfig.get_paths()["include"],
+           "-I", os.path.join(REPO, "include"), PACK_SRC, "-o", PACK + ".tmp"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("compiling pack.c failed")
+    os.replace(PACK + ".tmp", PACK)
+    return PACK
 
 
 if __name__ == "__main__":

@@ -130,87 +130,108 @@ def cmf_request(program, depth: int, K: int, shift_vals, trajectory_vals=None,
                        checkpoint=checkpoint, shadow=shadow)
 
 
+try:
+    from . import _pack as _pack_ext
+except ImportError:        # not built: _pack_py below computes the same arrays
+    _pack_ext = None
+
+
+def _pack_py(reqs: Sequence[WalkRequest]):
+    """Flat C-ABI arrays for a list of requests (the pure-Python statement of
+    csrc/pack.c, which _Packed uses when built): (n_programs, offsets, blobs,
+    desc, res_off, cp_off, axis, n_axis, n_res) with the arrays as bytearrays."""
+    n = len(reqs)
+    index: Dict[bytes, int] = {}
+    blobs: List[bytes] = []
+    flat: List[int] = []                 # 10 scalars per request
+    axis_vals: List[int] = []
+    vec_vals: List[int] = []
+    put_row, put_axis = flat.extend, axis_vals.extend
+    f_init, f_shadow, f_vec = N.DR_WALK_INIT_PCF, N.DR_WALK_SHADOW, N.DR_WALK_VEC
+    for r in reqs:
+        b = r.blob
+        j = index.get(b)
+        if j is None:
+            j = index[b] = len(blobs)
+            blobs.append(b)
+        ax = r.axis
+        for t in ax:
+            put_axis(t)
+        v = r.vec
+        if r.depth < 0:          # the reference treats a negative depth as no steps
+            r.depth = 0
+        put_row((j, r.K, r.depth, r.checkpoint, r.a0,
+                 (f_init if r.pcf_init else 0) | (f_shadow if r.shadow else 0) | (f_vec if v is not None else 0),
+                 r.q_row, r.p_row, 4 * len(ax), 0 if v is None else len(v)))
+        if v is not None:
+            vec_vals.extend(v)
+    n_programs = len(blobs)
+    offs = np.zeros(len(blobs) + 1, dtype=np.uint64)
+    np.cumsum(np.fromiter(map(len, blobs), dtype=np.uint64, count=len(blobs)), out=offs[1:])
+    blob = bytearray(b"".join(blobs) or b"\0")
+    try:
+        cols = np.fromiter(flat, dtype=np.int64, count=len(flat)).reshape(n, 10)
+    except OverflowError:
+        if any(not -2**63 <= int(r.a0) < 2**63 for r in reqs):
+            raise OverflowError("a0 outside int64") from None
+        raise
+    prog, Ks, depth, cps, a0, flags, q_row, p_row, alen, vlen = cols.T
+    if n and (Ks.min() < 1 or Ks.max() > N.DR_MAX_K):
+        raise ValueError(f"K must be in 1..{N.DR_MAX_K}")
+    if n and cps.min() < 0:
+        raise OverflowError("negative checkpoint")
+    try:
+        axis = np.array(axis_vals + vec_vals, dtype=np.int64)
+    except OverflowError:
+        raise OverflowError("axis parameter outside int64") from None
+    sizes = Ks + np.where(cps > 0, Ks, 0)
+    res_off = np.zeros(n, dtype=np.int64)
+    if n:
+        np.cumsum(sizes[:-1], out=res_off[1:])
+    desc = np.zeros(n, dtype=N.WALK_DTYPE)
+    desc["program"] = prog
+    desc["K"] = Ks
+    desc["depth"] = depth
+    desc["checkpoint"] = cps
+    desc["a0"] = a0
+    desc["flags"] = flags
+    desc["q_row"] = q_row
+    desc["p_row"] = p_row
+    a_total = int(alen.sum()) if n else 0
+    n_axis = int(axis.size)
+    voff = np.zeros(n, dtype=np.int64)
+    if n:
+        np.cumsum(vlen[:-1], out=voff[1:])
+    desc["vec_offset"] = np.where(vlen > 0, voff + a_total, 0)
+    aoff = np.zeros(n, dtype=np.int64)
+    if n:
+        np.cumsum(alen[:-1], out=aoff[1:])
+    desc["axis_offset"] = aoff
+    desc["res_offset"] = res_off
+    cp_off = np.where(cps > 0, res_off + Ks, -1)
+    desc["cp_res_offset"] = np.where(cps > 0, cp_off, 0)
+    if not axis.size:
+        axis = np.zeros(1, dtype=np.int64)
+    return (n_programs, bytearray(offs.tobytes()), blob, bytearray(desc.tobytes()),
+            bytearray(res_off.tobytes()), bytearray(cp_off.astype(np.int64).tobytes()),
+            bytearray(axis.tobytes()), n_axis, max(int(sizes.sum()) if n else 0, 1))
+
+
 class _Packed:
-    """Flat C-ABI arrays for a list of requests: one Python pass gathers each
-    request's scalars, numpy does the rest."""
+    """Flat C-ABI arrays for a list of requests: the blobs of the distinct
+    programs with their offsets, one dr_walk_desc per request, the axis
+    parameters (then state-vector entries) and the residue offsets."""
 
     def __init__(self, reqs: Sequence[WalkRequest]):
         n = len(reqs)
-        index: Dict[bytes, int] = {}
-        blobs: List[bytes] = []
-        flat: List[int] = []                 # 10 scalars per request
-        axis_vals: List[int] = []
-        vec_vals: List[int] = []
-        put_row, put_axis = flat.extend, axis_vals.extend
-        f_init, f_shadow, f_vec = N.DR_WALK_INIT_PCF, N.DR_WALK_SHADOW, N.DR_WALK_VEC
-        for r in reqs:
-            b = r.blob
-            j = index.get(b)
-            if j is None:
-                j = index[b] = len(blobs)
-                blobs.append(b)
-            ax = r.axis
-            for t in ax:
-                put_axis(t)
-            v = r.vec
-            if r.depth < 0:          # the reference treats a negative depth as no steps
-                r.depth = 0
-            put_row((j, r.K, r.depth, r.checkpoint, r.a0,
-                     (f_init if r.pcf_init else 0) | (f_shadow if r.shadow else 0) | (f_vec if v is not None else 0),
-                     r.q_row, r.p_row, 4 * len(ax), 0 if v is None else len(v)))
-            if v is not None:
-                vec_vals.extend(v)
-        self.n_programs = len(blobs)
-        offs = np.zeros(len(blobs) + 1, dtype=np.uint64)
-        np.cumsum(np.fromiter(map(len, blobs), dtype=np.uint64, count=len(blobs)), out=offs[1:])
-        self.offsets = offs
-        self.blobs = np.frombuffer(b"".join(blobs) or b"\0", dtype=np.uint8)   # read-only: passed as const
-        try:
-            cols = np.fromiter(flat, dtype=np.int64, count=len(flat)).reshape(n, 10)
-        except OverflowError:
-            if any(not -2**63 <= int(r.a0) < 2**63 for r in reqs):
-                raise OverflowError("a0 outside int64") from None
-            raise
-        prog, Ks, depth, cps, a0, flags, q_row, p_row, alen, vlen = cols.T
-        if n and (Ks.min() < 1 or Ks.max() > N.DR_MAX_K):
-            raise ValueError(f"K must be in 1..{N.DR_MAX_K}")
-        if n and cps.min() < 0:
-            raise OverflowError("negative checkpoint")
-        try:
-            axis = np.array(axis_vals + vec_vals, dtype=np.int64)
-        except OverflowError:
-            raise OverflowError("axis parameter outside int64") from None
-        sizes = Ks + np.where(cps > 0, Ks, 0)
-        res_off = np.zeros(n, dtype=np.int64)
-        if n:
-            np.cumsum(sizes[:-1], out=res_off[1:])
-        desc = np.zeros(n, dtype=N.WALK_DTYPE)
-        desc["program"] = prog
-        desc["K"] = Ks
-        desc["depth"] = depth
-        desc["checkpoint"] = cps
-        desc["a0"] = a0
-        desc["flags"] = flags
-        desc["q_row"] = q_row
-        desc["p_row"] = p_row
-        a_total = int(alen.sum()) if n else 0
-        voff = np.zeros(n, dtype=np.int64)
-        if n:
-            np.cumsum(vlen[:-1], out=voff[1:])
-        desc["vec_offset"] = np.where(vlen > 0, voff + a_total, 0)
-        aoff = np.zeros(n, dtype=np.int64)
-        if n:
-            np.cumsum(alen[:-1], out=aoff[1:])
-        desc["axis_offset"] = aoff
-        desc["res_offset"] = res_off
-        cp_off = np.where(cps > 0, res_off + Ks, -1)
-        desc["cp_res_offset"] = np.where(cps > 0, cp_off, 0)
-        self.res_off = res_off
-        self.cp_off = cp_off
-        self.desc = desc
-        self.axis = axis if axis.size else np.zeros(1, dtype=np.int64)
-        self.n_axis = int(axis.size)
-        self.n_res = max(int(sizes.sum()) if n else 0, 1)
+        packed = _pack_ext.pack(reqs) if _pack_ext is not None else _pack_py(reqs)
+        self.n_programs, off, blob, desc, res, cp, axis, self.n_axis, self.n_res = packed
+        self.offsets = np.frombuffer(off, dtype=np.uint64)
+        self.blobs = np.frombuffer(blob, dtype=np.uint8)
+        self.desc = np.frombuffer(desc, dtype=N.WALK_DTYPE)[:n]
+        self.res_off = np.frombuffer(res, dtype=np.int64)[:n]
+        self.cp_off = np.frombuffer(cp, dtype=np.int64)[:n]
+        self.axis = np.frombuffer(axis, dtype=np.int64)
         self.n = n
 
 

@@ -155,3 +155,56 @@ def test_walk_without_init_is_an_error():
             "print(rc)") % os.path.join(ROOT, "dreams-rns-cuda_b200")
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120)
     assert out.stdout.strip() == "-8", out.stderr
+
+
+def test_request_packing_extension_matches_python():
+    """The packing extension (csrc/pack.c) gives the same arrays as its
+    pure-Python statement, including the negative-depth clamp and the errors."""
+    import copy
+    from fractions import Fraction
+
+    import dreams_rns as dr
+    from dreams_rns import engine
+    if engine._pack_ext is None:
+        pytest.skip("dreams_rns._pack not built")
+    rng = random.Random(7)
+    pcfs = [dr.compile_pcf(a, b) for a, b in [("2", "n**2"), ("3*n+1", "-2*n**2"), ("n", "(n+1)/(n+2)")]]
+    cmf = dr.compile_cmf_from_dict({(0, 0): "1", (0, 1): "x", (1, 0): "y", (1, 1): "x+y"}, m=2, dim=2,
+                                   axis_names=["x", "y"])
+    reqs = []
+    for i in range(300):
+        kind = i % 4
+        if kind == 0:
+            depth = rng.randrange(-5, 900)
+            cp = rng.randrange(1, depth) if depth > 2 and i % 3 == 0 else 0
+            reqs.append(engine.pcf_request(pcfs[i % 3], rng.randrange(-9, 10), depth, rng.choice([1, 16, 32, 96]),
+                                           checkpoint=cp, shadow=i % 5 != 0))
+        elif kind == 1:
+            reqs.append(engine.cmf_request(cmf, rng.randrange(1, 600), rng.choice([8, 32]),
+                                           [Fraction(rng.randrange(-5, 6), rng.randrange(1, 4)), 2],
+                                           [1, Fraction(rng.randrange(1, 4), rng.randrange(1, 3))]))
+        elif kind == 2:
+            reqs.append(engine.vec_request(cmf, rng.randrange(1, 400), 8, [1, 1], [1, Fraction(1, 3)], 0, 1))
+        else:
+            reqs.append(engine.pcf_request(pcfs[0], 2, rng.randrange(0, 50), 64))
+    for batch in (reqs, reqs[:1], []):
+        a_reqs, b_reqs = copy.deepcopy(batch), copy.deepcopy(batch)
+        a, b = engine._pack_ext.pack(a_reqs), engine._pack_py(b_reqs)
+        assert (a[0], a[7], a[8]) == (b[0], b[7], b[8])
+        n = len(batch)
+        sizes = [8 * (a[0] + 1), None, engine.N.WALK_DTYPE.itemsize * n, 8 * n, 8 * n, 8 * max(a[7], 1)]
+        for k, (x, y) in enumerate(zip(a[1:7], b[1:7])):
+            lim = sizes[k]
+            assert bytes(x)[:lim] == bytes(y)[:lim], k
+        assert [r.depth for r in a_reqs] == [r.depth for r in b_reqs]   # negative depths clamped alike
+    bad_k = [engine.pcf_request(pcfs[0], 2, 10, 1)]
+    bad_k[0].K = 0
+    bad_a0 = [engine.pcf_request(pcfs[0], 2, 10, 1)]
+    bad_a0[0].a0 = 2 ** 70
+    bad_axis = [engine.pcf_request(pcfs[0], 2, 10, 1)]
+    bad_axis[0].axis = [(2 ** 70, 1, 1, 1)]
+    for bad, exc in ((bad_k, ValueError), (bad_a0, OverflowError), (bad_axis, OverflowError)):
+        with pytest.raises(exc):
+            engine._pack_ext.pack(copy.deepcopy(bad))
+        with pytest.raises(exc):
+            engine._pack_py(copy.deepcopy(bad))
