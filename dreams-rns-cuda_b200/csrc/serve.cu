@@ -85,6 +85,7 @@ struct Wave {
     uint32_t n_walks = 0;
     uint64_t prime_steps = 0;
     uint64_t n_tiles = 0, max_span = 0;   // walk tiles and longest shadow segment of the launch
+    double t_geom = 0, t_alloc = 0, t_launch = 0;   // host ms at the end of each launch_wave phase
     Wave() {
         for (DevBuf* b : {&up, &zero, &chunkP, &chunkSig, &res, &shadow, &mf}) b->pooled = true;
     }
@@ -96,6 +97,7 @@ struct WaveLog {
     float gpu_ms = 0;
     uint32_t n_req = 0, has_long = 0, wave = 0;
     uint64_t walk_tiles = 0, shadow_span = 0;
+    double t_geom = 0, t_alloc = 0, t_launch = 0;      // ms since dr_serve_open: launch_wave phases
 };
 
 struct Server {
@@ -116,6 +118,7 @@ struct Server {
     Clock::time_point t_open;
     std::vector<WaveLog> wlog;            // capped at kMaxWaveLog entries
     std::map<std::tuple<int, uint32_t, uint32_t, uint32_t, size_t>, int> occ_cache;
+    std::vector<void*> retired_pinned;    // outgrown pinned buffers, freed at close
     int error = DR_OK;
     std::string error_msg;
 };
@@ -147,12 +150,14 @@ cudaError_t grow(DevBuf& b, size_t n) {
     return b.alloc(std::max<size_t>(n + n / 2, 1u << 16));
 }
 
-// Grow-only pinned host buffer (cudaFreeHost waits for the whole device, so
-// growth doubles and is rare).
+// Grow-only pinned host buffer.  cudaFreeHost waits for the whole device
+// (every wave in flight), so an outgrown buffer is not freed here but kept in
+// `retired` until the server closes; growth doubles, so that costs at most
+// the final size again.
 template <class T>
-cudaError_t grow_host(T*& p, size_t& cap, size_t n) {
+cudaError_t grow_host(T*& p, size_t& cap, size_t n, std::vector<void*>& retired) {
     if (p && n <= cap) return cudaSuccess;
-    if (p) cudaFreeHost(p);
+    if (p) retired.push_back(p);
     p = nullptr;
     cap = std::max<size_t>(2 * n, (1u << 18) / sizeof(T));
     cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), sizeof(T) * cap);
@@ -385,13 +390,14 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     cudaStream_t st = W.st;
     cudaError_t e = cudaSuccess;
 #define SV(x) do { e = (x); if (e != cudaSuccess) return cuda_fail(e, #x); } while (0)
+    W.t_geom = ms_since(S, Clock::now());
     SV(cudaEventRecord(W.ev0, st));
     W.n_tiles = tiles.size();
     Packer pk;
     const size_t o_progs = pk.add(progs), o_code = pk.add(code), o_consts = pk.add(consts),
                  o_walks = pk.add(walks), o_axis = pk.add(axis), o_tiles = pk.add(tiles),
                  o_groups = pk.add(groups), o_segs = pk.add(segs), o_eval = pk.add(eval_items);
-    SV(grow_host(W.h_up, W.h_up_cap, pk.total + 16));
+    SV(grow_host(W.h_up, W.h_up_cap, pk.total + 16, S.retired_pinned));
     auto stage = [&](size_t off, const auto& v) {
         if (!v.empty()) std::memcpy(W.h_up + off, v.data(), sizeof(v[0]) * v.size());
     };
@@ -415,6 +421,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     SV(grow(W.chunkSig, 4ull * std::max<uint32_t>(slots, 1) * 32));
     SV(grow(W.res, 8ull * W.n_res));
     SV(grow(W.shadow, 8ull * 6 * std::max<uint32_t>(W.n_walks, 1)));
+    W.t_alloc = ms_since(S, Clock::now());
     WalkArgs wa{};
     wa.progs = reinterpret_cast<const DevProgram*>(at(o_progs));
     wa.code = reinterpret_cast<const uint4*>(at(o_code));
@@ -451,10 +458,11 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
             else SV(shadow_fd_dispatch(s.cls, s.m, s.D, s.grid, s.block, s.smem, st, sa, nullptr));
         }
     }
+    W.t_launch = ms_since(S, Clock::now());
     // outputs back to pinned host memory
-    SV(grow_host(W.h_res, W.h_res_cap, 2 * W.n_res));
-    SV(grow_host(W.h_sh, W.h_sh_cap, 3ull * W.n_walks));
-    SV(grow_host(W.h_st, W.h_st_cap, (size_t)W.n_walks));
+    SV(grow_host(W.h_res, W.h_res_cap, 2 * W.n_res, S.retired_pinned));
+    SV(grow_host(W.h_sh, W.h_sh_cap, 3ull * W.n_walks, S.retired_pinned));
+    SV(grow_host(W.h_st, W.h_st_cap, (size_t)W.n_walks, S.retired_pinned));
     SV(cudaMemcpyAsync(W.h_res, W.res.p, 8ull * W.n_res, cudaMemcpyDeviceToHost, st));
     SV(cudaMemcpyAsync(W.h_sh, W.shadow.p, 8ull * 3 * W.n_walks, cudaMemcpyDeviceToHost, st));
     SV(cudaMemcpyAsync(W.h_st, z_status, 4ull * W.n_walks, cudaMemcpyDeviceToHost, st));
@@ -556,11 +564,16 @@ void prewarm(Server& S) {
         for (uint32_t f = 0; f < 4; ++f) shadow_chain_dispatch(m, f, 0, 32, 0, nullptr, sa, &occ);
     cudaGetLastError();   // the instances that do not exist answered cudaErrorInvalidValue
     for (Wave& W : S.waves) {
-        grow_host(W.h_up, W.h_up_cap, 1);
-        grow_host(W.h_res, W.h_res_cap, 1);
-        grow_host(W.h_sh, W.h_sh_cap, 1);
-        grow_host(W.h_st, W.h_st_cap, 1);
-        for (DevBuf* b : {&W.up, &W.zero, &W.chunkP, &W.chunkSig, &W.res, &W.shadow, &W.mf}) grow(*b, 1);
+        // first sizes for waves of several thousand tiles and a few hundred requests
+        grow_host(W.h_up, W.h_up_cap, 1u << 20, S.retired_pinned);
+        grow_host(W.h_res, W.h_res_cap, 1u << 17, S.retired_pinned);
+        grow_host(W.h_sh, W.h_sh_cap, 1u << 13, S.retired_pinned);
+        grow_host(W.h_st, W.h_st_cap, 1u << 13, S.retired_pinned);
+        grow(W.up, 1u << 20);
+        grow(W.chunkP, 8u << 20);     // ~4000 chunk slots
+        grow(W.chunkSig, 1u << 19);
+        grow(W.mf, 16u << 20);        // ~128 interpreted shadow segments of 8192 steps
+        for (DevBuf* b : {&W.zero, &W.res, &W.shadow}) grow(*b, 1);
     }
 }
 
@@ -645,6 +658,9 @@ void loop(Server* Sp) {
                 g.t_launched = ms_since(S, Clock::now());
                 g.walk_tiles = free_wave->n_tiles;
                 g.shadow_span = free_wave->max_span;
+                g.t_geom = free_wave->t_geom;
+                g.t_alloc = free_wave->t_alloc;
+                g.t_launch = free_wave->t_launch;
             }
         }
         if (rc != DR_OK) {
@@ -824,6 +840,7 @@ int dr_serve_close(int32_t server) {
         if (W.h_sh) cudaFreeHost(W.h_sh);
         if (W.h_st) cudaFreeHost(W.h_st);
     }
+    for (void* p : S->retired_pinned) cudaFreeHost(p);
     return DR_OK;
 }
 
@@ -836,10 +853,10 @@ int dr_debug_serve_waves(int32_t server, int32_t max_waves, int32_t* n_waves, do
     const size_t n = std::min<size_t>(S->wlog.size(), (size_t)std::max(max_waves, 0));
     for (size_t i = 0; i < n; ++i) {
         const WaveLog& g = S->wlog[i];
-        double* o = rows + 9 * i;
+        double* o = rows + 12 * i;
         o[0] = g.t_sel; o[1] = g.t_launched; o[2] = g.t_harvest; o[3] = g.gpu_ms;
         o[4] = g.n_req; o[5] = g.has_long; o[6] = g.wave; o[7] = (double)g.walk_tiles;
-        o[8] = (double)g.shadow_span;
+        o[8] = (double)g.shadow_span; o[9] = g.t_geom; o[10] = g.t_alloc; o[11] = g.t_launch;
     }
     return DR_OK;
 }

@@ -110,10 +110,11 @@ class WalkServer:
     def wave_log(self) -> np.ndarray:
         """Scheduler record of the wave launches, one row each: selection, launch-issued
         and harvest times (ms after open), device ms, requests, long-request wave, wave
-        slot, walk tiles, longest shadow segment."""
+        slot, walk tiles, longest shadow segment, then the times (ms after open) at which
+        the wave's host build finished its geometry, allocation/upload and launches."""
         n = ctypes.c_int32()
         N.check(N.lib().dr_debug_serve_waves(self.handle, 0, ctypes.byref(n), None), "dr_debug_serve_waves")
-        rows = np.zeros((max(n.value, 1), 9))
+        rows = np.zeros((max(n.value, 1), 12))
         N.check(N.lib().dr_debug_serve_waves(self.handle, n.value, ctypes.byref(n), rows.ctypes.data),
                 "dr_debug_serve_waves")
         return rows[:n.value]

@@ -50,11 +50,14 @@ int dr_debug_build_phases(double *ms, int32_t n);
  * (Markstein correction, IEEE fallback).  Host buffers; b[i] > 1e10. */
 int dr_debug_rescale(const double *x, const double *b, int32_t n, double *out);
 
-/* The serving scheduler's record of its wave launches (first 65536): 9
+/* The serving scheduler's record of its wave launches (first 65536): 12
  * doubles per launch -- selection, launch issued and harvest times (ms after
  * dr_serve_open), device ms from the first upload to the last output copy,
  * requests, long-request wave (0/1), wave slot, walk tiles, longest shadow
- * segment (steps).  n_waves receives the number recorded. */
+ * segment (steps), then the times (ms after dr_serve_open) at which the
+ * wave's host build finished its tables and launch geometry, its buffer
+ * allocation and upload, and its kernel launches.  n_waves receives the
+ * number recorded. */
 int dr_debug_serve_waves(int32_t server, int32_t max_waves, int32_t *n_waves, double *rows);
 
 #ifdef __cplusplus
