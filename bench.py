@@ -253,7 +253,7 @@ def bench_cmf3(stream, torch, n_walks=16384):
             "batched_over_plain": rate / plain_rate}
 
 
-def bench_serving(seconds=3.0, rate=1000.0):
+def bench_serving(seconds=3.0, rate=1000.0, inflight=6):
     """Serving stream: Poisson arrivals drawn from the single-PCF, uniform-PCF
     and rational-PCF generators, plus 1% deep walks (deg-1 a, b, depth 10^6,
     K=512); p50/p99 request latency and prime-steps/s."""
@@ -286,7 +286,7 @@ def bench_serving(seconds=3.0, rate=1000.0):
             arrivals.append((t, kind, req))
     lat = {}
     kinds = {}
-    with WalkServer(max_inflight=6) as srv:
+    with WalkServer(max_inflight=inflight) as srv:
         t0 = time.perf_counter()
         ids = []
         for at, kind, req in arrivals:
@@ -499,6 +499,14 @@ def main():
         line["serving"] = bench_serving()
         line["p50_ms"] = line["serving"]["p50_ms"]
         line["p99_ms"] = line["serving"]["p99_ms"]
+        # the same stream at the top of the 1k-50k requests/s range (2 s each);
+        # at 50k/s the 1% deep walks alone (~2.5e11 prime-steps/s) exceed what
+        # the GPU walks, so that run is past saturation and its latency grows
+        line["serving_rates"] = {}
+        for rate in (10000.0, 50000.0):
+            r = bench_serving(seconds=2.0, rate=rate)
+            line["serving_rates"][str(int(rate))] = {k: r[k] for k in (
+                "requests", "p50_ms", "p99_ms", "p50_ms_by_kind", "p99_ms_by_kind", "prime_steps_per_s")}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(blobs, ws)
     batch.close()
