@@ -854,7 +854,7 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
         // has a whole chunk left with no checkpoint inside it; a chunk where a
         // lane rescaled outside the Markstein domain runs again exactly from
         // its saved start.  Other steps (segment ends, checkpoints) run exactly.
-        constexpr int kFdChunk = 8;
+        constexpr int kFdChunk = 32;
         uint64_t s = g.s0;
         if (LEAN) {
             for (; s < s_end; ++s) {
