@@ -452,6 +452,23 @@ def main():
                 "peak_source": "measured live: dr_bench_int_peak mix of mad.wide.u32 and add/min"}
     walk_only.close()
 
+    # ---- the step's critical path: the FP64 shadow chains, serial recurrences
+    # bound by the latency of one step.  Each shadow launch group of the
+    # benchmark batch runs alone (CUDA events); the floor is the same fast step
+    # on one warp with its step matrices computed in registers.
+    prof = batch.profile()
+    chains = [(p["ms2"] if p["kind"] == 1 else p["ms"], p) for p in prof if p["kind"] in (1, 2)]
+    chain_ms, chain_p = max(chains, key=lambda x: x[0])
+    floor = ctypes.c_double()
+    N.check(N.lib().dr_bench_chain_step(DEPTH, ctypes.byref(floor)), "chain floor")
+    chain_ns = chain_ms * 1e6 / DEPTH
+    shadow_chain = {"bound": "latency", "achieved_ns_per_step": chain_ns, "floor_ns_per_step": floor.value,
+                    "frac": floor.value / chain_ns, "chain_ms": chain_ms, "steps": DEPTH,
+                    "kernel": "k_shadow_chain<2,1>" if chain_p["kind"] == 1
+                    else f"k_shadow_intfd<1,2,{chain_p['degree']},0>",
+                    "floor_source": "dr_bench_chain_step: the same fast step on one warp, "
+                                    "step matrices computed in registers"}
+
     # ---- end to end through the public API with host buffers: one sweep()
     # call per step packs the requests, uploads descriptors and programs,
     # walks, runs CRT -> delta -> top-k on the device and copies residues,
@@ -486,6 +503,7 @@ def main():
                             "in, residues/shadows/deltas/top-k out"},
             "gpu_launches": n_launch,
             "roofline": roofline,
+            "shadow_chain": shadow_chain,
             "top1_delta": float(pipe["topk_val"][0]) if len(pipe["topk_val"]) else None}
     if dist:
         from dreams_rns.distributed import global_topk

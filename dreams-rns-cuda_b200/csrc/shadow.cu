@@ -1,4 +1,6 @@
 // Instantiations of the FP64 shadow kernels (see shadow_impl.cuh).
+#include <algorithm>
+
 #include "instances.h"
 #include "launch.h"
 #include "shadow_impl.cuh"
@@ -79,7 +81,60 @@ __global__ void k_debug_rescale(const double* x, const double* b, int n, double*
     out[i] = P[0][0];
 }
 
+// Latency floor of the m = 2 chain: one warp runs the companion fast step
+// on PCF step matrices computed in registers (b(n) cubic, a(n) linear), so
+// nothing but the step itself is on its dependency chain.
+__global__ void k_chain_floor(int steps, double* sink) {
+    const int lane = threadIdx.x & 31;
+    FChain<2> ch;
+    DevWalk W{};
+    W.flags = DR_WALK_INIT_PCF;
+    W.a0 = 1 + lane % 3;
+    ch.init(W);
+    const double b3 = -(1 + lane % 4), b1 = lane % 7 - 3, a1 = 1 + lane % 5;
+    bool out = false;
+    for (int s = 0; s < steps; s += 8) {
+#pragma unroll 2
+        for (int t = 0; t < 8; ++t) {
+            const double n = (double)(s + t + 1);
+            double c[2] = {(b3 * n * n + b1) * n + 5.0, a1 * n + 2.0};
+            ch.step_companion_fast(c, out);
+        }
+        ch.renorm();
+    }
+    sink[lane] = ch.P[0][1] + ch.sc_m + (out ? 1.0 : 0.0);
+}
+
 }  // namespace dr
+
+extern "C" int dr_bench_chain_step(int32_t steps, double* ns_per_step) {
+    using namespace dr;
+    if (steps < 8 || !ns_per_step) return DR_ERR_ARG;
+    double* d = nullptr;
+    if (cudaMalloc(&d, 32 * sizeof(double)) != cudaSuccess) return DR_ERR_NOMEM;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+        e = cudaEventRecord(e0);
+        if (e == cudaSuccess) {
+            k_chain_floor<<<1, 32>>>(steps, d);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(e1);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e == cudaSuccess) best = std::min(best, ms);
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d);
+    if (e != cudaSuccess) return DR_ERR_CUDA;
+    *ns_per_step = (double)best * 1e6 / steps;
+    return DR_OK;
+}
 
 extern "C" int dr_debug_rescale(const double* x, const double* b, int32_t n, double* out) {
     using namespace dr;

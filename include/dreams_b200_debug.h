@@ -45,6 +45,12 @@ int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t *n_laun
  * geometry, allocation and upload, final synchronisation (7 values). */
 int dr_debug_build_phases(double *ms, int32_t n);
 
+/* Latency floor of the FP64 shadow chain for m = 2: one warp runs `steps`
+ * (>= 8) companion fast steps on step matrices computed in registers, so
+ * only the step's own dependency chain is timed (best of three launches,
+ * CUDA events).  ns_per_step receives the time per step. */
+int dr_bench_chain_step(int32_t steps, double *ns_per_step);
+
 /* The FP64 shadow's rescale division on the device: out[i] = x[i] / b[i]
  * rounded to nearest through the same code path the shadow kernels use
  * (Markstein correction, IEEE fallback).  Host buffers; b[i] > 1e10. */
