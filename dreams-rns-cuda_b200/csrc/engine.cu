@@ -405,7 +405,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             for (size_t i = lo; i < hi; ++i) {
                 if (plans[i]) continue;
                 std::string err;
-                const int r = get_plan(blobs + blob_offsets[i], blob_offsets[i + 1] - blob_offsets[i], &plans[i], &err);
+                const int r = get_plan(blobs + blob_offsets[i], blob_offsets[i + 1] - blob_offsets[i],
+                                       &plans[i], &err);
                 if (r) {
                     if (perr[part].at < 0 || (int64_t)i < perr[part].at)
                         perr[part] = {(int64_t)i, r, "program " + std::to_string(i) + ": " + err};
@@ -472,7 +473,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
                     if (!P.ops.empty()) std::memcpy(&code[d.op_off], P.ops.data(), sizeof(Insn) * P.ops.size());
                     if (!P.dops.empty()) std::memcpy(&code[d.dop_off], P.dops.data(), sizeof(Insn) * P.dops.size());
                 }
-                if (!P.consts.empty()) std::memcpy(&consts[d.c_off], P.consts.data(), sizeof(int64_t) * P.consts.size());
+                if (!P.consts.empty())
+                    std::memcpy(&consts[d.c_off], P.consts.data(), sizeof(int64_t) * P.consts.size());
             }
         };
         const int parts = build_parts(n_programs);
@@ -497,32 +499,36 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             WalkAcc& acc = accs[part];
             for (size_t wi = w_lo; wi < w_hi; ++wi) {
                 const int32_t w = (int32_t)wi;
+                auto fail = [&](int code, const char* msg) { perr[part] = {(int64_t)w, code, msg}; };
                 const dr_walk_desc& W = walks[w];
-                if (W.program >= (uint32_t)n_programs) { perr[part] = {(int64_t)w, DR_ERR_ARG, "walk program index out of range"}; return; }
+                if (W.program >= (uint32_t)n_programs) { fail(DR_ERR_ARG, "walk program index out of range"); return; }
                 const DevProgram& G = dprogs[W.program];
-                if (W.K < 1 || W.K > DR_MAX_K) { perr[part] = {(int64_t)w, DR_ERR_UNSUPPORTED, "K outside 1..DR_MAX_K"}; return; }
-                if (W.q_row >= G.m || W.p_row >= G.m) { perr[part] = {(int64_t)w, DR_ERR_ARG, "p_row or q_row >= m"}; return; }
+                if (W.K < 1 || W.K > DR_MAX_K) { fail(DR_ERR_UNSUPPORTED, "K outside 1..DR_MAX_K"); return; }
+                if (W.q_row >= G.m || W.p_row >= G.m) { fail(DR_ERR_ARG, "p_row or q_row >= m"); return; }
                 if (W.flags & DR_WALK_VEC) {
                     if (W.flags & DR_WALK_INIT_PCF) {
-                        perr[part] = {(int64_t)w, DR_ERR_ARG, "a state-vector walk starts from v(0), not the PCF initial matrix"}; return;
+                        fail(DR_ERR_ARG, "a state-vector walk starts from v(0), not the PCF initial matrix"); return;
                     }
-                    if (W.checkpoint) { perr[part] = {(int64_t)w, DR_ERR_UNSUPPORTED, "state-vector walks have no checkpoint"}; return; }
+                    if (W.checkpoint) { fail(DR_ERR_UNSUPPORTED, "state-vector walks have no checkpoint"); return; }
                     if (W.vec_offset + (uint64_t)G.m * W.K + G.m > n_axis) {
-                        perr[part] = {(int64_t)w, DR_ERR_ARG, "state-vector initial values out of range of the axis parameters"}; return;
+                        fail(DR_ERR_ARG, "state-vector initial values out of range of the axis parameters"); return;
                     }
                 }
-                if (W.checkpoint && W.checkpoint >= W.depth) { perr[part] = {(int64_t)w, DR_ERR_ARG, "checkpoint must be < depth"}; return; }
-                if ((W.flags & DR_WALK_INIT_PCF) && G.m < 2) { perr[part] = {(int64_t)w, DR_ERR_ARG, "PCF initial matrix needs m >= 2"}; return; }
-                if (W.res_offset + W.K > n_res || (W.checkpoint && W.cp_res_offset + W.K > n_res)) {
-                    perr[part] = {(int64_t)w, DR_ERR_ARG, "residue output offset out of range"}; return;
+                if (W.checkpoint && W.checkpoint >= W.depth) { fail(DR_ERR_ARG, "checkpoint must be < depth"); return; }
+                if ((W.flags & DR_WALK_INIT_PCF) && G.m < 2) {
+                    fail(DR_ERR_ARG, "PCF initial matrix needs m >= 2");
+                    return;
                 }
-                if (W.axis_offset + 4ull * G.dim > n_axis) { perr[part] = {(int64_t)w, DR_ERR_ARG, "axis parameters out of range"}; return; }
-                if (W.depth > (1ull << 40)) { perr[part] = {(int64_t)w, DR_ERR_UNSUPPORTED, "depth above 2^40"}; return; }
+                if (W.res_offset + W.K > n_res || (W.checkpoint && W.cp_res_offset + W.K > n_res)) {
+                    fail(DR_ERR_ARG, "residue output offset out of range"); return;
+                }
+                if (W.axis_offset + 4ull * G.dim > n_axis) { fail(DR_ERR_ARG, "axis parameters out of range"); return; }
+                if (W.depth > (1ull << 40)) { fail(DR_ERR_UNSUPPORTED, "depth above 2^40"); return; }
                 for (uint32_t a = 0; a < G.dim; ++a) {
                     const int64_t* ax = axis + W.axis_offset + 4 * a;
                     if (ax[1] == 0 || ax[3] == 0) {
                         // the reference divides by float(sd*td) (cmf_walk.py:281): ZeroDivisionError
-                        perr[part] = {(int64_t)w, DR_ERR_ARG, "zero shift or trajectory denominator"}; return;
+                        fail(DR_ERR_ARG, "zero shift or trajectory denominator"); return;
                     }
                     const __int128 hi = (__int128)ax[0] * ax[3];
                     const __int128 st = (__int128)ax[2] * ax[1];
@@ -530,7 +536,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
                     const __int128 span = st * (__int128)(W.depth + 64);
                     if (hi > lim || hi < -lim || span > lim || span < -lim || (__int128)ax[1] * ax[3] > lim ||
                         (__int128)ax[1] * ax[3] < -lim) {
-                        perr[part] = {(int64_t)w, DR_ERR_UNSUPPORTED, "axis numerators exceed 2^62 over the walk"}; return;
+                        fail(DR_ERR_UNSUPPORTED, "axis numerators exceed 2^62 over the walk"); return;
                     }
                 }
                 DevWalk d{};
