@@ -1930,6 +1930,32 @@ int dr_autotune(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     return DR_OK;
 }
 
+int dr_debug_host_pool(int32_t parts, uint64_t n, int32_t repeats, uint64_t* index_sum, uint64_t* visits) {
+    if (parts < 1 || repeats < 0 || !index_sum || !visits || n > (1ull << 32)) return DR_ERR_ARG;
+    uint64_t sum = 0, count = 0;
+    for (int32_t r = 0; r < repeats; ++r) {
+        const int p = 1 + (int)((parts + r) % parts);          // vary the part count per job
+        std::vector<uint64_t> psum(p, 0), pcount(p, 0);
+        std::vector<uint8_t> seen(n, 0);
+        host_pool().run(p, (size_t)n, [&](int part, size_t lo, size_t hi) {
+            for (size_t i = lo; i < hi; ++i) {
+                psum[part] += i;
+                ++pcount[part];
+                seen[i] = (uint8_t)(seen[i] + 1);
+            }
+        });
+        for (int k = 0; k < p; ++k) {
+            sum += psum[k];
+            count += pcount[k];
+        }
+        for (uint64_t i = 0; i < n; ++i)
+            if (seen[i] != 1) return DR_ERR_INDEX;
+    }
+    *index_sum = sum;
+    *visits = count;
+    return DR_OK;
+}
+
 int dr_debug_build_phases(double* ms, int32_t n) {
     for (int i = 0; i < n && i < 7; ++i) ms[i] = g_build_ms[i];
     return DR_OK;

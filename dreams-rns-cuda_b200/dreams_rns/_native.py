@@ -143,6 +143,7 @@ _SIGNATURES = {
     "dr_serve_close": (ctypes.c_int, [_I32]),
     "dr_bench_int_peak": (ctypes.c_int, [_I32, _P]),
     "dr_bench_chain_step": (ctypes.c_int, [_I32, _P]),
+    "dr_debug_host_pool": (ctypes.c_int, [_I32, _U64, _I32, _P, _P]),
     "dr_debug_rescale": (ctypes.c_int, [_P, _P, _I32, _P]),
     "dr_debug_batch_timeline": (ctypes.c_int, [_I32, _I32, _P, _P]),
     "dr_debug_serve_waves": (ctypes.c_int, [_I32, _I32, _P, _P]),

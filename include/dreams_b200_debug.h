@@ -40,6 +40,13 @@ int dr_bench_int_peak(int32_t kind, double *lane_ops_per_s);
 int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t *n_launches,
                             float *spans);
 
+/* Exercises the host thread pool the batch build runs on: `repeats` jobs
+ * over [0, n) with 1..parts parts each; every index must be visited exactly
+ * once per job (else DR_ERR_INDEX).  index_sum and visits receive the
+ * totals over all jobs.  Needs no GPU. */
+int dr_debug_host_pool(int32_t parts, uint64_t n, int32_t repeats, uint64_t *index_sum,
+                       uint64_t *visits);
+
 /* Host milliseconds (cumulative from the start) at the end of each phase of
  * the last dr_batch_create: programs, walks, tiles, shadow lists, launch
  * geometry, allocation and upload, final synchronisation (7 values). */

@@ -208,3 +208,15 @@ def test_request_packing_extension_matches_python():
             engine._pack_ext.pack(copy.deepcopy(bad))
         with pytest.raises(exc):
             engine._pack_py(copy.deepcopy(bad))
+
+
+def test_host_pool_covers_every_index_once(L):
+    """The batch build's host thread pool: jobs with 1..16 contiguous parts
+    over [0, n) visit every index exactly once, job after job."""
+    L.dr_debug_host_pool.argtypes = [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_void_p,
+                                     ctypes.c_void_p]
+    for n in (0, 1, 7, 1000, 100_003):
+        s, v = ctypes.c_uint64(), ctypes.c_uint64()
+        assert L.dr_debug_host_pool(16, n, 64, ctypes.byref(s), ctypes.byref(v)) == 0
+        assert v.value == 64 * n
+        assert s.value == 64 * (n * (n - 1) // 2)
