@@ -732,7 +732,7 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
                 double X[NE];
 #pragma unroll
                 for (int e = 0; e < NE; ++e) X[e] = buf[e * 32 + lane];
-#pragma unroll 2
+#pragma unroll
                 for (int t = 0; t < CS; ++t) {
                     double Y[NE];
                     const int tn = t + 1 < CS ? t + 1 : t;
@@ -884,7 +884,7 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
                 if (__all_sync(0xffffffffu, !left || (s + kFdChunk <= s_end && !cp_in))) {
                     const FdChain<M_, NS, D> saved = st;
                     bool out = false;
-#pragma unroll 2
+#pragma unroll 8
                     for (int t = 0; t < kFdChunk; ++t) {
                         if (CLS == CLS_COMPANION) {
                             double c[M_];
