@@ -442,6 +442,30 @@ def test_vec_walks_vs_oracle():
             assert _close(r["p_float"], o["p_float"], 1e-9) and _close(r["q_float"], o["q_float"], 1e-9)
 
 
+def test_shadow_chunks_outside_the_markstein_domain_rerun_exactly():
+    """State-vector walks whose v(0) has a tiny or subnormal entry: with a
+    diagonal step matrix that entry stays far below the other, so every
+    rescale divides numbers outside the domain where the fast chunks'
+    Markstein quotient is exact; those chunks must run again with the IEEE
+    division and match the reference's numpy results bit for bit."""
+    from fractions import Fraction
+    from oracle import walk_np
+    prog = dr.compile_cmf_from_dict({(0, 0): "x", (1, 1): "x + 1"}, m=2, dim=1, axis_names=["x"])
+    blob = prog.serialize()
+    cases, reqs = [], []
+    for i in range(40):
+        v0 = [Fraction(1, 10 ** (310 if i % 2 else 300)), Fraction(1 + i % 3)]
+        depth = 100 + i
+        cases.append((depth, v0))
+        reqs.append(dr.vec_request(blob, depth, 8, [1 + i % 4], v0, 0, 1))
+    res = run_walks(reqs)
+    for (depth, v0), req, r in zip(cases, reqs, res):
+        o = walk_np.cmf_walk_vec(blob, depth, 8, [req.axis[0][0]], v0, 0, 1)
+        assert list(r["p_residues"]) == list(o["p_residues"])
+        assert r["p_float"] == o["p_float"] and r["q_float"] == o["q_float"], (depth, r["p_float"], o["p_float"])
+        assert _close(r["log_scale"], o["log_scale"], 1e-13)
+
+
 def test_device_crt_overflow_flag_matches_host_rule():
     """The pipeline's CRT-overflow status bits equal the host rule
     (runner.crt_overflowed, the reference's 1% test against the shadow) for
