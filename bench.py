@@ -445,8 +445,13 @@ def main():
     peak = ctypes.c_double()
     N.check(N.lib().dr_bench_int_peak(2, ctypes.byref(peak)), "int peak")
     achieved = ops / (walk_ms * 1e-3)
+    # DRAM bytes of one walk-only replay (its four k_walk launches): dram__bytes_read.sum +
+    # dram__bytes_write.sum from one ncu capture of this workload, averaged over its launches;
+    # the kernels read programs, descriptors and tiles once and keep the walk state on chip
+    walk_traffic = 4.571e6 if N_WALKS == 4096 else None
     roofline = {"bound": "int", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
-                "unit": "Tops/s", "frac": achieved / peak.value, "traffic": None,
+                "unit": "Tops/s", "frac": achieved / peak.value, "traffic": walk_traffic,
+                "traffic_unit": "DRAM bytes read + written per walk-only replay (ncu capture)",
                 "kernel": "k_walk (companion classes), walk-only batch, median of 5",
                 "kernel_ms": walk_ms,
                 "peak_source": "measured live: dr_bench_int_peak mix of mad.wide.u32 and add/min"}
