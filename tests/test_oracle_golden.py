@@ -45,8 +45,8 @@ def test_config1_pins(golden):
     assert w["p_residues"][:4] == [1351318807, 964958733, 777601130, 1778219253]
     assert w["q_residues"][:4] == [630692060, 1013274209, 1171650986, 1618286415]
     v = golden["verify_pcf"][0]["result"]
-    assert abs(float(v["delta_float"]) - (-0.998855)) < 1e-6   # README.md:30
-    assert v["p_bits"] == 992                                   # README.md:31
+    assert abs(float(v["delta_float"]) - (-0.998855)) < 1e-6   # reference README.md:30
+    assert v["p_bits"] == 992                                   # reference README.md:31
 
 
 @pytest.mark.parametrize("impl", ["np", "c"])
