@@ -1496,6 +1496,15 @@ int batch_run(Batch& B, cudaStream_t st) {
     return DR_OK;
 }
 
+// Waits until no work of this batch is in flight: its last run (on whatever
+// stream it was enqueued) and the engine stream, which carries its uploads.
+// Other work on the device (other batches, a server's waves) goes on.
+cudaError_t batch_idle(Batch& B) {
+    cudaError_t e = B.ev1 ? cudaEventSynchronize(B.ev1) : cudaSuccess;
+    if (e == cudaSuccess && g_ctx) e = cudaStreamSynchronize(g_ctx->stream);
+    return e;
+}
+
 int batch_read(Batch& B, uint32_t* p_res, uint32_t* q_res, uint64_t n_res, double* shadow,
                uint32_t* status) {
     Context& C = *g_ctx;
@@ -1667,7 +1676,8 @@ int dr_batch_read(int32_t batch, uint32_t* p_res, uint32_t* q_res, uint64_t n_re
     if (rc) return rc;
     Batch* B = find_batch(batch);
     if (!B) return DR_ERR_HANDLE;
-    DR_CUDA(cudaDeviceSynchronize());
+    // batch_read waits for this batch's end event (recorded on the stream it
+    // ran on); other work on the device, a server's waves included, goes on
     return batch_read(*B, p_res, q_res, n_res, shadow, status);
 }
 
@@ -1713,7 +1723,7 @@ int dr_batch_set_pipeline(int32_t batch, const dr_pipeline* pl) {
     if (pl->crt && Kmax > 1024) { set_error("device CRT supports K <= 1024"); return DR_ERR_UNSUPPORTED; }
     if (pl->delta_mode == DR_DELTA_FIXED && (!pl->lnum || !pl->lden || pl->l_limbs < 1)) return DR_ERR_ARG;
     cudaStream_t st = g_ctx->stream;
-    DR_CUDA(cudaDeviceSynchronize());
+    DR_CUDA(batch_idle(*B));
     if (B->graph) { cudaGraphExecDestroy(B->graph); B->graph = nullptr; }
     B->pipe = *pl;
     B->pipe.lnum = nullptr;
@@ -1785,7 +1795,7 @@ int dr_batch_set_bank(int32_t batch, int32_t n_consts, int32_t l_limbs, const ui
     if (!B) return DR_ERR_HANDLE;
     if (n_consts < 0 || (n_consts > 0 && (l_limbs < 1 || !num || !num_sign || !den))) return DR_ERR_ARG;
     if (n_consts > 4096 || l_limbs > 1024) { set_error("bank above 4096 constants or 1024 limbs"); return DR_ERR_UNSUPPORTED; }
-    DR_CUDA(cudaDeviceSynchronize());
+    DR_CUDA(batch_idle(*B));
     if (B->graph) { cudaGraphExecDestroy(B->graph); B->graph = nullptr; }
     B->bank_n = n_consts;
     B->bank_l = l_limbs;
@@ -1810,7 +1820,7 @@ int dr_batch_read_bank(int32_t batch, double* delta, int32_t max_values) {
         set_error("no constant bank on this batch");
         return DR_ERR_ARG;
     }
-    DR_CUDA(cudaDeviceSynchronize());
+    DR_CUDA(batch_idle(*B));
     const int64_t n = (int64_t)(B->tk_counts.empty() ? (int)B->n_walks
                                                      : std::min<int>(B->pipe.topk, (int)B->n_walks)) * B->bank_n;
     DR_CUDA(cudaMemcpy(delta, B->bank_out.p, 8ull * std::min<int64_t>(n, max_values), cudaMemcpyDeviceToHost));
@@ -1824,7 +1834,7 @@ int dr_batch_read_pipeline(int32_t batch, double* delta, int32_t* topk_idx, doub
     Batch* B = find_batch(batch);
     if (!B) return DR_ERR_HANDLE;
     if (!B->pipe_on) { set_error("no pipeline set on this batch"); return DR_ERR_ARG; }
-    DR_CUDA(cudaDeviceSynchronize());
+    DR_CUDA(batch_idle(*B));
     const uint32_t n = B->n_walks;
     std::vector<double> dl;
     if ((delta || topk_val) && B->pipe.delta_mode != DR_DELTA_NONE) {
@@ -2009,7 +2019,7 @@ int dr_batch_destroy(int32_t batch) {
         B = std::move(it->second);
         g_batches.erase(it);
     }
-    if (g_ctx) cudaDeviceSynchronize();
+    if (g_ctx) batch_idle(*B);
     return DR_OK;
 }
 
