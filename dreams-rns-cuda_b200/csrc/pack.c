@@ -41,12 +41,57 @@ static int vec_push(I64Vec* a, int64_t x) {
     return 0;
 }
 
-static PyObject *s_blob, *s_K, *s_depth, *s_checkpoint, *s_a0, *s_pcf_init, *s_shadow, *s_q_row,
-    *s_p_row, *s_axis, *s_vec;
+/* the request attributes read, in this order */
+enum { A_BLOB, A_K, A_DEPTH, A_CHECKPOINT, A_A0, A_PCF_INIT, A_SHADOW, A_Q_ROW, A_P_ROW, A_AXIS, A_VEC, A_N };
+static const char* const attr_names[A_N] = {"blob", "K", "depth", "checkpoint", "a0", "pcf_init",
+                                             "shadow", "q_row", "p_row", "axis", "vec"};
+static PyObject* names[A_N];
+
+#ifndef Py_T_OBJECT_EX
+#include <structmember.h>
+#define Py_T_OBJECT_EX T_OBJECT_EX
+#endif
+
+/* Attribute reads.  For objects of exactly one type (the type of the first
+ * request) whose attributes are __slots__ members and whose attribute lookup
+ * is the generic one, a read is the slot's pointer at its offset: the value
+ * the generic lookup returns, since a member descriptor is a data descriptor
+ * and takes precedence over anything else.  An empty slot, another type or
+ * any other kind of attribute goes through PyObject_GetAttr (which raises
+ * the AttributeError of an empty slot). */
+typedef struct {
+    PyTypeObject* type;
+    Py_ssize_t off[A_N]; /* -1: no slot read */
+} Slots;
+
+static void slots_init(Slots* s, PyTypeObject* t) {
+    s->type = t;
+    for (int k = 0; k < A_N; ++k) {
+        s->off[k] = -1;
+        if (!t || t->tp_getattro != PyObject_GenericGetAttr) continue;
+        PyObject* d = _PyType_Lookup(t, names[k]); /* borrowed */
+        if (d && Py_IS_TYPE(d, &PyMemberDescr_Type)) {
+            const PyMemberDef* m = ((PyMemberDescrObject*)d)->d_member;
+            if (m->type == Py_T_OBJECT_EX && m->offset > 0) s->off[k] = m->offset;
+        }
+    }
+}
+
+/* new reference to attribute k of o, NULL with an exception set */
+static PyObject* get_attr(const Slots* s, PyObject* o, int k) {
+    if (Py_TYPE(o) == s->type && s->off[k] > 0) {
+        PyObject* v = *(PyObject**)((char*)o + s->off[k]);
+        if (v) {
+            Py_INCREF(v);
+            return v;
+        }
+    }
+    return PyObject_GetAttr(o, names[k]);
+}
 
 /* attribute as int64; msg names the overflow (NULL: the default message) */
-static int attr_i64(PyObject* o, PyObject* name, int64_t* out, const char* msg) {
-    PyObject* v = PyObject_GetAttr(o, name);
+static int attr_i64(const Slots* s, PyObject* o, int k, int64_t* out, const char* msg) {
+    PyObject* v = get_attr(s, o, k);
     if (!v) return -1;
     int overflow = 0;
     long long x = PyLong_AsLongLongAndOverflow(v, &overflow);
@@ -60,14 +105,71 @@ static int attr_i64(PyObject* o, PyObject* name, int64_t* out, const char* msg) 
     return 0;
 }
 
-static int attr_bool(PyObject* o, PyObject* name, int* out) {
-    PyObject* v = PyObject_GetAttr(o, name);
+static int attr_bool(const Slots* s, PyObject* o, int k, int* out) {
+    PyObject* v = get_attr(s, o, k);
     if (!v) return -1;
     int t = PyObject_IsTrue(v);
     Py_DECREF(v);
     if (t < 0) return -1;
     *out = t;
     return 0;
+}
+
+/* Distinct program blobs by content, in first-seen order: an open-addressing
+ * table of bytes objects keyed by their (cached) hash, holding a reference to
+ * each distinct blob. */
+typedef struct {
+    Py_hash_t h;
+    PyObject* b;   /* NULL: empty */
+    int64_t idx;
+} BlobSlot;
+
+typedef struct {
+    BlobSlot* slot;
+    size_t mask;
+    PyObject** uniq;   /* distinct blobs, owned references */
+    Py_ssize_t n;
+} BlobSet;
+
+static int blobset_init(BlobSet* s, Py_ssize_t max_items) {
+    size_t cap = 16;
+    while (cap < 2 * (size_t)max_items) cap *= 2;
+    s->slot = (BlobSlot*)calloc(cap, sizeof(BlobSlot));
+    s->uniq = (PyObject**)malloc((max_items ? (size_t)max_items : 1) * sizeof(PyObject*));
+    s->mask = cap - 1;
+    s->n = 0;
+    if (!s->slot || !s->uniq) {
+        PyErr_NoMemory();
+        return -1;
+    }
+    return 0;
+}
+
+static void blobset_free(BlobSet* s) {
+    for (Py_ssize_t k = 0; k < s->n; ++k) Py_DECREF(s->uniq[k]);
+    free(s->slot);
+    free(s->uniq);
+}
+
+/* index of blob b (bytes), added when new; -1 with an exception set */
+static int64_t blobset_index(BlobSet* s, PyObject* b) {
+    const Py_hash_t h = PyObject_Hash(b);
+    if (h == -1 && PyErr_Occurred()) return -1;
+    const Py_ssize_t len = PyBytes_GET_SIZE(b);
+    for (size_t i = (size_t)h & s->mask;; i = (i + 1) & s->mask) {
+        BlobSlot* e = &s->slot[i];
+        if (!e->b) {
+            Py_INCREF(b);
+            e->h = h;
+            e->b = b;
+            e->idx = s->n;
+            s->uniq[s->n++] = b;
+            return e->idx;
+        }
+        if (e->h == h && (e->b == b || (PyBytes_GET_SIZE(e->b) == len &&
+                                         memcmp(PyBytes_AS_STRING(e->b), PyBytes_AS_STRING(b), (size_t)len) == 0)))
+            return e->idx;
+    }
 }
 
 /* append the ints of a sequence to a (overflow: the axis message) */
@@ -104,44 +206,32 @@ static PyObject* pack(PyObject* self, PyObject* arg) {
     if (!seq) return NULL;
     const Py_ssize_t n = PySequence_Fast_GET_SIZE(seq);
     PyObject** items = PySequence_Fast_ITEMS(seq);
-    PyObject* index = PyDict_New();          /* blob -> program index */
-    PyObject* blobs = PyList_New(0);         /* unique blobs in first-seen order */
+    BlobSet blobs = {0};
     Row* rows = (Row*)calloc(n ? (size_t)n : 1, sizeof(Row));
     I64Vec axis = {0}, vec = {0};
     PyObject* result = NULL;
-    if (!index || !blobs || !rows) {
-        if (!rows) PyErr_NoMemory();
+    Slots sl;
+    slots_init(&sl, n ? Py_TYPE(items[0]) : NULL);
+    if (!rows) {
+        PyErr_NoMemory();
         goto done;
     }
+    if (blobset_init(&blobs, n)) goto done;
     for (Py_ssize_t i = 0; i < n; ++i) {
         PyObject* r = items[i];
         Row* w = &rows[i];
-        PyObject* b = PyObject_GetAttr(r, s_blob);
+        PyObject* b = get_attr(&sl, r, A_BLOB);
         if (!b) goto done;
         if (!PyBytes_Check(b)) {
             Py_DECREF(b);
             PyErr_SetString(PyExc_TypeError, "program blob must be bytes");
             goto done;
         }
-        PyObject* j = PyDict_GetItemWithError(index, b);   /* borrowed */
-        if (j) {
-            w->prog = PyLong_AsLongLong(j);
-        } else if (PyErr_Occurred()) {
-            Py_DECREF(b);
-            goto done;
-        } else {
-            w->prog = PyList_GET_SIZE(blobs);
-            PyObject* k = PyLong_FromLongLong(w->prog);
-            if (!k || PyDict_SetItem(index, b, k) || PyList_Append(blobs, b)) {
-                Py_XDECREF(k);
-                Py_DECREF(b);
-                goto done;
-            }
-            Py_DECREF(k);
-        }
+        w->prog = blobset_index(&blobs, b);
         Py_DECREF(b);
+        if (w->prog < 0) goto done;
         /* axis: every tuple's entries, 4 per program axis */
-        PyObject* ax = PyObject_GetAttr(r, s_axis);
+        PyObject* ax = get_attr(&sl, r, A_AXIS);
         if (!ax) goto done;
         PyObject* axf = PySequence_Fast(ax, "axis must be a sequence of tuples");
         Py_DECREF(ax);
@@ -155,7 +245,7 @@ static PyObject* pack(PyObject* self, PyObject* arg) {
         Py_DECREF(axf);
         w->alen = 4 * (int64_t)n_ax;
         /* state vector */
-        PyObject* v = PyObject_GetAttr(r, s_vec);
+        PyObject* v = get_attr(&sl, r, A_VEC);
         if (!v) goto done;
         int has_vec = v != Py_None;
         if (has_vec) {
@@ -168,10 +258,10 @@ static PyObject* pack(PyObject* self, PyObject* arg) {
             Py_DECREF(v);
         }
         /* scalars; the reference treats a negative depth as no steps */
-        if (attr_i64(r, s_depth, &w->depth, NULL)) goto done;
+        if (attr_i64(&sl, r, A_DEPTH, &w->depth, NULL)) goto done;
         if (w->depth < 0) {
             PyObject* zero = PyLong_FromLong(0);
-            if (!zero || PyObject_SetAttr(r, s_depth, zero)) {
+            if (!zero || PyObject_SetAttr(r, names[A_DEPTH], zero)) {
                 Py_XDECREF(zero);
                 goto done;
             }
@@ -179,10 +269,10 @@ static PyObject* pack(PyObject* self, PyObject* arg) {
             w->depth = 0;
         }
         int pinit = 0, shadow = 0;
-        if (attr_i64(r, s_K, &w->K, NULL) || attr_i64(r, s_checkpoint, &w->checkpoint, NULL) ||
-            attr_i64(r, s_a0, &w->a0, "a0 outside int64") || attr_bool(r, s_pcf_init, &pinit) ||
-            attr_bool(r, s_shadow, &shadow) || attr_i64(r, s_q_row, &w->q_row, NULL) ||
-            attr_i64(r, s_p_row, &w->p_row, NULL))
+        if (attr_i64(&sl, r, A_K, &w->K, NULL) || attr_i64(&sl, r, A_CHECKPOINT, &w->checkpoint, NULL) ||
+            attr_i64(&sl, r, A_A0, &w->a0, "a0 outside int64") || attr_bool(&sl, r, A_PCF_INIT, &pinit) ||
+            attr_bool(&sl, r, A_SHADOW, &shadow) || attr_i64(&sl, r, A_Q_ROW, &w->q_row, NULL) ||
+            attr_i64(&sl, r, A_P_ROW, &w->p_row, NULL))
             goto done;
         w->flags = (pinit ? DR_WALK_INIT_PCF : 0) | (shadow ? DR_WALK_SHADOW : 0) | (has_vec ? DR_WALK_VEC : 0);
     }
@@ -197,9 +287,9 @@ static PyObject* pack(PyObject* self, PyObject* arg) {
             goto done;
         }
     {
-        const Py_ssize_t n_prog = PyList_GET_SIZE(blobs);
+        const Py_ssize_t n_prog = blobs.n;
         size_t blob_bytes = 0;
-        for (Py_ssize_t k = 0; k < n_prog; ++k) blob_bytes += (size_t)PyBytes_GET_SIZE(PyList_GET_ITEM(blobs, k));
+        for (Py_ssize_t k = 0; k < n_prog; ++k) blob_bytes += (size_t)PyBytes_GET_SIZE(blobs.uniq[k]);
         const size_t n_axis = axis.n + vec.n;
         PyObject* o_off = PyByteArray_FromStringAndSize(NULL, (Py_ssize_t)(8 * (n_prog + 1)));
         PyObject* o_blob = PyByteArray_FromStringAndSize(NULL, (Py_ssize_t)(blob_bytes ? blob_bytes : 1));
@@ -217,7 +307,7 @@ static PyObject* pack(PyObject* self, PyObject* arg) {
         bl[0] = 0;
         off[0] = 0;
         for (Py_ssize_t k = 0; k < n_prog; ++k) {
-            PyObject* b = PyList_GET_ITEM(blobs, k);
+            PyObject* b = blobs.uniq[k];
             const Py_ssize_t sz = PyBytes_GET_SIZE(b);
             memcpy(bl + off[k], PyBytes_AS_STRING(b), (size_t)sz);
             off[k + 1] = off[k] + (uint64_t)sz;
@@ -266,8 +356,7 @@ done:
     free(rows);
     free(axis.v);
     free(vec.v);
-    Py_XDECREF(index);
-    Py_XDECREF(blobs);
+    blobset_free(&blobs);
     Py_DECREF(seq);
     return result;
 }
@@ -280,18 +369,7 @@ static PyMethodDef methods[] = {
 static struct PyModuleDef module = {PyModuleDef_HEAD_INIT, "_pack", NULL, -1, methods, NULL, NULL, NULL, NULL};
 
 PyMODINIT_FUNC PyInit__pack(void) {
-#define INTERN(v, s) if (!(v = PyUnicode_InternFromString(s))) return NULL
-    INTERN(s_blob, "blob");
-    INTERN(s_K, "K");
-    INTERN(s_depth, "depth");
-    INTERN(s_checkpoint, "checkpoint");
-    INTERN(s_a0, "a0");
-    INTERN(s_pcf_init, "pcf_init");
-    INTERN(s_shadow, "shadow");
-    INTERN(s_q_row, "q_row");
-    INTERN(s_p_row, "p_row");
-    INTERN(s_axis, "axis");
-    INTERN(s_vec, "vec");
-#undef INTERN
+    for (int k = 0; k < A_N; ++k)
+        if (!(names[k] = PyUnicode_InternFromString(attr_names[k]))) return NULL;
     return PyModule_Create(&module);
 }

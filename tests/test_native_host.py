@@ -197,6 +197,36 @@ def test_request_packing_extension_matches_python():
             lim = sizes[k]
             assert bytes(x)[:lim] == bytes(y)[:lim], k
         assert [r.depth for r in a_reqs] == [r.depth for r in b_reqs]   # negative depths clamped alike
+    # requests of another type than the first one's (a subclass with a
+    # property over a slot), blobs equal by content but not identity: the
+    # generic attribute path and content de-duplication
+    class Req(engine.WalkRequest):
+        __slots__ = ()
+
+        @property
+        def K(self):
+            return 8
+
+        @K.setter
+        def K(self, v):
+            pass
+
+    mixed = copy.deepcopy(reqs[:40])
+    for i in range(0, 40, 3):
+        r = mixed[i]
+        mixed[i] = Req(blob=bytes(bytearray(r.blob)), K=r.K, depth=r.depth, axis=r.axis, a0=r.a0,
+                       pcf_init=r.pcf_init, q_row=r.q_row, checkpoint=r.checkpoint, shadow=r.shadow,
+                       p_row=r.p_row, vec=r.vec)
+    a_reqs, b_reqs = copy.deepcopy(mixed), copy.deepcopy(mixed)
+    a, b = engine._pack_ext.pack(a_reqs), engine._pack_py(b_reqs)
+    assert (a[0], a[7], a[8]) == (b[0], b[7], b[8])
+    for k, (x, y) in enumerate(zip(a[1:7], b[1:7])):
+        assert bytes(x) == bytes(y), k
+    unset = engine.pcf_request(pcfs[0], 2, 10, 1)
+    del unset.K                          # an empty slot raises as attribute access does
+    for f in (engine._pack_ext.pack, engine._pack_py):
+        with pytest.raises(AttributeError):
+            f([copy.deepcopy(reqs[0]), copy.copy(unset)])
     bad_k = [engine.pcf_request(pcfs[0], 2, 10, 1)]
     bad_k[0].K = 0
     bad_a0 = [engine.pcf_request(pcfs[0], 2, 10, 1)]
