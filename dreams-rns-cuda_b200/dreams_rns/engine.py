@@ -418,10 +418,13 @@ class WalkBatch:
         delta = np.zeros(max(n, 1), dtype=np.float64)
         ti = np.zeros(max(k, 1), dtype=np.int32)
         tv = np.zeros(max(k, 1), dtype=np.float64)
-        Kmax = max(r.K for r in self.reqs)
-        stride = (31 * Kmax + 31) // 32 + 2
-        limbs = np.zeros((4 * n, stride), dtype=np.uint32) if values else None
-        signs = np.zeros(4 * n, dtype=np.int32) if values else None
+        limbs = signs = None
+        stride = 0
+        if values:
+            Kmax = int(self.pk.desc["K"].max()) if n else 1
+            stride = (31 * Kmax + 31) // 32 + 2
+            limbs = np.zeros((4 * n, stride), dtype=np.uint32)
+            signs = np.zeros(4 * n, dtype=np.int32)
         N.check(N.lib().dr_batch_read_pipeline(
             self.handle, N.ptr(delta) if self.pipeline["delta"] else None,
             N.ptr(ti) if k else None, N.ptr(tv) if k else None,
