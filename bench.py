@@ -203,6 +203,53 @@ def bench_rational(stream, torch):
             "top1_delta": float(pl["topk_val"][0]) if len(pl["topk_val"]) else None}
 
 
+def bench_crt_stage(torch, n=1 << 20, reps=5):
+    """The CRT stage alone, on residues already in HBM: ``n`` values of K = 32
+    residues through dr_crt_batch_device on one stream, each call timed with
+    CUDA events around it (median of ``reps`` after two untimed calls).  The
+    residues (128 MiB) and limbs (132 MiB) together exceed L2.  Algorithmic
+    bytes per value: 4K read, 4 * ceil(31K / 32) limb bytes plus sign and
+    significant-limb count written."""
+    import ctypes
+    from dreams_rns import _native as N
+    stride = (31 * K + 31) // 32 + 2
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    # every prime of the table lies in (2^30, 2^31), so values below 2^30 are residues
+    res = torch.randint(0, 1 << 30, (n, K), dtype=torch.int32, device=dev, generator=g)
+    limbs = torch.empty((n, stride), dtype=torch.int32, device=dev)
+    sign = torch.empty(n, dtype=torch.int32, device=dev)
+    nl = torch.empty(n, dtype=torch.int32, device=dev)
+    st = torch.cuda.Stream()
+    times = []
+    with torch.cuda.stream(st):
+        for i in range(2 + reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            N.check(N.lib().dr_crt_batch_device(res.data_ptr(), K, n, None, limbs.data_ptr(), stride,
+                                                sign.data_ptr(), nl.data_ptr(),
+                                                ctypes.c_void_p(st.cuda_stream)), "dr_crt_batch_device")
+            e1.record(st)
+            e1.synchronize()
+            if i >= 2:
+                times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    per_value = 4 * K + 4 * ((31 * K + 31) // 32) + 8
+    gbs = per_value * n / (ms * 1e-3) / 1e9
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        pass
+    del res, limbs, sign, nl
+    return {"values": n, "K": K, "ms": ms, "bytes_per_value": per_value, "achieved_gbs": gbs,
+            "hbm_peak_gbs": peak, "hbm_frac": gbs / peak if peak else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)" if peak else None,
+            "kernel": "k_crt (Garner mixed radix, O(K^2) integer work per value)"}
+
+
 def bench_cmf3(stream, torch, n_walks=16384):
     """3x3 CMF sweep: 16384 (shift, direction) pairs over 64 cubic CMFs, depth
     5000, K=64, top-100 by delta against zeta(3); plus the plain path (one walk
@@ -530,6 +577,11 @@ def main():
             r = bench_serving(seconds=2.0, rate=rate)
             line["serving_rates"][str(int(rate))] = {k: r[k] for k in (
                 "requests", "p50_ms", "p99_ms", "p50_ms_by_kind", "p99_ms_by_kind", "prime_steps_per_s")}
+    if world == 1 and not args.no_extras:
+        try:
+            line["crt_stage"] = bench_crt_stage(torch)
+        except Exception as exc:  # noqa: BLE001 - report it, keep the bench line
+            line["crt_stage"] = {"error": f"{type(exc).__name__}: {exc}"}
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_reference(blobs, ws)
     batch.close()
