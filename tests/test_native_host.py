@@ -250,3 +250,33 @@ def test_host_pool_covers_every_index_once(L):
         assert L.dr_debug_host_pool(16, n, 64, ctypes.byref(s), ctypes.byref(v)) == 0
         assert v.value == 64 * n
         assert s.value == 64 * (n * (n - 1) // 2)
+
+
+def test_read_pipeline_limb_stride_from_descriptors(monkeypatch):
+    """WalkBatch.read_pipeline passes no limb buffer unless values are asked
+    for, and then a limb stride of ceil(31 Kmax / 32) + 2 with Kmax taken from
+    the packed descriptors (a stand-in library records the call; no GPU)."""
+    import dreams_rns as dr
+    from dreams_rns import engine
+    prog = dr.compile_pcf("2", "n**2")
+    reqs = [engine.pcf_request(prog, 2, 50, K, checkpoint=20) for K in (16, 96, 32)]
+    seen = {}
+
+    class Lib:
+        def dr_batch_read_pipeline(self, h, delta, ti, tv, limbs, signs, stride):
+            seen["limbs"], seen["stride"] = limbs is not None, stride
+            return 0
+
+    monkeypatch.setattr(engine.N, "lib", lambda: Lib())
+    b = object.__new__(engine.WalkBatch)
+    b.reqs, b.pk, b.handle = reqs, engine._Packed(reqs), 1
+    b.pipeline = {"topk": 2, "delta": True}
+    try:
+        out = b.read_pipeline()
+        assert seen == {"limbs": False, "stride": 0}
+        assert sorted(out) == ["delta", "topk_idx", "topk_val"]
+        out = b.read_pipeline(values=True)
+        assert seen == {"limbs": True, "stride": (31 * 96 + 31) // 32 + 2}
+        assert len(out["p"]) == len(out["cp_q"]) == 3
+    finally:
+        b.handle = 0
