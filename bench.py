@@ -30,9 +30,9 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "dreams-rns-cuda_b200")
-for _p in (ROOT, PKG):
-    if _p not in sys.path:
-        sys.path.insert(0, _p)
+# the reference package, installed unmodified from its source by
+#   pip install --no-index --no-build-isolation --no-deps --target baseline/_ref <reference>/python
+REF_DIR = os.path.join(ROOT, "baseline", "_ref")
 
 METRIC = "walk prime-steps/sec and p50/p99 request latency, bit-exact vs reference"
 N_WALKS = 4096
@@ -42,63 +42,185 @@ K = 32
 TOPK = 100
 
 
+def _use_repo_package():
+    """Make ``import dreams_rns`` load this repository's package (the B200 arm)."""
+    for p in (PKG, ROOT):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+
+
+def _standalone(name: str, filename: str):
+    """Load one pure-Python module of the package by its path, without the
+    package itself (whose ``__init__`` loads the native library)."""
+    import importlib.util
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(PKG, "dreams_rns", filename))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod          # dataclasses resolve their module by name
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _host_cores() -> int:
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except (AttributeError, OSError):
+        return max(1, os.cpu_count() or 1)
+
+
 def _compile(ab):
     import dreams_rns as dr
     return dr.compile_pcf(*ab).serialize()
 
 
 def workload(seed: int):
-    import dreams_rns as dr
-    return dr.synth.uniform_pcfs(N_WALKS, seed=seed, depth=CHECKPOINT, limit_depth=DEPTH, K=K)
+    return _standalone("_bench_synth", "synth.py").uniform_pcfs(
+        N_WALKS, seed=seed, depth=CHECKPOINT, limit_depth=DEPTH, K=K)
 
 
 def compile_all(ws):
-    with mp.get_context("spawn").Pool(min(os.cpu_count() or 4, 16)) as pool:
+    with mp.get_context("spawn").Pool(min(_host_cores(), 16)) as pool:
         return pool.map(_compile, [(w.a, w.b) for w in ws], chunksize=32)
 
 
-# ---- reference (CPU) side -----------------------------------------------------
+# ---- CPU legs: the reference's own walk, or the numpy port of it ---------------
 
-def _ref_walk(args):
-    """One workload walk through the numpy restatement of the reference
-    (oracle/walk_np), plus CRT and mpmath delta like the device step."""
-    blob, a0 = args
-    from oracle import walk_np
-    r = walk_np.pcf_walk(blob, a0, DEPTH, K, 1, checkpoints=(CHECKPOINT,))
-    c = r["checkpoints"][CHECKPOINT]
-    pr = [int(p) for p in r["primes"]]
-    vals = []
-    for res in (r["p_residues"], r["q_residues"], c["p_residues"], c["q_residues"]):
-        x, M = walk_np.crt([int(v) for v in res], pr)
-        vals.append(walk_np.centered(x, M))
-    import mpmath as mp_
-    mp_.mp.dps = 200
-    L = mp_.mpf(vals[0]) / mp_.mpf(vals[1]) if vals[1] else mp_.mpf(0)
-    return walk_np.delta_exact(vals[2], vals[3], L, 200)
+def cpu_kind() -> str:
+    """"reference" when the reference package is installed in baseline/_ref,
+    else "port" (oracle/walk_np, the numpy restatement of its runner.py)."""
+    return "reference" if os.path.isfile(os.path.join(REF_DIR, "dreams_rns", "runner.py")) else "port"
 
 
-def cpu_reference(blobs, ws, budget_s: float = 12.0):
-    """Time the numpy restatement on a bounded sample with every host core."""
-    cores = os.cpu_count() or 1
-    n = max(cores, 2)
-    sample = [(blobs[i], ws[i].a0) for i in range(n)]
-    os.environ.setdefault("OMP_NUM_THREADS", "1")
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
-    with mp.get_context("spawn").Pool(cores) as pool:
-        pool.map(_ref_walk, sample[:cores])           # warm the workers
-        t0 = time.perf_counter()
-        done = 0
+_CPU_KIND = None
+
+
+def _cpu_init(kind: str):
+    """Pool-worker set-up: ``import dreams_rns`` resolves to the installed
+    reference (kind "reference"), never to this repository's package."""
+    global _CPU_KIND
+    _CPU_KIND = kind
+    os.environ["OMP_NUM_THREADS"] = "1"
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    pkg = os.path.realpath(PKG)
+    sys.path[:] = [p for p in sys.path if os.path.realpath(p or os.curdir) != pkg]
+    if kind == "reference":
+        sys.path.insert(0, REF_DIR)
+        import dreams_rns  # noqa: F401  (the reference package)
+    else:
+        if ROOT not in sys.path:
+            sys.path.insert(0, ROOT)
+        from oracle import walk_np  # noqa: F401
+    import mpmath  # noqa: F401
+
+
+def _cpu_compile(ab):
+    """Program bytes: the reference's own compile_pcf, or (port) this
+    repository's pure-Python compiler loaded without the package."""
+    if _CPU_KIND == "reference":
+        import dreams_rns
+        return dreams_rns.compile_pcf(*ab).serialize()
+    return _standalone("_bench_compiler", "compiler.py").compile_pcf(*ab).serialize()
+
+
+def _cpu_walk(task):
+    """One workload walk on the CPU: residues at depth 8000 and 2000, CRT and
+    the exact delta of the depth-2000 convergent against the depth-8000 one.
+    The reference's run_pcf_walk has no checkpoint, so it walks twice."""
+    blob, a0 = task
+    if _CPU_KIND == "reference":
+        import dreams_rns as ref
+        prog = ref.CmfProgram.deserialize(blob)
+        cp = ref.run_pcf_walk(prog, a0, CHECKPOINT, K)
+        fin = ref.run_pcf_walk(prog, a0, DEPTH, K)
+        crt, cen, dex = ref.crt_reconstruct, ref.centered, ref.compute_dreams_delta_exact
+    else:
+        from oracle import walk_np
+        fin = walk_np.pcf_walk(blob, a0, DEPTH, K, 1, checkpoints=(CHECKPOINT,))
+        cp = fin["checkpoints"][CHECKPOINT]
+        crt, cen, dex = walk_np.crt, walk_np.centered, walk_np.delta_exact
+    res = [fin["p_residues"], fin["q_residues"], cp["p_residues"], cp["q_residues"]]
+    pr = [int(p) for p in fin["primes"]]
+    vals = [cen(*crt([int(v) for v in r], pr)) for r in res]
+    import mpmath
+    mpmath.mp.dps = 200
+    L = mpmath.mpf(vals[0]) / mpmath.mpf(vals[1]) if vals[1] else mpmath.mpf(0)
+    d = dex(vals[2], vals[3], L, 200)
+    return [[int(v) for v in r] for r in res], float(d)
+
+
+def cpu_leg(pairs, blobs=None, passes=None, budget_s=12.0, warmup=0):
+    """Run ``pairs`` = [(a, b, a0)] (one walk per host core) through the CPU
+    path in timed passes on a spawn pool over every host core: ``passes``
+    passes, or as many as ``budget_s`` allows (at least one).  Programs are
+    compiled before the timed passes (the reference's compiler for kind
+    "reference"; the given ``blobs`` for the port)."""
+    kind = cpu_kind()
+    cores = _host_cores()
+    with mp.get_context("spawn").Pool(cores, initializer=_cpu_init, initargs=(kind,)) as pool:
+        if blobs is None or kind == "reference":
+            blobs = pool.map(_cpu_compile, [(a, b) for a, b, _ in pairs], chunksize=1)
+        tasks = [(bl, a0) for bl, (_, _, a0) in zip(blobs, pairs)]
+        for _ in range(warmup):
+            pool.map(_cpu_walk, tasks, chunksize=1)
+        times, first = [], None
+        t_all = time.perf_counter()
         while True:
-            pool.map(_ref_walk, sample)
-            done += len(sample)
-            if time.perf_counter() - t0 > budget_s:
+            t0 = time.perf_counter()
+            out = pool.map(_cpu_walk, tasks, chunksize=1)
+            times.append(time.perf_counter() - t0)
+            if first is None:
+                first = out
+            if passes is not None:
+                if len(times) >= passes:
+                    break
+            elif time.perf_counter() - t_all >= budget_s:
                 break
-        dt = time.perf_counter() - t0
-    ps = done * K * DEPTH
-    return {"value": ps / dt, "unit": "prime-steps/s", "cores": cores, "kind": "port",
-            "sample": f"{done} of the workload's walks (depth 8000, checkpoint 2000, K=32) "
-                      f"through oracle/walk_np (numpy restatement of runner.py) + CRT + mpmath "
-                      f"delta, multiprocessing over {cores} cores, {dt:.1f} s"}
+    return {"kind": kind, "cores": cores, "walks": len(tasks), "pass_s": times, "outputs": first,
+            "blobs": blobs}
+
+
+def _cpu_what(kind: str) -> str:
+    if kind == "reference":
+        return ("the reference's own run_pcf_walk (twice: to depth 2000 and to 8000, it has no "
+                "checkpoint) + crt_reconstruct + centered + compute_dreams_delta_exact, installed "
+                "unmodified from its source into baseline/_ref")
+    return ("oracle/walk_np (numpy restatement of the reference's runner.py; the reference package "
+            "is not installed here) + CRT + mpmath delta")
+
+
+def cpu_baseline_entry(leg) -> dict:
+    total = sum(leg["pass_s"])
+    done = leg["walks"] * len(leg["pass_s"])
+    return {"value": done * K * DEPTH / total, "unit": "prime-steps/s", "cores": leg["cores"],
+            "kind": leg["kind"],
+            "sample": f"{done} walk runs over {len(leg['pass_s'])} passes of the workload's first "
+                      f"{leg['walks']} PCFs (one per core; depth 8000 with the depth-2000 convergent, "
+                      f"K=32) through {_cpu_what(leg['kind'])}; multiprocessing over {leg['cores']} "
+                      f"cores, {total:.1f} s"}
+
+
+def parity_vs_cpu(dev, delta, blobs, leg) -> dict:
+    """The timed batch's results for the CPU leg's walks against the CPU
+    outputs: p, q residues at both depths bit-exact, delta within 1e-9,
+    program bytes identical."""
+    bad = 0
+    for i, (res, d) in enumerate(leg["outputs"]):
+        r = dev[i]
+        c = r["checkpoint"]
+        same = (list(r["p_residues"]) == res[0] and list(r["q_residues"]) == res[1] and
+                list(c["p_residues"]) == res[2] and list(c["q_residues"]) == res[3])
+        g = float(delta[i])
+        if math.isinf(d) or math.isinf(g) or math.isnan(d) or math.isnan(g):
+            same &= (g == d) or (math.isnan(g) and math.isnan(d))
+        else:
+            same &= abs(g - d) <= 1e-9
+        bad += not same
+    prog_same = sum(bytes(a) == bytes(b) for a, b in zip(leg["blobs"], blobs))
+    return {"walks": len(leg["outputs"]), "against": leg["kind"], "mismatches": bad,
+            "programs_identical": prog_same,
+            "checked": "p, q residues at depth 8000 and 2000 bit-exact, delta(2000 vs own 8000) "
+                       "within 1e-9, program bytes"}
 
 
 # ---- clocks -------------------------------------------------------------------
@@ -145,15 +267,62 @@ class ClockSampler:
 
 # ---- roofline accounting ------------------------------------------------------
 
-def algorithmic_int_ops(info, K_, depth, m=2):
-    """Integer lane-instructions one walk needs with the difference-table
-    companion algorithm: per prime-step, D modular additions per stream
-    (add + min) and for each of the m last-column entries m wide multiply-adds,
-    2 per extra product beyond two (fold), and a Montgomery reduction (2 wide
-    multiplies + add + min)."""
-    D = max(info["degree"], 1)
-    per = 2 * m * D + m * (m + 2 * max(0, m - 2) + 4)
-    return per * K_ * depth
+def companion_op_split(D: int, m: int):
+    """Integer lane-instructions one prime-step of the difference-table
+    companion step needs, by the pipe that can execute them on B200 (ncu
+    assigns mad.wide.u32 to the ALU pipe and the low multiply to the FMA pipe,
+    profiles/int_pipes_microbench.md):
+      wide  m+1 per last-column entry: its m products and the Montgomery
+            reduction's q*p (ALU only)
+      low   1 per entry: the reduction's quotient q = t*(-p^-1) (FMA only)
+      mins  per entry the reduction's conditional subtraction and one per
+            extra product's fold, plus one per difference-table addition (ALU)
+      adds  the subtraction beside each of those mins, plus the addition
+            itself per difference-table update (either pipe)."""
+    D = max(int(D), 1)
+    wide = m * (m + 1)
+    low = m
+    mins = m * (1 + max(0, m - 2)) + m * D
+    adds = m * (1 + max(0, m - 2)) + 2 * m * D
+    return wide, low, mins, adds
+
+
+def pipe_bound(splits, peaks):
+    """Shortest time the integer pipes allow for work given as
+    [(prime_steps, (wide, low, mins, adds))]: ALU-only work at the ALU rate,
+    FMA-only work at the FMA rate, everything over both pipes together, and
+    everything at the issue rate -- whichever is slowest.  peaks: measured
+    lane-ops/s of mad.wide.u32 alone (ALU pipe), mad.lo.u32 alone (FMA pipe)
+    and add+min (both pipes, issue-bound)."""
+    alu = sum(n * (w + mi) for n, (w, lo, mi, ad) in splits)
+    fma = sum(n * lo for n, (w, lo, mi, ad) in splits)
+    tot = sum(n * (w + lo + mi + ad) for n, (w, lo, mi, ad) in splits)
+    t = {"alu": alu / peaks["alu"], "fma": fma / peaks["fma"],
+         "alu+fma": tot / (peaks["alu"] + peaks["fma"]), "issue": tot / peaks["issue"]}
+    return max(t.values()), t, tot
+
+
+def int_peaks(N):
+    import ctypes
+    out = {}
+    for name, kind in (("alu", 0), ("fma", 3), ("issue", 1)):
+        v = ctypes.c_double()
+        N.check(N.lib().dr_bench_int_peak(kind, ctypes.byref(v)), "int peak")
+        out[name] = v.value
+    return out
+
+
+def walk_roofline(splits, ms, peaks, kernel):
+    t_bound, parts, tot = pipe_bound(splits, peaks)
+    t = ms * 1e-3
+    return {"bound": "int", "achieved": tot / t / 1e12, "peak": tot / t_bound / 1e12, "unit": "Tops/s",
+            "frac": t_bound / t, "traffic": None, "kernel": kernel, "kernel_ms": ms,
+            "binding_pipe": max(parts, key=parts.get),
+            "pipe_frac": {k: v / t for k, v in parts.items()},
+            "peaks_tops": {k: v / 1e12 for k, v in peaks.items()},
+            "model": "algorithmic lane-ops of the difference-table companion step split by pipe "
+                     "(bench.companion_op_split); peak = the rate the binding pipe allows for this "
+                     "mix, from live microbenchmarks (dr_bench_int_peak kinds 0, 3, 1)"}
 
 
 # ---- further workloads (single-GPU runs) ------------------------------------
@@ -244,10 +413,65 @@ def bench_crt_stage(torch, n=1 << 20, reps=5):
     except (OSError, KeyError, ValueError):
         pass
     del res, limbs, sign, nl
+    # integer work per value of the lane kernel: K(K-1)/2 Garner steps of a
+    # modular subtraction (3) and a Montgomery product (5), the Horner limb
+    # updates (one wide multiply-add per limb, about K^2/2 * 31/32 of them)
+    # and three borrow passes of the centring over L limbs (3 each)
+    L = (31 * K + 31) // 32 + 2
+    ops = K * (K - 1) // 2 * 8 + (K * (K - 1) // 2) * 31 // 32 + 9 * L
+    issue = int_peaks(N)["issue"]
     return {"values": n, "K": K, "ms": ms, "bytes_per_value": per_value, "achieved_gbs": gbs,
             "hbm_peak_gbs": peak, "hbm_frac": gbs / peak if peak else None,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)" if peak else None,
-            "kernel": "k_crt (Garner mixed radix, O(K^2) integer work per value)"}
+            "int_roofline": {"bound": "int", "ops_per_value": ops, "achieved": ops * n / (ms * 1e-3) / 1e12,
+                             "peak": issue / 1e12, "unit": "Tops/s",
+                             "frac": ops * n / (ms * 1e-3) / issue,
+                             "peak_source": "dr_bench_int_peak kind 1 (issue-bound add+min), measured live"},
+            "kernel": "k_crt_lanes (Garner column recurrence per lane, 32 values per warp; Horner to limbs)"}
+
+
+def bench_topk_stage(torch, n=1 << 24, k=256, reps=5):
+    """Top-k by delta on HBM-resident deltas: n doubles through
+    dr_topk_device (a strided-sample threshold, one filtering pass over the
+    values, a sort of the few candidates), each call timed with CUDA events
+    (median of ``reps`` after two untimed calls).  Algorithmic bytes: the n
+    deltas read once, the k (index, value) pairs written."""
+    import ctypes
+    from dreams_rns import _native as N
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    d = torch.randn(n, dtype=torch.float64, device="cuda", generator=g) * 0.01 - 1.0
+    idx = torch.zeros(k, dtype=torch.int32, device="cuda")
+    val = torch.zeros(k, dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+    flag = ctypes.c_int32()
+    times = []
+    for i in range(2 + reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        N.check(N.lib().dr_topk_device(d.data_ptr(), n, k, idx.data_ptr(), val.data_ptr(),
+                                       ctypes.c_void_p(st.cuda_stream), ctypes.byref(flag)), "dr_topk_device")
+        e1.record(st)
+        e1.synchronize()
+        if i >= 2:
+            times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
+    # the result against torch's own sort of the same values (checker, untimed)
+    ref = torch.sort(d, descending=True, stable=True).indices[:k].to(torch.int32)
+    ok = bool(torch.equal(ref, idx))
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        pass
+    nbytes = 8 * n + 12 * k
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    del d, idx, val
+    return {"values": n, "k": k, "ms": ms, "bytes": nbytes, "achieved_gbs": gbs, "hbm_peak_gbs": peak,
+            "hbm_frac": gbs / peak if peak else None, "threshold_filter": bool(flag.value),
+            "matches_torch_sort": ok,
+            "kernel": "k_topk_filter (one pass over the deltas) + sample and candidate tile sorts"}
 
 
 def bench_cmf3(stream, torch, n_walks=16384):
@@ -273,13 +497,33 @@ def bench_cmf3(stream, torch, n_walks=16384):
     st = batch.stats()
     batch.close()
     rate = st["prime_steps"] / (ms * 1e-3)
-    plain_ms = []
-    for w in ws[:3]:
+    # the plain path: one walk per launch (a batch of one walk on the plain
+    # engine: the same per-class step code, one warp per 32-prime block over
+    # the whole depth, its FP64 shadow, CRT and delta), the sweep's first
+    # n_plain walks back to back on one stream, inputs resident
+    n_plain = 256
+    tgt = dr.runner.target_ratio(mp_.zeta(3))
+    plain = []
+    for w in ws[:n_plain]:
         b = WalkBatch([cmf_request(kb[w.program_key], w.depth, w.K, w.shifts, w.trajectory)],
                       engine=N.DR_ENGINE_PLAIN)
-        plain_ms.append(_time_batch(b, stream, torch, reps=1))
+        b.set_pipeline(delta="fixed", target=tgt)
+        plain.append(b)
+    for _ in range(2):              # direct run, then graph capture
+        for b in plain:
+            b.run(stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for b in plain:
+        b.run(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain_steps = sum(w.depth * w.K for w in ws[:n_plain])
+    for b in plain:
         b.close()
-    plain_rate = 5000 * 64 / (statistics.median(plain_ms) * 1e-3)
+    plain_rate = plain_steps / (plain_ms * 1e-3)
     # integer-pipe roofline of the walk kernels on this sweep (no shadow)
     import ctypes
     walk_only = WalkBatch([cmf_request(kb[w.program_key], w.depth, w.K, w.shifts, w.trajectory, shadow=False)
@@ -287,23 +531,25 @@ def bench_cmf3(stream, torch, n_walks=16384):
     walk_ms = _time_batch(walk_only, stream, torch, reps=5)
     walk_only.close()
     infos = {k: N.program_info(b) for k, b in kb.items()}
-    ops = sum(algorithmic_int_ops(infos[w.program_key], w.K, w.depth, m=3) for w in ws)
-    peak = ctypes.c_double()
-    N.check(N.lib().dr_bench_int_peak(2, ctypes.byref(peak)), "int peak")
-    roof = {"bound": "int", "achieved": ops / (walk_ms * 1e-3) / 1e12, "peak": peak.value / 1e12,
-            "unit": "Tops/s", "frac": ops / (walk_ms * 1e-3) / peak.value, "kernel_ms": walk_ms,
-            "classes": sorted({(i["class"], i["degree"]) for i in infos.values()})}
+    splits = [(w.K * w.depth, companion_op_split(infos[w.program_key]["degree"], 3)) for w in ws]
+    roof = walk_roofline(splits, walk_ms, int_peaks(N), "k_walk<COMPANION, 3, D>, walk-only sweep")
+    roof["classes"] = sorted({(i["class"], i["degree"]) for i in infos.values()})
     return {"walks": len(reqs), "prime_steps": st["prime_steps"], "ms": ms, "prime_steps_per_s": rate,
             "walk_roofline": roof,
             "autotuned": tuned,
             "plain_one_walk_per_launch_prime_steps_per_s": plain_rate,
+            "plain_path": {"walks": n_plain, "ms": plain_ms, "ms_per_walk": plain_ms / n_plain,
+                           "what": "batch of one walk per launch on DR_ENGINE_PLAIN (same per-class "
+                                   "step code, K/32 warps over the whole depth, FP64 shadow, CRT, "
+                                   "delta), back to back on one stream, CUDA events"},
             "batched_over_plain": rate / plain_rate}
 
 
-def bench_serving(seconds=3.0, rate=1000.0, inflight=6):
+def bench_serving(seconds=3.0, rate=1000.0, inflight=6, plain=False):
     """Serving stream: Poisson arrivals drawn from the single-PCF, uniform-PCF
     and rational-PCF generators, plus 1% deep walks (deg-1 a, b, depth 10^6,
-    K=512); p50/p99 request latency and prime-steps/s."""
+    K=512); p50/p99 request latency and prime-steps/s.  ``plain`` serves the
+    same stream with one plain walk launch per request instead."""
     import random
     import numpy as np
     import dreams_rns as dr
@@ -333,6 +579,31 @@ def bench_serving(seconds=3.0, rate=1000.0, inflight=6):
             arrivals.append((t, kind, req))
     lat = {}
     kinds = {}
+    if plain:
+        # the same stream served by the plain path: one request at a time in
+        # arrival order, each one walk per launch (run_walks on the plain
+        # engine: build, walk with its shadow, read back)
+        from dreams_rns import _native as N
+        from dreams_rns.engine import run_walks
+        t0 = time.perf_counter()
+        steps = 0
+        for at, kind, req in arrivals:
+            left = at - (time.perf_counter() - t0)
+            if left > 0:
+                time.sleep(left)
+            run_walks([req], engine=N.DR_ENGINE_PLAIN)
+            lat.setdefault(kind, []).append(time.perf_counter() - t0 - at)
+            steps += req.K * req.depth
+        wall = time.perf_counter() - t0
+        allv = sorted(v for vs in lat.values() for v in vs)
+        pct = lambda v, q: v[min(len(v) - 1, int(q * len(v)))] * 1e3  # noqa: E731
+        return {"requests": len(arrivals), "arrival_rate_per_s": rate, "seconds": seconds,
+                "p50_ms": pct(allv, 0.50), "p99_ms": pct(allv, 0.99),
+                "p50_ms_by_kind": {k: pct(sorted(v), 0.5) for k, v in lat.items()},
+                "p99_ms_by_kind": {k: pct(sorted(v), 0.99) for k, v in lat.items()},
+                "prime_steps": steps, "prime_steps_per_s": steps / wall, "wall_s": wall,
+                "what": "one request at a time in arrival order, each a one-walk launch on "
+                        "DR_ENGINE_PLAIN (run_walks: build, walk + shadow, read)"}
     with WalkServer(max_inflight=inflight) as srv:
         t0 = time.perf_counter()
         ids = []
@@ -391,19 +662,37 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        # The reference's own code on the host cores; this process never
+        # imports the repository's package (its synthetic generator is loaded
+        # by path).  One step = one timed pass over a bounded sample: the
+        # workload's first PCFs, one per host core.
         ws = workload(seed=2)
-        blobs = compile_all(ws)
-        cb = cpu_reference(blobs, ws)
-        line = {"metric": METRIC, "value": cb["value"], "unit": "prime-steps/s", "impl": "reference",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": N_WALKS * K * DEPTH / cb["value"] * 1e3, "higher_is_better": True,
+        cores = _host_cores()
+        pairs = [(w.a, w.b, w.a0) for w in ws[:cores]]
+        blobs = None
+        if cpu_kind() == "port":
+            comp = _standalone("_bench_compiler", "compiler.py")
+            blobs = [comp.compile_pcf(a, b).serialize() for a, b, _ in pairs]
+        leg = cpu_leg(pairs, blobs=blobs, passes=max(args.steps, 1), warmup=args.warmup)
+        cb = cpu_baseline_entry(leg)
+        step_s = leg["pass_s"]
+        value = cb["value"]
+        line = {"metric": METRIC, "value": value, "unit": "prime-steps/s", "impl": "reference",
+                "n_gpus": args.gpus, "steps": len(step_s), "warmup": args.warmup,
+                "ms_per_step": statistics.mean(step_s) * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-                "config": config, "cpu_baseline": cb,
-                "e2e": {"value": cb["value"], "unit": "prime-steps/s", "h2d_bytes_per_step": 0,
+                "config": dict(config, step=f"one pass over a bounded sample: the workload's first "
+                                            f"{leg['walks']} PCFs, one per host core",
+                               prime_steps_per_step=leg["walks"] * K * DEPTH,
+                               prime_steps_note="the workload's prime-steps (depth 8000 x K per walk); "
+                                                "the reference walks 2000 + 8000 steps to produce them"),
+                "cpu_baseline": cb,
+                "e2e": {"value": value, "unit": "prime-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return
 
+    _use_repo_package()
     ws = workload(seed=2 + 1000 * rank)
     blobs = compile_all(ws)          # process pool before the first GPU call
 
@@ -483,25 +772,14 @@ def main():
     torch.cuda.synchronize()
     walk_ms = statistics.median(a.elapsed_time(b) for a, b in wt)
     infos = {}
-    ops = 0
     for b in blobs:
         if b not in infos:
             infos[b] = N.program_info(b)
-        ops += algorithmic_int_ops(infos[b], K, DEPTH)
+    splits = [(K * DEPTH, companion_op_split(infos[b]["degree"], 2)) for b in blobs]
     import ctypes
-    peak = ctypes.c_double()
-    N.check(N.lib().dr_bench_int_peak(2, ctypes.byref(peak)), "int peak")
-    achieved = ops / (walk_ms * 1e-3)
-    # DRAM bytes of one walk-only replay (its four k_walk launches): dram__bytes_read.sum +
-    # dram__bytes_write.sum from one ncu capture of this workload, averaged over its launches;
-    # the kernels read programs, descriptors and tiles once and keep the walk state on chip
-    walk_traffic = 4.571e6 if N_WALKS == 4096 else None
-    roofline = {"bound": "int", "achieved": achieved / 1e12, "peak": peak.value / 1e12,
-                "unit": "Tops/s", "frac": achieved / peak.value, "traffic": walk_traffic,
-                "traffic_unit": "DRAM bytes read + written per walk-only replay (ncu capture)",
-                "kernel": "k_walk (companion classes), walk-only batch, median of 5",
-                "kernel_ms": walk_ms,
-                "peak_source": "measured live: dr_bench_int_peak mix of mad.wide.u32 and add/min"}
+    peaks = int_peaks(N)
+    roofline = walk_roofline(splits, walk_ms, peaks,
+                             "k_walk<COMPANION, 2, D> (D = 1..4), walk-only batch, median of 5")
     walk_only.close()
 
     # ---- the step's critical path: the FP64 shadow chains, serial recurrences
@@ -527,10 +805,19 @@ def main():
     # shadows, statuses, deltas and the top-k back to host memory
     e2e_times = []
     n = len(reqs)
+    dr.stage_times(reset=True)
     for it in range(3):
         t0 = time.perf_counter()
         out = dr.sweep(reqs, delta="self", topk=TOPK)
         e2e_times.append(time.perf_counter() - t0)
+    stages = dr.stage_times(reset=True)
+    e2e_stages = {k[:-3]: stages[k] / 3 for k in stages if k.endswith("_ms")}
+    import numpy as np_
+    phases = np_.zeros(7)
+    N.check(N.lib().dr_debug_build_phases(N.ptr(phases), 7), "build phases")
+    e2e_stages["build_phases_cumulative"] = dict(zip(
+        ("programs", "walks", "tiles", "shadow_lists", "geometry", "alloc_upload", "sync"),
+        [round(float(v), 3) for v in phases]))
     from dreams_rns import _native as N_
     blob_bytes = sum(len(b) for b in set(blobs))
     h2d = n * N_.WALK_DTYPE.itemsize + blob_bytes + 8 * n * 4      # descriptors, programs, axes
@@ -551,6 +838,7 @@ def main():
             "clocks": clocks,
             "e2e": {"value": e2e_val, "unit": "prime-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "seconds_per_step": e2e_s,
+                    "stage_ms_per_call": e2e_stages,
                     "path": "dreams_rns.sweep(requests, delta='self', topk=100): host descriptors "
                             "in, residues/shadows/deltas/top-k out"},
             "gpu_launches": n_launch,
@@ -569,6 +857,14 @@ def main():
         line["serving"] = bench_serving()
         line["p50_ms"] = line["serving"]["p50_ms"]
         line["p99_ms"] = line["serving"]["p99_ms"]
+        # the same arrivals (1 s of the 1k/s stream) through the plain path,
+        # and the continuous-batching server on that same second
+        pl = bench_serving(seconds=1.0, plain=True)
+        cb = bench_serving(seconds=1.0)
+        line["serving_vs_plain"] = {"plain": pl, "batched": {k: cb[k] for k in (
+            "requests", "p50_ms", "p99_ms", "prime_steps_per_s", "wall_s")},
+            "prime_steps_per_s_ratio": cb["prime_steps_per_s"] / pl["prime_steps_per_s"],
+            "p99_ratio": pl["p99_ms"] / cb["p99_ms"]}
         # the same stream at the top of the 1k-50k requests/s range (2 s each);
         # at 50k/s the 1% deep walks alone (~2.5e11 prime-steps/s) exceed what
         # the GPU walks, so that run is past saturation and its latency grows
@@ -582,8 +878,17 @@ def main():
             line["crt_stage"] = bench_crt_stage(torch)
         except Exception as exc:  # noqa: BLE001 - report it, keep the bench line
             line["crt_stage"] = {"error": f"{type(exc).__name__}: {exc}"}
-    if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference(blobs, ws)
+        try:
+            line["topk_stage"] = bench_topk_stage(torch)
+        except Exception as exc:  # noqa: BLE001 - report it, keep the bench line
+            line["topk_stage"] = {"error": f"{type(exc).__name__}: {exc}"}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the CPU path on the workload's first PCFs, one per host core; its
+        # outputs also check the timed batch's results for those walks
+        cores = _host_cores()
+        leg = cpu_leg([(w.a, w.b, w.a0) for w in ws[:cores]], blobs=blobs[:cores])
+        line["cpu_baseline"] = cpu_baseline_entry(leg)
+        line["parity_checked"] = parity_vs_cpu(batch.read()[:cores], pipe["delta"], blobs, leg)
     batch.close()
     if rank == 0:
         print(json.dumps(line), flush=True)

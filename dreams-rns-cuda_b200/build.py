@@ -1,10 +1,14 @@
 """Build libdreams_b200.so (sm_100a) in-tree.
 
-    python dreams-rns-cuda_b200/build.py [--force] [--jobs N]
+    python dreams-rns-cuda_b200/build.py [--force] [--jobs N] [--debug]
 
 Each translation unit under csrc/ is compiled by nvcc in parallel into
 _build/, then linked into dreams_rns/_native/libdreams_b200.so (the CUDA
 runtime is linked statically, so the library only needs the driver).
+--debug builds the same sources with -DDR_DEBUG (device bounds checks on
+every table index a walk tile uses; see csrc/debug_check.cuh) into
+_build_debug/ and dreams_rns/_native/libdreams_b200_debug.so, which the
+package loads instead when DREAMS_B200_DEBUG=1.
 csrc/pack.c (request packing, CPython API) is compiled by the C compiler
 into dreams_rns/_pack.*.so.
 Rebuilds a unit when it or any header in csrc/ or include/ is newer than its
@@ -24,9 +28,11 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
-OBJ = os.path.join(HERE, "_build")
 OUT_DIR = os.path.join(HERE, "dreams_rns", "_native")
+OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libdreams_b200.so")
+OBJ_DEBUG = os.path.join(HERE, "_build_debug")
+LIB_DEBUG = os.path.join(OUT_DIR, "libdreams_b200_debug.so")
 
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -43,12 +49,12 @@ def _units():
     return sorted(glob.glob(os.path.join(SRC, "*.cu")) + glob.glob(os.path.join(SRC, "*.cpp")))
 
 
-def _compile(src: str, force: bool, verbose_ptxas: bool) -> str:
-    obj = os.path.join(OBJ, os.path.basename(src) + ".o")
+def _compile(src: str, force: bool, verbose_ptxas: bool, obj_dir: str, defines) -> str:
+    obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
     newest = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in _headers()])
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= newest:
         return obj
-    cmd = [NVCC] + ARCH + COMMON
+    cmd = [NVCC] + ARCH + COMMON + list(defines)
     if verbose_ptxas and src.endswith(".cu"):
         cmd += ["-Xptxas", "-v"]
     cmd += ["-c", src, "-o", obj + ".tmp"]
@@ -63,23 +69,28 @@ def _compile(src: str, force: bool, verbose_ptxas: bool) -> str:
     return obj
 
 
-def build(force: bool = False, jobs: int = 0, verbose_ptxas: bool = False) -> str:
-    os.makedirs(OBJ, exist_ok=True)
+def build(force: bool = False, jobs: int = 0, verbose_ptxas: bool = False, debug: bool = False) -> str:
+    obj_dir, lib = (OBJ_DEBUG, LIB_DEBUG) if debug else (OBJ, LIB)
+    defines = ["-DDR_DEBUG=1"] if debug else []
+    os.makedirs(obj_dir, exist_ok=True)
     os.makedirs(OUT_DIR, exist_ok=True)
     units = _units()
     jobs = jobs or min(len(units), os.cpu_count() or 4)
     with ThreadPoolExecutor(max_workers=jobs) as ex:
-        objs = list(ex.map(lambda s: _compile(s, force, verbose_ptxas), units))
-    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        objs = list(ex.map(lambda s: _compile(s, force, verbose_ptxas, obj_dir, defines), units))
+    stale = [o for o in glob.glob(os.path.join(obj_dir, "*.o")) if o not in objs]
+    for o in stale:          # objects of removed sources must not be linked
+        os.remove(o)
+    if force or not os.path.exists(lib) or os.path.getmtime(lib) < max(os.path.getmtime(o) for o in objs):
         cmd = [NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-cudart", "static",
-                               "-o", LIB + ".tmp"] + objs + ["-lpthread"]
+                               "-o", lib + ".tmp"] + objs + ["-lpthread"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
             raise RuntimeError("link failed")
-        os.replace(LIB + ".tmp", LIB)
+        os.replace(lib + ".tmp", lib)
     build_pack(force)
-    return LIB
+    return lib
 
 
 PACK_SRC = os.path.join(SRC, "pack.c")
@@ -107,5 +118,6 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--jobs", type=int, default=0)
     ap.add_argument("--ptxas", action="store_true", help="keep -Xptxas -v reports next to objects")
+    ap.add_argument("--debug", action="store_true", help="DR_DEBUG build (device bounds checks)")
     a = ap.parse_args()
-    print(build(a.force, a.jobs, a.ptxas))
+    print(build(a.force, a.jobs, a.ptxas, a.debug))

@@ -1,5 +1,6 @@
 // Host-only ABI entry points: errors, prime table, program inspection, and
 // the CPU re-statement hook used by the tests.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -40,6 +41,31 @@ const std::vector<uint32_t>& prime_table(int K) {
         }
     }
     return g_primes;
+}
+
+namespace {
+std::atomic<uint64_t> g_stage_ns[STAGE_COUNT];
+std::atomic<uint64_t> g_stage_calls[STAGE_COUNT];
+}  // namespace
+
+void stage_add(int stage, double ms) {
+    if (stage < 0 || stage >= STAGE_COUNT || !(ms >= 0.0)) return;
+    g_stage_ns[stage].fetch_add((uint64_t)(ms * 1e6), std::memory_order_relaxed);
+    g_stage_calls[stage].fetch_add(1, std::memory_order_relaxed);
+}
+
+int prime_table_copy(int K, uint32_t* out) {
+    std::lock_guard<std::mutex> lk(g_prime_mu);
+    if ((int)g_primes.size() < K) {
+        uint32_t c = g_primes.empty() ? 0x7fffffffu : g_primes.back() - 2;
+        while ((int)g_primes.size() < K && c >= (1u << 30)) {
+            if (is_prime_u32(c)) g_primes.push_back(c);
+            c -= 2;
+        }
+    }
+    if ((int)g_primes.size() < K) return DR_ERR_UNSUPPORTED;
+    if (K > 0) std::memcpy(out, g_primes.data(), sizeof(uint32_t) * (size_t)K);
+    return DR_OK;
 }
 
 PrimeMeta prime_meta(uint32_t p) {
@@ -85,15 +111,28 @@ const char* dr_last_error(void) { return dr::last_error().c_str(); }
 
 int dr_version(void) { return 10000; }
 
+int dr_stage_times(double* ms_out, uint64_t* calls_out, int32_t n, int32_t reset) {
+    if (n < 0 || (n > 0 && !ms_out)) {
+        dr::set_error("dr_stage_times: null output or negative count");
+        return DR_ERR_ARG;
+    }
+    for (int s = 0; s < dr::STAGE_COUNT; ++s) {
+        const uint64_t ns = reset ? dr::g_stage_ns[s].exchange(0) : dr::g_stage_ns[s].load();
+        const uint64_t c = reset ? dr::g_stage_calls[s].exchange(0) : dr::g_stage_calls[s].load();
+        if (s < n) {
+            ms_out[s] = (double)ns * 1e-6;
+            if (calls_out) calls_out[s] = c;
+        }
+    }
+    return DR_OK;
+}
+
 int dr_prime_table(int K, uint32_t* out) {
     if (K < 0 || K > DR_MAX_K || (K > 0 && !out)) {
         dr::set_error("dr_prime_table: K outside 0..DR_MAX_K");
         return DR_ERR_ARG;
     }
-    const auto& t = dr::prime_table(K);
-    if ((int)t.size() < K) return DR_ERR_UNSUPPORTED;
-    std::memcpy(out, t.data(), sizeof(uint32_t) * (size_t)K);
-    return DR_OK;
+    return dr::prime_table_copy(K, out);
 }
 
 int dr_program_info(const uint8_t* blob, uint64_t size, int32_t* cls_out, int32_t* degree_out,
@@ -127,8 +166,9 @@ int dr_debug_sim_walk(const uint8_t* blob, uint64_t size, int32_t K, uint64_t de
         return rc;
     }
     if (force_interp) plan.cls = dr::CLS_INTERP;
-    if (q_row >= plan.m) return DR_ERR_ARG;
-    const auto& primes = dr::prime_table(K);
+    if (q_row >= plan.m || K < 0 || K > DR_MAX_K || (K > 0 && (!p_out || !q_out))) return DR_ERR_ARG;
+    std::vector<uint32_t> primes((size_t)K);
+    if ((rc = dr::prime_table_copy(K, primes.data())) != DR_OK) return rc;
     for (int k = 0; k < K; ++k) {
         uint64_t o[4];
         dr::sim_walk_prime(plan, primes[k], depth, checkpoint, axis_params, pcf_init, a0, q_row,

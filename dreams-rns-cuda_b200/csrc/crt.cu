@@ -3,7 +3,10 @@
 // The reference's iterative CRT adds one mixed-radix digit per modulus:
 //     t_i = (a_i - x mod p_i) * inv(M_i mod p_i) mod p_i,  x += M_i t_i,
 // with M_i = p_0 ... p_{i-1}, x starting at the raw first residue and
-// inv(v) = v^(p-2) mod p (0 when p | M_i).  One warp handles one value:
+// inv(v) = v^(p-2) mod p (0 when p | M_i).  Two kernels compute it.  For the
+// standard prime table and K <= kCrtLanesMaxK, k_crt_lanes runs each value's
+// whole reconstruction on one lane (32 values per warp; see there).  For any
+// other odd moduli, and larger K, k_crt gives one warp to one value:
 //   1. digits: for i = 1..K-1 the lane owning modulus i computes t_i and
 //      broadcasts it; every lane folds t_i into the running x mod p_j of its
 //      own moduli j > i -- K sequential steps, K/32 mulmods each per lane;
@@ -13,6 +16,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -38,7 +42,7 @@ __device__ __forceinline__ Mont mont_of(uint32_t p, uint32_t pinv, uint32_t r2) 
 // Thread j handles modulus j; thread 0 builds the limb table.  Setup work,
 // run once per moduli set and cached by the host.
 __global__ void k_crt_setup(const uint32_t* moduli, int K, int L, uint32_t* pinv, uint32_t* r2,
-                            uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal) {
+                            uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal, uint32_t* garner) {
     for (int j = threadIdx.x; j < K; j += blockDim.x) {
         const uint32_t p = moduli[j];
         uint32_t x = p;
@@ -50,7 +54,12 @@ __global__ void k_crt_setup(const uint32_t* moduli, int K, int L, uint32_t* pinv
         r2[j] = rr;
         const Mont M = mont_of(p, pi, rr);
         uint32_t acc = M.one;  // prod_{i<j} p_i mod p_j
-        for (int i = 0; i < j; ++i) acc = mmul(acc, mmul(moduli[i] % p, rr, M), M);
+        for (int i = 0; i < j; ++i) {
+            const uint32_t pim = mmul(moduli[i] % p, rr, M);
+            acc = mmul(acc, pim, M);
+            // Garner constant of the lane kernel: p_i^-1 mod p_j, Montgomery form
+            if (garner) garner[(size_t)i * K + j] = minv_any(pim, M);
+        }
         ginv[j] = minv_any(acc, M);
     }
     if (threadIdx.x == 0) {
@@ -214,10 +223,169 @@ __global__ void __launch_bounds__(128) k_crt(const uint32_t* __restrict__ residu
     }
 }
 
+// ---- lane-per-value kernel (standard primes) -------------------------------
+// One lane carries one value through the whole reconstruction; a warp takes
+// 32 values, so every instruction does 32 values' work (the warp-per-value
+// kernel above spends a sequential K-step broadcast chain per value).  For
+// distinct primes above 2^30 the reference's digits
+//     t_k = (a_k - x mod p_k) * inv(M_k mod p_k)  (runner.py:70-74)
+// equal Garner's column recurrence
+//     d = a_k;  d = (d - t_i mod p_k) * p_i^-1 mod p_k  for i = 0 .. k-1
+// (inverses exist and multiply, so inv(M_k) = prod p_i^-1), with t_0 the raw
+// first residue as the reference starts from it.  Then x = t_0 + p_0 (t_1 +
+// p_1 (t_2 + ...)) by Horner in 32-bit limbs, and the centring of
+// runner.py:79-81.  Per warp, shared memory holds the digits [k][lane] and
+// the limbs [l][lane] in rows of 33 words, so both the lane-parallel compute
+// (lanes differ in the column) and the coalesced load/store of one value's
+// row (lanes differ in the row) are free of bank conflicts.
+constexpr int kCrtPitch = 33;
+
+__host__ __device__ inline size_t crt_lanes_warp_words(int K, int L) {
+    return (size_t)kCrtPitch * ((K > L ? K : L) + L);
+}
+
+__global__ void __launch_bounds__(128) k_crt_lanes(const uint32_t* __restrict__ residues, int n,
+                                                   CrtTables T, uint32_t* __restrict__ limbs,
+                                                   int stride, int32_t* __restrict__ sign_out,
+                                                   int32_t* __restrict__ nlimbs_out,
+                                                   uint32_t* __restrict__ ulimbs,
+                                                   const uint64_t* __restrict__ in_off,
+                                                   const uint32_t* __restrict__ out_idx) {
+    extern __shared__ uint32_t csm[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    const int K = T.K, L = T.L;
+    uint32_t* sp = csm;            // moduli
+    uint32_t* spi = sp + K;        // -p^-1 mod 2^32
+    for (int j = threadIdx.x; j < K; j += blockDim.x) {
+        sp[j] = T.moduli[j];
+        spi[j] = T.pinv[j];
+    }
+    __syncthreads();
+    uint32_t* D = csm + 2 * K + (size_t)warp * crt_lanes_warp_words(K, L);   // digits, then M - x
+    uint32_t* X = D + (size_t)kCrtPitch * (K > L ? K : L);                   // limbs of x
+    const int groups = (n + 31) / 32;
+    for (int g = blockIdx.x * wpb + warp; g < groups; g += gridDim.x * wpb) {
+        const int j0 = g * 32;
+        const int cnt = min(32, n - j0);
+        // residues of the warp's values, one value's row at a time (coalesced)
+        for (int v = 0; v < cnt; ++v) {
+            const uint32_t* a = residues + (in_off ? in_off[j0 + v] : (uint64_t)(j0 + v) * K);
+            for (int k = lane; k < K; k += 32) D[k * kCrtPitch + v] = __ldg(a + k);
+        }
+        __syncwarp();
+        // digits, column by column: digit k needs the final digits i < k
+        const uint32_t t0 = D[lane];                 // raw, as the reference starts from it
+        for (int k = 1; k < K; ++k) {
+            const uint32_t p = sp[k];
+            const Mont M{p, spi[k], 0u, 0u};
+            uint32_t d = D[k * kCrtPitch + lane];
+            d = umin32(d, d - 2u * p);               // a_k < 2^32 < 4p: reduce mod p
+            d = umin32(d, d - p);
+            uint32_t t = umin32(t0, t0 - 2u * p);    // t_0 < 2^32: t_0 mod p
+            t = umin32(t, t - p);
+            d = mmul(subm(d, t, p), __ldg(T.garner + k), M);              // row i = 0
+            for (int i = 1; i < k; ++i) {
+                const uint32_t ti = D[i * kCrtPitch + lane];              // < p_i < 2p
+                d = mmul(subm(d, umin32(ti, ti - p), p), __ldg(T.garner + (size_t)i * K + k), M);
+            }
+            D[k * kCrtPitch + lane] = d;
+        }
+        // x = t_0 + p_0 (t_1 + p_1 (t_2 + ...)): Horner from the top digit;
+        // the limb count grows when some lane's carry needs a new limb
+        int len = 1;
+        X[lane] = D[(K - 1) * kCrtPitch + lane];
+        for (int i = K - 2; i >= 0; --i) {
+            const uint32_t p = sp[i];
+            uint64_t c = D[i * kCrtPitch + lane];
+            for (int l = 0; l < len; ++l) {
+                const uint64_t t = (uint64_t)X[l * kCrtPitch + lane] * p + c;
+                X[l * kCrtPitch + lane] = (uint32_t)t;
+                c = t >> 32;
+            }
+            if (len < L && __any_sync(0xffffffffu, c != 0)) X[len++ * kCrtPitch + lane] = (uint32_t)c;
+        }
+        for (int l = len; l < L; ++l) X[l * kCrtPitch + lane] = 0u;
+        __syncwarp();
+        if (ulimbs)
+            for (int v = 0; v < cnt; ++v) {
+                uint32_t* uo = ulimbs + (size_t)(out_idx ? out_idx[j0 + v] : (uint32_t)(j0 + v)) * stride;
+                for (int l = lane; l < stride; l += 32) uo[l] = l < L ? X[l * kCrtPitch + v] : 0u;
+            }
+        // centring (runner.py:79-81): x - M if x > M // 2, else x.  d = M - x;
+        // x >= M when that borrows or is zero; otherwise 2x > M (M odd) when
+        // x > d, i.e. when x - d does not borrow
+        uint32_t bd = 0, dz = 0;
+        for (int l = 0; l < L; ++l) {
+            const uint32_t m = __ldg(T.Mtotal + l), x = X[l * kCrtPitch + lane];
+            const uint32_t s = m - x, dl = s - bd;
+            bd = (m < x) | (s < bd);
+            D[l * kCrtPitch + lane] = dl;
+            dz |= dl;
+        }
+        const bool ge = bd || dz == 0u;
+        uint32_t be = 0;
+        for (int l = 0; l < L; ++l) {
+            const uint32_t x = X[l * kCrtPitch + lane], dl = D[l * kCrtPitch + lane];
+            const uint32_t s = x - dl;
+            be = (x < dl) | (s < be);
+        }
+        const bool neg = !ge && !be;                  // 2x > M: the value is -(M - x)
+        uint32_t bm = 0;
+        int nl = 0;
+        for (int l = 0; l < L; ++l) {
+            const uint32_t x = X[l * kCrtPitch + lane];
+            uint32_t o;
+            if (ge) {                                 // x - M
+                const uint32_t m = __ldg(T.Mtotal + l), s = x - m;
+                o = s - bm;
+                bm = (x < m) | (s < bm);
+            } else {
+                o = neg ? D[l * kCrtPitch + lane] : x;
+            }
+            X[l * kCrtPitch + lane] = o;
+            if (o) nl = l + 1;
+        }
+        __syncwarp();
+        if (lane < cnt) {
+            const uint32_t row = out_idx ? out_idx[j0 + lane] : (uint32_t)(j0 + lane);
+            sign_out[row] = nl ? (neg ? -1 : 1) : 0;
+            if (nlimbs_out) nlimbs_out[row] = nl;
+        }
+        for (int v = 0; v < cnt; ++v) {
+            uint32_t* out = limbs + (size_t)(out_idx ? out_idx[j0 + v] : (uint32_t)(j0 + v)) * stride;
+            for (int l = lane; l < stride; l += 32) out[l] = l < L ? X[l * kCrtPitch + v] : 0u;
+        }
+        __syncwarp();
+    }
+}
+
 // ---- host launchers -----------------------------------------------------
 cudaError_t launch_crt_setup(const uint32_t* moduli, int K, int L, uint32_t* pinv, uint32_t* r2,
-                             uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal, cudaStream_t st) {
-    k_crt_setup<<<1, 256, 0, st>>>(moduli, K, L, pinv, r2, ginv, Mlimbs, Mtotal);
+                             uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal, uint32_t* garner,
+                             cudaStream_t st) {
+    k_crt_setup<<<1, 256, 0, st>>>(moduli, K, L, pinv, r2, ginv, Mlimbs, Mtotal, garner);
+    return cudaGetLastError();
+}
+
+static cudaError_t launch_crt_lanes(const uint32_t* res, int n, const CrtTables& T, uint32_t* limbs,
+                                    int stride, int32_t* sign, int32_t* nl, uint32_t* ul, int sms,
+                                    cudaStream_t st, const uint64_t* in_off, const uint32_t* out_idx) {
+    const size_t per_warp = 4 * crt_lanes_warp_words(T.K, T.L);
+    int wpb = (int)std::min<size_t>(4, std::max<size_t>(1, (96 * 1024) / per_warp));
+    const size_t smem = 4ull * 2 * T.K + (size_t)wpb * per_warp;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_crt_lanes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int groups = (n + 31) / 32;
+    int blocks = (groups + wpb - 1) / wpb;
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_crt_lanes, 32 * wpb, smem);
+    if (e != cudaSuccess) return e;
+    blocks = std::max(1, std::min(blocks, std::max(occ, 1) * sms));
+    k_crt_lanes<<<blocks, 32 * wpb, smem, st>>>(res, n, T, limbs, stride, sign, nl, ul, in_off, out_idx);
     return cudaGetLastError();
 }
 
@@ -243,6 +411,8 @@ cudaError_t launch_crt(const uint32_t* res, int n, const CrtTables& T, uint32_t*
                        int32_t* sign, int32_t* nl, uint32_t* ul, int sms, cudaStream_t st,
                        const uint64_t* in_off, const uint32_t* out_idx) {
     if (n <= 0) return cudaSuccess;
+    if (T.garner && T.K <= kCrtLanesMaxK)
+        return launch_crt_lanes(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
     const int own = (T.K + 31) / 32;
     if (own <= 1) return launch_crt_t<1>(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
     if (own <= 2) return launch_crt_t<2>(res, n, T, limbs, stride, sign, nl, ul, sms, st, in_off, out_idx);
@@ -261,16 +431,28 @@ cudaError_t launch_crt(const uint32_t* res, int n, const CrtTables& T, uint32_t*
 // its own pool, or that must not trigger the device-wide synchronisation a
 // cudaFree implies.  The per-moduli tables that dr_crt_batch_device keeps in
 // cudaMalloc'd buffers live here in one file-scope device array instead:
-// every GPU that loads the library holds it (about 66 KB) until the process
+// every GPU that loads the library holds it (about 130 KB) until the process
 // exits, and every call rebuilds the tables in it, so calls that overlap on
 // the GPU race on its contents.
 namespace dr {
 
 constexpr int kStaticCrtMaxK = 128;
 constexpr int kStaticCrtL = (31 * kStaticCrtMaxK + 31) / 32 + 2;
-constexpr int kStaticCrtWords = 4 * kStaticCrtMaxK + kStaticCrtMaxK * kStaticCrtL + kStaticCrtL;
+constexpr int kStaticCrtWords = 4 * kStaticCrtMaxK + kStaticCrtMaxK * kStaticCrtL + kStaticCrtL +
+                                kStaticCrtMaxK * kStaticCrtMaxK;
 
 static __device__ __align__(256) uint32_t g_crt_static[kStaticCrtWords];
+
+// The moduli travel by value as a kernel argument (512 bytes), so a call
+// makes no host-to-device copy; this kernel stores them at the head of the
+// static array, where k_crt_setup then reads them.
+struct CrtModuli {
+    uint32_t p[kStaticCrtMaxK];
+};
+
+__global__ void k_crt_static_moduli(const CrtModuli mods, int K) {
+    for (int j = threadIdx.x; j < K; j += blockDim.x) g_crt_static[j] = mods.p[j];
+}
 
 namespace {
 std::mutex g_static_mu;
@@ -319,22 +501,29 @@ extern "C" int dr_crt_batch_device_noalloc(const uint32_t* residues_d, int32_t K
         base = static_cast<uint32_t*>(g_static_addr[dev]);
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // layout: moduli[K] pinv[K] r2[K] ginv[K] Mlimbs[K*L] Mtotal[L]
+    // layout: moduli[K] pinv[K] r2[K] ginv[K] Mlimbs[K*L] Mtotal[L] garner[K*K]
     uint32_t* moduli = base;
     uint32_t* pinv = base + K;
     uint32_t* r2 = base + 2 * K;
     uint32_t* ginv = base + 3 * K;
     uint32_t* Ml = base + 4 * K;
     uint32_t* Mt = Ml + (size_t)K * L;
-    // own copy: another thread may grow (and move) the shared table meanwhile
-    const std::vector<uint32_t> tab(prime_table(K).begin(), prime_table(K).begin() + K);
-    e = cudaMemcpyToSymbolAsync(g_crt_static, tab.data(), 4ull * K, 0, cudaMemcpyHostToDevice, st);
-    if (e == cudaSuccess) e = launch_crt_setup(moduli, K, L, pinv, r2, ginv, Ml, Mt, st);
+    uint32_t* gar = Mt + L;
+    // the moduli, copied under the prime table's lock (another thread may
+    // grow the table meanwhile), go to the device as a kernel argument
+    CrtModuli mods{};
+    if (prime_table_copy(K, mods.p) != DR_OK) {
+        set_error("dr_crt_batch_device_noalloc: prime table");
+        return DR_ERR_UNSUPPORTED;
+    }
+    k_crt_static_moduli<<<1, 128, 0, st>>>(mods, K);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = launch_crt_setup(moduli, K, L, pinv, r2, ginv, Ml, Mt, gar, st);
     if (e != cudaSuccess) {
         set_error(std::string("dr_crt_batch_device_noalloc setup: ") + cudaGetErrorString(e));
         return DR_ERR_CUDA;
     }
-    CrtTables T{moduli, pinv, r2, ginv, Ml, Mt, K, L};
+    CrtTables T{moduli, pinv, r2, ginv, Ml, Mt, K, L, gar};
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     e = launch_crt(residues_d, n, T, limbs_d, limb_stride, sign_d, nullptr, nullptr, sms, st);

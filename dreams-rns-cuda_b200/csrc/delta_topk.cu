@@ -278,4 +278,83 @@ cudaError_t launch_topk_tile(const double* vals, const uint64_t* in_keys, const 
 
 int topk_tile_size() { return kTopkTile; }
 
+// ---- top-k of a large array: threshold filter --------------------------------
+// Sorting every tile costs far more than reading the values once.  For large
+// n the host picks a threshold from a strided sample (its r-th best key, r
+// chosen so that several times k values are expected to reach it), one pass
+// over all n values keeps the (key, index) pairs at or above it, and only
+// those go through the tile sort.  The result is exact whenever at least k
+// values pass and the candidate buffer holds all of them; the host checks
+// the count and otherwise sorts every value.
+
+// sample_keys[j] = key of vals[j * stride], j < s
+__global__ void k_topk_sample(const double* __restrict__ vals, int64_t stride, int s,
+                              uint64_t* __restrict__ sample_keys, uint32_t* __restrict__ sample_idx) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < s; j += gridDim.x * blockDim.x) {
+        sample_keys[j] = desc_key(vals[(int64_t)j * stride]);
+        sample_idx[j] = (uint32_t)j;
+    }
+}
+
+// Appends (key, index) of every value whose key is >= *thr to the candidate
+// buffer (warp-aggregated: one atomic per warp and pass); *count counts all
+// of them, also those beyond cap, which are not written.
+__global__ void __launch_bounds__(256) k_topk_filter(const double* __restrict__ vals, int n,
+                                                     const uint64_t* __restrict__ thr,
+                                                     uint64_t* __restrict__ cand_keys,
+                                                     uint32_t* __restrict__ cand_idx, int cap,
+                                                     unsigned int* __restrict__ count) {
+    const uint64_t t = *thr;
+    const int lane = threadIdx.x & 31;
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int i = base + threadIdx.x;
+        uint64_t key = 0;
+        bool keep = false;
+        if (i < n) {
+            key = desc_key(__ldcs(vals + i));   // streamed once: no reuse to cache
+            keep = key >= t;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (m == 0u) continue;
+        unsigned pos = 0;
+        if (lane == __ffs(m) - 1) pos = atomicAdd(count, (unsigned)__popc(m));
+        pos = __shfl_sync(0xffffffffu, pos, __ffs(m) - 1) + __popc(m & ((1u << lane) - 1u));
+        if (keep && pos < (unsigned)cap) {
+            cand_keys[pos] = key;
+            cand_idx[pos] = (uint32_t)i;
+        }
+    }
+}
+
+// vals_out[j] = vals[idx[j]], j < k
+__global__ void k_topk_gather(const double* __restrict__ vals, const uint32_t* __restrict__ idx, int k,
+                              double* __restrict__ vals_out, int32_t* __restrict__ idx_out) {
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < k; j += gridDim.x * blockDim.x) {
+        const uint32_t i = idx[j];
+        if (idx_out) idx_out[j] = (int32_t)i;
+        if (vals_out) vals_out[j] = vals[i];
+    }
+}
+
+cudaError_t launch_topk_sample(const double* vals, int64_t stride, int s, uint64_t* keys, uint32_t* idx,
+                               cudaStream_t st) {
+    k_topk_sample<<<(s + 255) / 256, 256, 0, st>>>(vals, stride, s, keys, idx);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_topk_filter(const double* vals, int n, const uint64_t* thr, uint64_t* cand_keys,
+                               uint32_t* cand_idx, int cap, unsigned int* count, int sms, cudaStream_t st) {
+    int blocks = (n + 255) / 256;
+    if (blocks > sms * 8) blocks = sms * 8;
+    k_topk_filter<<<blocks, 256, 0, st>>>(vals, n, thr, cand_keys, cand_idx, cap, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_topk_gather(const double* vals, const uint32_t* idx, int k, double* vals_out,
+                               int32_t* idx_out, cudaStream_t st) {
+    k_topk_gather<<<(k + 255) / 256, 256, 0, st>>>(vals, idx, k, vals_out, idx_out);
+    return cudaGetLastError();
+}
+
 }  // namespace dr

@@ -6,10 +6,13 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
 #include "../../include/dreams_b200.h"
+#include "../../include/dreams_b200_debug.h"
+#include "debug_check.cuh"
 #include "host_common.h"
 #include "launch.h"
 #include "shadow_impl.cuh"
@@ -160,7 +163,9 @@ HostPool& host_pool() {
 
 int crt_limbs_for(int K) { return (31 * K + 31) / 32 + 2; }
 
-static int build_crt_set(const uint32_t* moduli_host, int K, CrtSet& S, cudaStream_t st) {
+// standard: the moduli are the prime table's (distinct primes above 2^30),
+// which the lane-per-value CRT kernel needs
+static int build_crt_set(const uint32_t* moduli_host, int K, CrtSet& S, cudaStream_t st, bool standard) {
     S.K = K;
     S.L = crt_limbs_for(K);
     DR_CUDA(S.moduli.alloc(4ull * K));
@@ -169,9 +174,12 @@ static int build_crt_set(const uint32_t* moduli_host, int K, CrtSet& S, cudaStre
     DR_CUDA(S.ginv.alloc(4ull * K));
     DR_CUDA(S.Mlimbs.alloc(4ull * K * S.L));
     DR_CUDA(S.Mtotal.alloc(4ull * S.L));
+    const bool lanes = standard && K <= kCrtLanesMaxK;
+    if (lanes) DR_CUDA(S.garner.alloc(4ull * K * K));
     DR_CUDA(cudaMemcpyAsync(S.moduli.p, moduli_host, 4ull * K, cudaMemcpyHostToDevice, st));
     DR_CUDA(launch_crt_setup(S.moduli.as<uint32_t>(), K, S.L, S.pinv.as<uint32_t>(), S.r2.as<uint32_t>(),
-                             S.ginv.as<uint32_t>(), S.Mlimbs.as<uint32_t>(), S.Mtotal.as<uint32_t>(), st));
+                             S.ginv.as<uint32_t>(), S.Mlimbs.as<uint32_t>(), S.Mtotal.as<uint32_t>(),
+                             lanes ? S.garner.as<uint32_t>() : nullptr, st));
     DR_CUDA(cudaStreamSynchronize(st));
     return DR_OK;
 }
@@ -187,7 +195,7 @@ int crt_tables_std(int K, std::shared_ptr<CrtSet>* out) {
     }
     auto S = std::make_shared<CrtSet>();
     const auto& tab = prime_table(K);
-    int rc = build_crt_set(tab.data(), K, *S, g_ctx->stream);
+    int rc = build_crt_set(tab.data(), K, *S, g_ctx->stream, true);
     if (rc != DR_OK) return rc;
     std::lock_guard<std::mutex> lk(g_ctx->mu);
     g_ctx->crt_std[K] = S;
@@ -370,6 +378,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     B->n_walks = (uint32_t)n_walks;
     B->n_res = n_res;
     build_mark(0);
+    NvtxRange nvtx_build("dr.build");
+    const auto t_build0 = std::chrono::steady_clock::now();
 
     // ---- programs
     std::vector<std::shared_ptr<Plan>> plans(n_programs);
@@ -427,7 +437,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         DevProgram d{};
         d.m = P.m;
         d.dim = P.dim;
-        d.cls = (engine == DR_ENGINE_AUTO) ? (uint32_t)P.cls : (uint32_t)CLS_INTERP;
+        // AUTO and PLAIN run the planned class; INTERP forces the interpreter
+        d.cls = (engine == DR_ENGINE_INTERP) ? (uint32_t)CLS_INTERP : (uint32_t)P.cls;
         d.degree = P.degree;
         if (P.code_id != last_code_id) {
             auto at = code_at.find(P.code_id);
@@ -643,9 +654,19 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         if (W.checkpoint) return nc(W.checkpoint) + nc(W.depth - W.checkpoint);
         return nc(W.depth);
     };
+    // per launch: the most registers, constants and axes of its programs
+    // (the rows of its per-warp shared memory)
+    struct Rows {
+        uint32_t regs = 1, consts = 1, axes = 1;
+        void merge(const Rows& o) {
+            regs = std::max(regs, o.regs);
+            consts = std::max(consts, o.consts);
+            axes = std::max(axes, o.axes);
+        }
+    };
     struct TileCount {
         std::map<LaunchKey, size_t> tiles;   // count, then this part's first index in the set
-        std::map<LaunchKey, std::pair<uint32_t, uint32_t>> rows;   // max registers, constants
+        std::map<LaunchKey, Rows> rows;
         uint64_t groups = 0, slots = 0;      // count, then this part's first group / slot
     };
     const int tparts = build_parts((size_t)n_walks);
@@ -654,18 +675,17 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         TileCount& T = tcount[part];
         LaunchKey prev{-1, 0, 0, 0};
         size_t* cur = nullptr;
-        std::pair<uint32_t, uint32_t>* rows = nullptr;
+        Rows* rows = nullptr;
         for (size_t w = w_lo; w < w_hi; ++w) {
             const DevWalk& W = dwalks[w];
             const LaunchKey key = walk_key(W);
             if (!cur || key < prev || prev < key) {
                 cur = &T.tiles[key];
-                rows = &T.rows.emplace(key, std::make_pair(1u, 1u)).first->second;
+                rows = &T.rows[key];
                 prev = key;
             }
             const DevProgram& G = dprogs[W.prog];
-            rows->first = std::max(rows->first, std::max(G.n_regs, G.dn_regs));
-            rows->second = std::max(rows->second, G.n_consts);
+            rows->merge(Rows{std::max(G.n_regs, G.dn_regs), G.n_consts, G.dim});
             const uint64_t nb = (W.K + 31) / 32, nc = n_chunks_of(W);
             *cur += nb * nc;
             T.groups += nb;
@@ -675,16 +695,12 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     if (tparts > 1) host_pool().run(tparts, (size_t)n_walks, count_range);
     else count_range(0, 0, (size_t)n_walks);
     std::map<LaunchKey, std::vector<DevTile>> tile_sets;
-    std::map<LaunchKey, std::pair<uint32_t, uint32_t>> key_rows;   // max registers, constants
+    std::map<LaunchKey, Rows> key_rows;
     uint64_t n_group_total = 0, slots64 = 0;
     {
         std::map<LaunchKey, size_t> total;
         for (const TileCount& T : tcount)
-            for (const auto& kv : T.rows) {
-                auto& r = key_rows.emplace(kv.first, std::make_pair(1u, 1u)).first->second;
-                r.first = std::max(r.first, kv.second.first);
-                r.second = std::max(r.second, kv.second.second);
-            }
+            for (const auto& kv : T.rows) key_rows[kv.first].merge(kv.second);
         for (TileCount& T : tcount) {
             for (auto& kv : T.tiles) {
                 const size_t c = kv.second;
@@ -780,12 +796,13 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         L.off = (uint32_t)tiles.size();
         L.count = (uint32_t)v.size();
         L.items = L.count;
-        const uint32_t rr = key_rows[kv.first].first, rc_ = key_rows[kv.first].second;
+        const Rows& kr = key_rows[kv.first];
         const uint32_t ns = (uint32_t)std::max(streams_for(L.cls, L.m), 0);
-        L.rows_regs = rr;
-        L.rows_consts = rc_;
+        L.rows_regs = kr.regs;
+        L.rows_consts = kr.consts;
+        L.rows_axes = std::min<uint32_t>(std::max<uint32_t>(kr.axes, 1), kMaxAxes);
         L.rows_stage = std::max(L.m * L.m, (L.D + 1) * ns);
-        L.rows_per_warp = L.rows_regs + L.rows_consts + 3 * kMaxAxes + L.rows_stage;
+        L.rows_per_warp = L.rows_regs + L.rows_consts + 3 * L.rows_axes + L.rows_stage;
         append_longest_first(tiles, v, [](const DevTile& t) { return t.s1 - t.s0; });
         B->launches.push_back(L);
     }
@@ -881,7 +898,10 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         walk_ops += per * (double)W.K * (double)W.depth;
     }
     const double walk_ns = walk_ops / 1.7e13 * 1e9;
-    const int wpb = (tune && tune->warps_per_block) ? (int)tune->warps_per_block
+    // the plain engine launches one single-warp block per tile: a warp per
+    // (walk, prime block) over the whole depth, no queue
+    const int wpb = plain ? 1
+                  : (tune && tune->warps_per_block) ? (int)tune->warps_per_block
                   : tuned_wpb ? (int)tuned_wpb : 4;
     B->wpb_used = (uint32_t)wpb;
     uint32_t q = 0;
@@ -935,12 +955,14 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             return DR_ERR_UNSUPPORTED;
         }
         const int want = (int)((L.items + wpb - 1) / wpb);
-        L.grid = std::max(1, std::min(want, occ * C.sms));
-        if (plain) L.grid = 1;
+        L.grid = plain ? std::max(1, want) : std::max(1, std::min(want, occ * C.sms));
     }
     B->n_queues = q;
 
     build_mark(5);
+    nvtx_build.end();
+    NvtxRange nvtx_upload("dr.upload");
+    const auto t_upload0 = std::chrono::steady_clock::now();
     // ---- upload
     cudaStream_t st = C.stream;
     if ((rc = upload(B->progs, dprogs, st))) return rc;
@@ -961,6 +983,15 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     for (auto& d : dprogs) max_m = std::max(max_m, d.m);
     B->chunk_stride = max_m * max_m * 32;
     DR_CUDA(B->chunkP.alloc(4ull * std::max<uint32_t>(slots, 1) * B->chunk_stride));
+    B->n_progs = (uint32_t)n_programs;
+    B->n_slots = slots;
+    B->n_code = code.size();
+    B->n_consts = consts.size();
+    B->n_axis = n_axis;
+    if (kDebugChecks) {
+        DR_CUDA(B->dbg.alloc(16));
+        DR_CUDA(cudaMemsetAsync(B->dbg.p, 0, 16, st));
+    }
     DR_CUDA(B->chunkSig.alloc(4ull * std::max<uint32_t>(slots, 1) * 32));
     DR_CUDA(B->queues.alloc(4ull * std::max<uint32_t>(B->n_queues, 1)));
     DR_CUDA(B->res.alloc(8ull * std::max<uint64_t>(n_res, 1)));
@@ -983,11 +1014,18 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     B->joins.resize(C.pool.size() + C.hpool.size());
     B->evals.assign(B->launches.size(), nullptr);
     for (size_t i = 0; i < B->launches.size(); ++i)
-        if (B->launches[i].kind == 1) DR_CUDA(cudaEventCreateWithFlags(&B->evals[i], cudaEventDisableTiming));
+        if (B->launches[i].kind == 1 || (B->launches[i].kind == 2 && !B->launches[i].lean))
+            DR_CUDA(cudaEventCreateWithFlags(&B->evals[i], cudaEventDisableTiming));
     for (auto& e : B->joins) DR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     build_mark(6);
     DR_CUDA(cudaStreamSynchronize(st));
     build_mark(7);
+    {
+        using ms = std::chrono::duration<double, std::milli>;
+        const auto t_end = std::chrono::steady_clock::now();
+        stage_add(STAGE_BUILD, ms(t_upload0 - t_build0).count());
+        stage_add(STAGE_UPLOAD, ms(t_end - t_upload0).count());
+    }
     *out = std::move(B);
     return DR_OK;
 }
@@ -1269,6 +1307,15 @@ static void batch_args(Batch& B, WalkArgs& wa, ShadowArgs& sa) {
     wa.p_res = B.res.as<uint32_t>();
     wa.q_res = B.res.as<uint32_t>() + std::max<uint64_t>(B.n_res, 1);
     wa.status = B.status.as<uint32_t>();
+    wa.n_progs = B.n_progs;
+    wa.n_walks = B.n_walks;
+    wa.n_groups = B.n_groups;
+    wa.n_slots = B.n_slots;
+    wa.n_code = B.n_code;
+    wa.n_consts = B.n_consts;
+    wa.n_axis = B.n_axis;
+    wa.n_res = B.n_res;
+    wa.dbg = kDebugChecks ? B.dbg.as<uint32_t>() : nullptr;
     sa = ShadowArgs{};
     sa.progs = wa.progs;
     sa.code = wa.code;
@@ -1282,6 +1329,17 @@ static void batch_args(Batch& B, WalkArgs& wa, ShadowArgs& sa) {
     sa.mf = B.mf.as<double>();
 }
 
+// Whether the walk launches wait for the integer-difference shadow chains to
+// be placed (launch completion events).  DREAMS_B200_CHAIN_FIRST=0 turns it
+// off.
+static bool chain_first() {
+    static const bool on = [] {
+        const char* v = std::getenv("DREAMS_B200_CHAIN_FIRST");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, ShadowArgs& sa, cudaStream_t s) {
     unsigned long long* ts = B.stamping ? B.tstamps.as<unsigned long long>() + 4 * (&L - B.launches.data()) : nullptr;
     wa.tstamp = ts;
@@ -1293,6 +1351,7 @@ static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, Shado
         wa.rows_regs = L.rows_regs;
         wa.rows_consts = L.rows_consts;
         wa.rows_stage = L.rows_stage;
+        wa.rows_axes = L.rows_axes;
         wa.rows_per_warp = L.rows_per_warp;
         return walk_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, wa, nullptr);
     }
@@ -1304,6 +1363,10 @@ static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, Shado
     if (L.kind == 2) {
         sa.n_items = L.items;
         sa.queue = B.queues.as<uint32_t>() + L.queue;
+        // the walk launches wait until these chain blocks are placed (not
+        // finished), so the chains get their SMs before the walks fill them
+        const cudaEvent_t started = (chain_first() && !L.lean) ? B.evals[&L - B.launches.data()] : nullptr;
+        StartedEvent se(started);
         return shadow_fd_dispatch(L.cls, L.m, L.D, L.grid, L.block, L.smem, s, sa, nullptr);
     }
     const size_t i = &L - B.launches.data();
@@ -1346,7 +1409,9 @@ static int enqueue_batch(Batch& B, cudaStream_t st, std::vector<cudaEvent_t>* en
                 // shadow chains (high priority) are placed before them
                 if (s && pass == 1)
                     for (size_t j = 0; j < B.launches.size(); ++j)
-                        if (B.launches[j].kind == 1 && !B.launches[j].follow && B.launches[j].items)
+                        if ((B.launches[j].kind == 1 ||
+                             (B.launches[j].kind == 2 && chain_first() && !B.launches[j].lean)) &&
+                            !B.launches[j].follow && B.launches[j].items)
                             if (cudaStreamWaitEvent(s, B.evals[j], 0) != cudaSuccess) s = nullptr;
             }
             if (!s) { rc = cuda_fail(cudaErrorUnknown, "stream fork"); break; }
@@ -1505,12 +1570,31 @@ cudaError_t batch_idle(Batch& B) {
     return e;
 }
 
+// DR_DEBUG builds: a failed device bounds check of the batch's runs becomes
+// DR_ERR_INDEX with the site, index and bound (the batch must be idle).
+static int debug_report(Batch& B) {
+    if (!kDebugChecks || !B.dbg.p) return DR_OK;
+    uint32_t rec[4] = {0, 0, 0, 0};
+    DR_CUDA(cudaMemcpy(rec, B.dbg.p, sizeof(rec), cudaMemcpyDeviceToHost));
+    if (!rec[0]) return DR_OK;
+    set_error("device bounds check failed (DR_DEBUG build): site " + std::to_string(rec[0]) + ", index " +
+              std::to_string(rec[1]) + " not below " + std::to_string(rec[2]) + " (" +
+              std::to_string(rec[3]) + " failed checks)");
+    return DR_ERR_INDEX;
+}
+
 int batch_read(Batch& B, uint32_t* p_res, uint32_t* q_res, uint64_t n_res, double* shadow,
                uint32_t* status) {
     Context& C = *g_ctx;
     DR_CUDA(cudaStreamSynchronize(C.stream));
     DR_CUDA(cudaEventSynchronize(B.ev1));
     cudaEventElapsedTime(&B.last_ms, B.ev0, B.ev1);
+    if (B.runs != B.runs_read) {      // each run's device time is counted once
+        stage_add(STAGE_DEVICE, B.last_ms);
+        B.runs_read = B.runs;
+    }
+    int rc = debug_report(B);
+    if (rc) return rc;
     const uint64_t n = std::min(n_res, B.n_res);
     if (p_res) DR_CUDA(cudaMemcpy(p_res, B.res.p, 4 * n, cudaMemcpyDeviceToHost));
     if (q_res)
@@ -1540,6 +1624,7 @@ static CrtTables tables_of(const CrtSet& S) {
     T.Mtotal = S.Mtotal.as<uint32_t>();
     T.K = S.K;
     T.L = S.L;
+    T.garner = S.garner.p ? S.garner.as<uint32_t>() : nullptr;
     return T;
 }
 
@@ -1562,7 +1647,7 @@ static int crt_device(const uint32_t* res_d, int32_t K, int32_t n, const uint32_
     if (moduli_host) {
         int rc = moduli_ok(moduli_host, K);
         if (rc) return rc;
-        rc = build_crt_set(moduli_host, K, custom, g_ctx->stream);
+        rc = build_crt_set(moduli_host, K, custom, g_ctx->stream, false);
         if (rc) return rc;
     } else {
         int rc = crt_tables_std(K, &S);
@@ -1629,8 +1714,16 @@ int dr_walk_batch(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blo
                          n_axis_params, tune, n_res, &B);
     if (rc) return rc;
     if (n_walks == 0) return DR_OK;
-    rc = batch_run(*B, ctx()->stream);
+    {
+        StageScope sc(STAGE_RUN, "dr.run");
+        rc = batch_run(*B, ctx()->stream);
+        if (rc == DR_OK) {
+            const cudaError_t e = cudaEventSynchronize(B->ev1);
+            if (e != cudaSuccess) rc = cuda_fail(e, "dr_walk_batch");
+        }
+    }
     if (rc) return rc;
+    StageScope sc(STAGE_READ, "dr.read");
     return batch_read(*B, p_res, q_res, n_res, shadow, status);
 }
 
@@ -1667,6 +1760,7 @@ int dr_batch_run(int32_t batch, void* stream) {
     Batch* B = find_batch(batch);
     if (!B) return DR_ERR_HANDLE;
     if (B->n_walks == 0) return DR_OK;
+    StageScope sc(STAGE_RUN, "dr.run");
     return batch_run(*B, static_cast<cudaStream_t>(stream));
 }
 
@@ -1678,6 +1772,7 @@ int dr_batch_read(int32_t batch, uint32_t* p_res, uint32_t* q_res, uint64_t n_re
     if (!B) return DR_ERR_HANDLE;
     // batch_read waits for this batch's end event (recorded on the stream it
     // ran on); other work on the device, a server's waves included, goes on
+    StageScope sc(STAGE_READ, "dr.read");
     return batch_read(*B, p_res, q_res, n_res, shadow, status);
 }
 
@@ -1834,7 +1929,9 @@ int dr_batch_read_pipeline(int32_t batch, double* delta, int32_t* topk_idx, doub
     Batch* B = find_batch(batch);
     if (!B) return DR_ERR_HANDLE;
     if (!B->pipe_on) { set_error("no pipeline set on this batch"); return DR_ERR_ARG; }
+    StageScope sc(STAGE_READ, "dr.read");
     DR_CUDA(batch_idle(*B));
+    if ((rc = debug_report(*B))) return rc;
     const uint32_t n = B->n_walks;
     std::vector<double> dl;
     if ((delta || topk_val) && B->pipe.delta_mode != DR_DELTA_NONE) {
@@ -1968,6 +2065,12 @@ int dr_debug_host_pool(int32_t parts, uint64_t n, int32_t repeats, uint64_t* ind
 
 int dr_debug_build_phases(double* ms, int32_t n) {
     for (int i = 0; i < n && i < 7; ++i) ms[i] = g_build_ms[i];
+    return DR_OK;
+}
+
+int dr_debug_build_info(int32_t* debug_checks) {
+    if (!debug_checks) return DR_ERR_ARG;
+    *debug_checks = kDebugChecks ? 1 : 0;
     return DR_OK;
 }
 
@@ -2112,44 +2215,130 @@ int dr_delta_batch(const uint32_t* p_limbs, const int32_t* p_sign, const uint32_
     return DR_OK;
 }
 
+}  // extern "C"
+
+namespace dr {
+
+// Tile sort of n (key, index) pairs -- from vals (keys computed) or from
+// in_keys/in_idx -- down to the best k, in passes over the two scratch pairs;
+// returns the buffer pair holding the sorted best k (at least min(k, n)).
+static int topk_tiles(const double* vals, const uint64_t* in_keys, const uint32_t* in_idx, int n, int k,
+                      DevBuf (&keys)[2], DevBuf (&idx)[2], cudaStream_t st, int* out_buf) {
+    const int tile = topk_tile_size();
+    const size_t cap = (size_t)((n + tile - 1) / tile) * k + 16;
+    for (int b = 0; b < 2; ++b) {
+        keys[b].pooled = idx[b].pooled = true;
+        DR_CUDA(keys[b].alloc(8 * cap));
+        DR_CUDA(idx[b].alloc(4 * cap));
+    }
+    int cnt = n, cur = 0;
+    cudaError_t e = launch_topk_tile(vals, in_keys, in_idx, cnt, k, keys[0].as<uint64_t>(), idx[0].as<uint32_t>(), st);
+    if (e != cudaSuccess) return cuda_fail(e, "topk");
+    cnt = ((cnt + tile - 1) / tile) * std::min(k, tile);
+    while (cnt > k) {
+        e = launch_topk_tile(nullptr, keys[cur].as<uint64_t>(), idx[cur].as<uint32_t>(), cnt, k,
+                             keys[cur ^ 1].as<uint64_t>(), idx[cur ^ 1].as<uint32_t>(), st);
+        if (e != cudaSuccess) return cuda_fail(e, "topk");
+        cnt = ((cnt + tile - 1) / tile) * std::min(k, tile);
+        cur ^= 1;
+    }
+    *out_buf = cur;
+    return DR_OK;
+}
+
+// Values below this count use the tile sort directly; above it the
+// threshold filter (delta_topk.cu) reads them once.
+constexpr int kTopkFilterMin = 1 << 18;
+constexpr int kTopkSample = 1 << 16;
+constexpr int kTopkCand = 1 << 16;
+
+// Top-k (k <= 2048) of n device doubles, highest first, NaN last, ties by
+// lower index: idx_d[j], val_d[j] (device pointers; either may be null) for
+// j < min(k, n).  Ends with a stream synchronisation (the filter's count is
+// checked on the host).  *filtered: whether the threshold filter decided.
+int topk_device(const double* vals, int n, int k, int32_t* idx_d, double* val_d, cudaStream_t st,
+                bool* filtered) {
+    const int keep = std::min(k, n);
+    if (filtered) *filtered = false;
+    if (keep <= 0) return DR_OK;
+    DevBuf keys[2], idx[2];
+    int out = 0, rc;
+    if (n >= kTopkFilterMin) {
+        // threshold: the r-th best of a strided sample, r about 4x the k it
+        // should hold at the sample's density, plus a margin
+        const int64_t stride = n / kTopkSample;
+        const int s = kTopkSample;
+        const int r = std::min(topk_tile_size() / 2,
+                               (int)(4 * (((int64_t)k * s + n - 1) / n)) + 8);
+        DevBuf skeys, sidx, ckeys, cidx, count;
+        skeys.pooled = sidx.pooled = ckeys.pooled = cidx.pooled = count.pooled = true;
+        DR_CUDA(skeys.alloc(8ull * s));
+        DR_CUDA(sidx.alloc(4ull * s));
+        DR_CUDA(ckeys.alloc(8ull * kTopkCand));
+        DR_CUDA(cidx.alloc(4ull * kTopkCand));
+        DR_CUDA(count.alloc(16));
+        DR_CUDA(launch_topk_sample(vals, stride, s, skeys.as<uint64_t>(), sidx.as<uint32_t>(), st));
+        DevBuf sk[2], si[2];
+        int sb = 0;
+        if ((rc = topk_tiles(nullptr, skeys.as<uint64_t>(), sidx.as<uint32_t>(), s, r, sk, si, st, &sb))) return rc;
+        const uint64_t* thr = sk[sb].as<uint64_t>() + (r - 1);
+        DR_CUDA(cudaMemsetAsync(ckeys.p, 0, 8ull * kTopkCand, st));      // key 0, index ~0: rank last
+        DR_CUDA(cudaMemsetAsync(cidx.p, 0xff, 4ull * kTopkCand, st));
+        DR_CUDA(cudaMemsetAsync(count.p, 0, 16, st));
+        DR_CUDA(launch_topk_filter(vals, n, thr, ckeys.as<uint64_t>(), cidx.as<uint32_t>(), kTopkCand,
+                                   count.as<unsigned int>(), g_ctx->sms, st));
+        if ((rc = topk_tiles(nullptr, ckeys.as<uint64_t>(), cidx.as<uint32_t>(), kTopkCand, k, keys, idx, st, &out)))
+            return rc;
+        DR_CUDA(launch_topk_gather(vals, idx[out].as<uint32_t>(), keep, val_d, idx_d, st));
+        unsigned int cnt = 0;
+        DR_CUDA(cudaMemcpyAsync(&cnt, count.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+        DR_CUDA(cudaStreamSynchronize(st));
+        if (cnt >= (unsigned)keep && cnt <= (unsigned)kTopkCand) {
+            if (filtered) *filtered = true;
+            return DR_OK;
+        }
+        // too few or too many candidates (heavy ties, NaNs): sort everything
+    }
+    if ((rc = topk_tiles(vals, nullptr, nullptr, n, k, keys, idx, st, &out))) return rc;
+    DR_CUDA(launch_topk_gather(vals, idx[out].as<uint32_t>(), keep, val_d, idx_d, st));
+    DR_CUDA(cudaStreamSynchronize(st));
+    return DR_OK;
+}
+
+}  // namespace dr
+
+extern "C" {
+
 int dr_topk(const double* delta, int32_t n, int32_t k, int32_t* idx_out, double* val_out) {
     int rc = ensure_ctx();
     if (rc) return rc;
-    if (n < 0 || k < 0 || (n > 0 && !delta)) return DR_ERR_ARG;
-    const int tile = topk_tile_size();
-    if (k > tile / 2) { set_error("k above 2048"); return DR_ERR_UNSUPPORTED; }
+    if (n < 0 || k < 0 || (n > 0 && !delta) || (k > 0 && n > 0 && !idx_out)) return DR_ERR_ARG;
+    if (k > topk_tile_size() / 2) { set_error("k above 2048"); return DR_ERR_UNSUPPORTED; }
     const int keep = std::min(k, n);
     if (keep == 0) return DR_OK;
     cudaStream_t st = g_ctx->stream;
-    DevBuf v, k1, i1, k2, i2;
+    DevBuf v, oi;
+    v.pooled = oi.pooled = true;
     DR_CUDA(v.alloc(8ull * n));
+    DR_CUDA(oi.alloc(4ull * keep));
     DR_CUDA(cudaMemcpyAsync(v.p, delta, 8ull * n, cudaMemcpyHostToDevice, st));
-    const size_t cap = (size_t)((n + tile - 1) / tile) * k + 16;
-    DR_CUDA(k1.alloc(8 * cap)); DR_CUDA(i1.alloc(4 * cap));
-    DR_CUDA(k2.alloc(8 * cap)); DR_CUDA(i2.alloc(4 * cap));
-    int cnt = n;
-    cudaError_t e = launch_topk_tile(v.as<double>(), nullptr, nullptr, cnt, k, k1.as<uint64_t>(), i1.as<uint32_t>(), st);
-    if (e != cudaSuccess) return cuda_fail(e, "topk");
-    cnt = ((cnt + tile - 1) / tile) * std::min(k, tile);
-    bool flip = false;
-    while (cnt > k) {
-        uint64_t* ik = flip ? k2.as<uint64_t>() : k1.as<uint64_t>();
-        uint32_t* ii = flip ? i2.as<uint32_t>() : i1.as<uint32_t>();
-        uint64_t* ok = flip ? k1.as<uint64_t>() : k2.as<uint64_t>();
-        uint32_t* oi = flip ? i1.as<uint32_t>() : i2.as<uint32_t>();
-        e = launch_topk_tile(nullptr, ik, ii, cnt, k, ok, oi, st);
-        if (e != cudaSuccess) return cuda_fail(e, "topk");
-        cnt = ((cnt + tile - 1) / tile) * std::min(k, tile);
-        flip = !flip;
-        if (cnt <= k) break;
-    }
-    std::vector<uint32_t> idx(keep);
-    DR_CUDA(cudaMemcpyAsync(idx.data(), flip ? i2.p : i1.p, 4ull * keep, cudaMemcpyDeviceToHost, st));
-    DR_CUDA(cudaStreamSynchronize(st));
-    for (int i = 0; i < keep; ++i) {
-        idx_out[i] = (int32_t)idx[i];
-        if (val_out) val_out[i] = delta[idx[i]];
-    }
+    if ((rc = topk_device(v.as<double>(), n, k, oi.as<int32_t>(), nullptr, st, nullptr))) return rc;
+    DR_CUDA(cudaMemcpy(idx_out, oi.p, 4ull * keep, cudaMemcpyDeviceToHost));
+    if (val_out)
+        for (int i = 0; i < keep; ++i) val_out[i] = delta[idx_out[i]];
+    return DR_OK;
+}
+
+int dr_topk_device(const double* delta_d, int32_t n, int32_t k, int32_t* idx_d, double* val_d, void* stream,
+                   int32_t* filtered) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    if (n < 0 || k < 0 || (n > 0 && !delta_d)) return DR_ERR_ARG;
+    if (k > topk_tile_size() / 2) { set_error("k above 2048"); return DR_ERR_UNSUPPORTED; }
+    bool f = false;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : g_ctx->stream;
+    if ((rc = topk_device(delta_d, n, k, idx_d, val_d, st, &f))) return rc;
+    if (filtered) *filtered = f ? 1 : 0;
     return DR_OK;
 }
 

@@ -99,6 +99,7 @@ HostPool& host_pool();
 struct CrtSet {
     int K = 0, L = 0;
     DevBuf moduli, pinv, r2, ginv, Mlimbs, Mtotal;
+    DevBuf garner;     // standard primes only: the lane kernel's Garner constants
 };
 
 struct Context {
@@ -143,7 +144,9 @@ struct LaunchSpec {
     uint32_t rows_regs, rows_consts, rows_stage, rows_per_warp;
     size_t smem;
     int grid, block;
-    // kind 1: the evaluation launch above is followed by the chain launch
+    // kind 1: the evaluation launch above is followed by the chain launch.
+    // rows_axes: axis rows per sub-block (kind 1) or, for a walk launch, the
+    // rows each of axis start values, steps and current values per warp
     uint32_t U = 1, rows_axes = 0, eoff = 0;   // sub-blocks, axis rows, first evaluation item
     uint32_t items2 = 0, queue2 = 0;
     size_t smem2 = 0;
@@ -200,6 +203,9 @@ struct Batch {
     uint64_t prime_steps = 0;
     std::vector<LaunchSpec> launches;
     uint32_t n_tiles = 0, n_groups = 0, n_queues = 0;
+    uint32_t n_progs = 0, n_slots = 0;            // table sizes (DR_DEBUG bounds checks)
+    uint64_t n_code = 0, n_consts = 0, n_axis = 0;
+    DevBuf dbg;                                   // DR_DEBUG builds: first failed device check
     uint32_t chunk_stride = 0;   // words per chunk-product slot
     DevBuf progs, code, consts, walks, axis, tiles, groups, group_done, chunkP, chunkSig;
     DevBuf shadow_list, queues, res, shadow, status;   // res: p residues then q residues
@@ -220,6 +226,7 @@ struct Batch {
     std::vector<uint64_t> h_res_off, h_cp_off;
     cudaGraphExec_t graph = nullptr;
     uint32_t runs = 0;             // dr_batch_run calls so far (the first launches directly)
+    uint32_t runs_read = 0;        // value of runs when a read last counted the device time
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr, join = nullptr;
     std::vector<cudaEvent_t> joins;
     std::vector<cudaEvent_t> evals;     // per launch: its step-matrix evaluation is done

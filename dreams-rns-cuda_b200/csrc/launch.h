@@ -17,7 +17,15 @@ struct CrtTables {
     const uint32_t* Mlimbs;   // [K][L]  M_i (M_0 = 1), little-endian limbs
     const uint32_t* Mtotal;   // [L]  product of all moduli
     int K, L;
+    // [K][K] p_i^-1 mod p_j for i < j, Montgomery form mod p_j (null: not
+    // built).  Built for the standard prime table only -- distinct primes
+    // above 2^30 -- where it lets one lane run a value's whole Garner chain.
+    const uint32_t* garner = nullptr;
 };
+
+// Largest K the lane-per-value CRT kernel takes (its per-warp shared memory
+// grows with K); larger K use the warp-per-value kernel.
+constexpr int kCrtLanesMaxK = 256;
 
 // Delta kernel arguments (delta_topk.cu).  Item i reads p at p + i*istride,
 // q at q + i*istride (nl limbs each), signs at ps/qs + i*sstride, and target
@@ -42,7 +50,8 @@ struct DeltaArgs {
 };
 
 cudaError_t launch_crt_setup(const uint32_t* moduli, int K, int L, uint32_t* pinv, uint32_t* r2,
-                             uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal, cudaStream_t st);
+                             uint32_t* ginv, uint32_t* Mlimbs, uint32_t* Mtotal, uint32_t* garner,
+                             cudaStream_t st);
 // in_off[j]: offset of value j's K residues (null: j*K); out_idx[j]: output
 // row of value j in limbs/sign/nl (null: j).
 cudaError_t launch_crt(const uint32_t* res, int n, const CrtTables& T, uint32_t* limbs, int stride,
@@ -57,6 +66,13 @@ cudaError_t launch_crt_check(const uint32_t* limbs, const int32_t* signs, int L,
 cudaError_t launch_topk_tile(const double* vals, const uint64_t* in_keys, const uint32_t* in_idx,
                              int n, int k, uint64_t* out_keys, uint32_t* out_idx, cudaStream_t st);
 int topk_tile_size();
+// threshold-filter top-k of large arrays (delta_topk.cu)
+cudaError_t launch_topk_sample(const double* vals, int64_t stride, int s, uint64_t* keys, uint32_t* idx,
+                               cudaStream_t st);
+cudaError_t launch_topk_filter(const double* vals, int n, const uint64_t* thr, uint64_t* cand_keys,
+                               uint32_t* cand_idx, int cap, unsigned int* count, int sms, cudaStream_t st);
+cudaError_t launch_topk_gather(const double* vals, const uint32_t* idx, int k, double* vals_out,
+                               int32_t* idx_out, cudaStream_t st);
 
 // occ != nullptr: only report resident blocks per SM for (block, smem).
 cudaError_t walk_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block, size_t smem,
@@ -87,6 +103,18 @@ cudaError_t walk_dispatch_interp(uint32_t m, int grid, int block, size_t smem, c
 // in the stream: its blocks may become resident while that kernel still
 // runs (once it has executed griddepcontrol.launch_dependents) and must
 // execute griddepcontrol.wait before reading what it wrote.
+// A launch made while a StartedEvent is in scope on the calling thread also
+// records that event once all its blocks have begun execution (the launch
+// completion event), so other streams can wait for the kernel to be placed
+// without waiting for it to finish.
+inline thread_local cudaEvent_t tl_started_event = nullptr;
+struct StartedEvent {
+    explicit StartedEvent(cudaEvent_t e) { tl_started_event = e; }
+    ~StartedEvent() { tl_started_event = nullptr; }
+    StartedEvent(const StartedEvent&) = delete;
+    StartedEvent& operator=(const StartedEvent&) = delete;
+};
+
 template <typename KernelT, typename ArgT>
 inline cudaError_t run_kernel(KernelT k, int grid, int block, size_t smem, cudaStream_t st,
                               const ArgT& a, int* occ, bool early_start = false) {
@@ -97,13 +125,14 @@ inline cudaError_t run_kernel(KernelT k, int grid, int block, size_t smem, cudaS
     if (occ) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(occ, k, block, smem);
     int prio = 0;
     const bool has_prio = st && cudaStreamGetPriority(st, &prio) == cudaSuccess && prio != 0;
-    if (has_prio || early_start) {
+    const cudaEvent_t started = tl_started_event;
+    if (has_prio || early_start || started) {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)grid);
         cfg.blockDim = dim3((unsigned)block);
         cfg.dynamicSmemBytes = smem;
         cfg.stream = st;
-        cudaLaunchAttribute attr[2];
+        cudaLaunchAttribute attr[3];
         unsigned n = 0;
         if (has_prio) {
             attr[n].id = cudaLaunchAttributePriority;
@@ -113,6 +142,12 @@ inline cudaError_t run_kernel(KernelT k, int grid, int block, size_t smem, cudaS
         if (early_start) {
             attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
             attr[n].val.programmaticStreamSerializationAllowed = 1;
+            ++n;
+        }
+        if (started) {
+            attr[n].id = cudaLaunchAttributeLaunchCompletionEvent;
+            attr[n].val.launchCompletionEvent.event = started;
+            attr[n].val.launchCompletionEvent.flags = 0;
             ++n;
         }
         cfg.attrs = attr;

@@ -1,10 +1,13 @@
-// Integer-pipe peak microbenchmark: the denominator of the walk kernels'
-// roofline.  Each thread runs 8 independent dependency chains so issue, not
-// latency, is the limit; one launch fills every SM with 1024 threads.
+// Integer-pipe peak microbenchmarks: the denominators of the walk kernels'
+// roofline, one per instruction class the Montgomery step uses.  Each thread
+// runs 8 independent dependency chains so issue, not latency, is the limit;
+// one launch fills every SM with 2048 threads.
 //   kind 0: 32x32->64 wide multiply-add (mad.wide.u32), the Montgomery product
 //   kind 1: 32-bit add + unsigned min, the modular addition
 //   kind 2: 1:2 mix of kind 0 and kind 1 instructions
-// Reports lane-instructions per second.
+//   kind 3: 32-bit low multiply-add (mad.lo.u32), the Montgomery quotient
+//   kind 4: unsigned min alone (plus one add per 8 mins for a varying operand)
+// Reports lane-instructions per second (kind 4 counts its mins only).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -36,6 +39,14 @@ __global__ void __launch_bounds__(256) k_int_peak(uint32_t* out, int iters, uint
                 asm volatile("add.u32 %0, %1, %2;" : "=r"(s) : "r"(a[k]), "r"(b));
                 asm volatile("min.u32 %0, %1, %2;" : "=r"(a[k]) : "r"(s), "r"(s - p));
             }
+            if (KIND == 3) {
+                asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[k]) : "r"(b), "r"(p));
+            }
+        }
+        if (KIND == 4) {
+            const uint32_t v = b + (uint32_t)i * 0x9e3779b9u;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) asm volatile("min.u32 %0, %0, %1;" : "+r"(a[k]) : "r"(v));
         }
     }
     uint32_t acc = 0;
@@ -51,13 +62,19 @@ extern "C" int dr_bench_int_peak(int32_t kind, double* lane_ops_per_s) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return DR_ERR_CUDA;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (kind < 0 || kind > 4) {
+        set_error("dr_bench_int_peak: kind must be 0..4");
+        return DR_ERR_ARG;
+    }
     uint32_t* out = nullptr;
     if (cudaMalloc(&out, 16) != cudaSuccess) return DR_ERR_NOMEM;
     const int iters = 4096, threads = 256, blocks = sms * 8;
     auto launch = [&](int it) {
         if (kind == 0) k_int_peak<0><<<blocks, threads>>>(out, it, 12345u);
         else if (kind == 1) k_int_peak<1><<<blocks, threads>>>(out, it, 12345u);
-        else k_int_peak<2><<<blocks, threads>>>(out, it, 12345u);
+        else if (kind == 2) k_int_peak<2><<<blocks, threads>>>(out, it, 12345u);
+        else if (kind == 3) k_int_peak<3><<<blocks, threads>>>(out, it, 12345u);
+        else k_int_peak<4><<<blocks, threads>>>(out, it, 12345u);
     };
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -76,7 +93,7 @@ extern "C" int dr_bench_int_peak(int32_t kind, double* lane_ops_per_s) {
         set_error(cudaGetErrorString(err));
         return DR_ERR_CUDA;
     }
-    const double per_iter = kind == 0 ? 8.0 : kind == 1 ? 16.0 : 24.0;
+    const double per_iter = kind == 1 ? 16.0 : kind == 2 ? 24.0 : 8.0;
     *lane_ops_per_s = per_iter * iters * (double)threads * blocks / (ms * 1e-3);
     return DR_OK;
 }

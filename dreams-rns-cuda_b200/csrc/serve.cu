@@ -57,6 +57,8 @@ struct Req {
     std::vector<uint32_t> p, q;
     double sh[3] = {0, 0, 0};
     uint32_t status = 0;
+    int error = DR_OK;            // the request failed (done with no results): poll returns it
+    std::string error_msg;
 };
 
 struct Wave {
@@ -121,6 +123,11 @@ struct Server {
     std::vector<void*> retired_pinned;    // outgrown pinned buffers, freed at close
     int error = DR_OK;
     std::string error_msg;
+    uint64_t failed = 0;                  // requests ended with an error of their own
+    // host-side fault injection (dr_debug_serve_inject): the next admissions
+    // fail as if allocating their resident state had failed, and the next
+    // wave launches fail as if growing their device buffers had failed
+    uint32_t inject_admit = 0, inject_wave = 0;
 };
 
 std::mutex g_srv_mu;
@@ -391,36 +398,49 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
     cudaError_t e = cudaSuccess;
 #define SV(x) do { e = (x); if (e != cudaSuccess) return cuda_fail(e, #x); } while (0)
     W.t_geom = ms_since(S, Clock::now());
-    SV(cudaEventRecord(W.ev0, st));
     W.n_tiles = tiles.size();
     Packer pk;
     const size_t o_progs = pk.add(progs), o_code = pk.add(code), o_consts = pk.add(consts),
                  o_walks = pk.add(walks), o_axis = pk.add(axis), o_tiles = pk.add(tiles),
                  o_groups = pk.add(groups), o_segs = pk.add(segs), o_eval = pk.add(eval_items);
-    SV(grow_host(W.h_up, W.h_up_cap, pk.total + 16, S.retired_pinned));
+    // zero-filled: combine counters | queues | status
+    const size_t n_done = std::max<size_t>(groups.size(), 1), n_q = std::max<uint32_t>(q, 1),
+                 n_st = std::max<uint32_t>(W.n_walks, 1);
+    const size_t zbytes = 4ull * (n_done + n_q + n_st);
+    // every buffer grows before any work is enqueued, so a failed allocation
+    // leaves the wave idle and only this wave's requests fail (DR_ERR_NOMEM)
+    if (S.inject_wave) {
+        --S.inject_wave;
+        set_error("serving: wave buffer allocation failed (injected by dr_debug_serve_inject)");
+        return DR_ERR_NOMEM;
+    }
+    {
+        const cudaError_t g[] = {
+            grow_host(W.h_up, W.h_up_cap, pk.total + 16, S.retired_pinned), grow(W.up, pk.total + 16),
+            grow(W.zero, zbytes), grow(W.mf, 8ull * std::max<uint64_t>(mf_doubles, 1)),
+            grow(W.chunkP, 4ull * std::max<uint32_t>(slots, 1) * kServeStride),
+            grow(W.chunkSig, 4ull * std::max<uint32_t>(slots, 1) * 32), grow(W.res, 8ull * W.n_res),
+            grow(W.shadow, 8ull * 6 * std::max<uint32_t>(W.n_walks, 1))};
+        for (cudaError_t ge : g)
+            if (ge != cudaSuccess) {
+                cudaGetLastError();   // an allocation failure is not sticky: clear it
+                set_error(std::string("serving: wave buffer allocation failed: ") + cudaGetErrorString(ge));
+                return ge == cudaErrorMemoryAllocation ? DR_ERR_NOMEM : DR_ERR_CUDA;
+            }
+    }
+    SV(cudaEventRecord(W.ev0, st));
     auto stage = [&](size_t off, const auto& v) {
         if (!v.empty()) std::memcpy(W.h_up + off, v.data(), sizeof(v[0]) * v.size());
     };
     stage(o_progs, progs); stage(o_code, code); stage(o_consts, consts); stage(o_walks, walks);
     stage(o_axis, axis); stage(o_tiles, tiles); stage(o_groups, groups); stage(o_segs, segs);
     stage(o_eval, eval_items);
-    SV(grow(W.up, pk.total + 16));
     if (pk.total) SV(cudaMemcpyAsync(W.up.p, W.h_up, pk.total, cudaMemcpyHostToDevice, st));
     auto at = [&](size_t off) { return static_cast<uint8_t*>(W.up.p) + off; };
-    // zero-filled: combine counters | queues | status
-    const size_t n_done = std::max<size_t>(groups.size(), 1), n_q = std::max<uint32_t>(q, 1),
-                 n_st = std::max<uint32_t>(W.n_walks, 1);
-    const size_t zbytes = 4ull * (n_done + n_q + n_st);
-    SV(grow(W.zero, zbytes));
     SV(cudaMemsetAsync(W.zero.p, 0, zbytes, st));
     uint32_t* z_done = W.zero.as<uint32_t>();
     uint32_t* z_queue = z_done + n_done;
     uint32_t* z_status = z_queue + n_q;
-    SV(grow(W.mf, 8ull * std::max<uint64_t>(mf_doubles, 1)));
-    SV(grow(W.chunkP, 4ull * std::max<uint32_t>(slots, 1) * kServeStride));
-    SV(grow(W.chunkSig, 4ull * std::max<uint32_t>(slots, 1) * 32));
-    SV(grow(W.res, 8ull * W.n_res));
-    SV(grow(W.shadow, 8ull * 6 * std::max<uint32_t>(W.n_walks, 1)));
     W.t_alloc = ms_since(S, Clock::now());
     WalkArgs wa{};
     wa.progs = reinterpret_cast<const DevProgram*>(at(o_progs));
@@ -449,6 +469,7 @@ int launch_wave(Server& S, Wave& W, const std::vector<Req*>& sel) {
             wa.queue = z_queue + s.queue;
             wa.rows_regs = s.rows_regs; wa.rows_consts = s.rows_consts; wa.rows_stage = s.rows_stage;
             wa.rows_per_warp = s.rows_per_warp;
+            wa.rows_axes = kMaxAxes;   // the wave layout keeps rows for every axis
             SV(walk_dispatch(s.cls, s.m, s.D, s.grid, s.block, s.smem, st, wa, nullptr));
         } else {
             sa.segs = d_segs + s.off; sa.n_items = s.items; sa.n_list = s.count;
@@ -528,6 +549,20 @@ void harvest(Server& S, Wave& W) {
     W.busy = false;
 }
 
+// End a request with an error of its own: it keeps no slots and no memory,
+// poll returns the error, and the server goes on with the others.
+void fail_request(Server& S, Req& r, int rc, const std::string& msg) {
+    release(S, r);
+    r.inflight = false;
+    r.error = rc;
+    r.error_msg = msg;
+    r.done = true;
+    r.t_done = Clock::now();
+    ++S.failed;
+    auto a = std::find(S.active.begin(), S.active.end(), r.id);
+    if (a != S.active.end()) S.active.erase(a);
+}
+
 void admit(Server& S) {
     for (auto it = S.pending.begin(); it != S.pending.end();) {
         Req& r = *S.reqs[*it];
@@ -536,6 +571,14 @@ void admit(Server& S) {
         const bool fits = S.admitted + r.need <= S.cap && S.free_slots.size() >= nb &&
                           (r.shadow_mode == SHADOW_NONE || !S.free_shadow.empty());
         if (!fits) { ++it; continue; }   // smaller later requests may still fit
+        if (S.inject_admit) {
+            --S.inject_admit;
+            fail_request(S, r, DR_ERR_NOMEM,
+                         "serving: admission could not allocate the request's resident state "
+                         "(injected by dr_debug_serve_inject)");
+            it = S.pending.erase(it);
+            continue;
+        }
         for (uint64_t b = 0; b < nb; ++b) { r.slots.push_back(S.free_slots.back()); S.free_slots.pop_back(); }
         if (r.shadow_mode != SHADOW_NONE) { r.shadow_slot = (int)S.free_shadow.back(); S.free_shadow.pop_back(); }
         S.admitted += r.need;
@@ -650,7 +693,11 @@ void loop(Server* Sp) {
                 S.wlog.push_back(g);
             }
         }
-        int rc = launch_wave(S, *free_wave, sel);
+        int rc;
+        {
+            NvtxRange nvtx("dr.serve.wave");
+            rc = launch_wave(S, *free_wave, sel);
+        }
         {
             std::lock_guard<std::mutex> lk(S.mu);
             if (free_wave->log < S.wlog.size()) {
@@ -663,7 +710,14 @@ void loop(Server* Sp) {
                 g.t_launch = free_wave->t_launch;
             }
         }
-        if (rc != DR_OK) {
+        if (rc == DR_ERR_NOMEM) {
+            // the wave's buffers could not grow: its requests fail, the
+            // server (whose context is intact) serves the rest
+            std::lock_guard<std::mutex> lk(S.mu);
+            const std::string msg = last_error();
+            for (Req* r : sel) fail_request(S, *r, rc, msg);
+            S.cv.notify_all();
+        } else if (rc != DR_OK) {
             std::lock_guard<std::mutex> lk(S.mu);
             S.error = rc;
             S.error_msg = last_error();
@@ -777,6 +831,12 @@ int dr_serve_poll(int32_t server, int64_t request, uint32_t* p_res, uint32_t* q_
     Req& r = *it->second;
     if (r.cancelled) return DR_ERR_HANDLE;
     if (!r.done) return DR_ERR_BUSY;
+    if (r.error != DR_OK) {
+        const int rc = r.error;
+        set_error(r.error_msg);
+        S->reqs.erase(it);
+        return rc;
+    }
     if (p_res) std::memcpy(p_res, r.p.data(), 4ull * r.d.K);
     if (q_res) std::memcpy(q_res, r.q.data(), 4ull * r.d.K);
     if (shadow) std::memcpy(shadow, r.sh, sizeof(r.sh));
@@ -858,6 +918,21 @@ int dr_debug_serve_waves(int32_t server, int32_t max_waves, int32_t* n_waves, do
         o[4] = g.n_req; o[5] = g.has_long; o[6] = g.wave; o[7] = (double)g.walk_tiles;
         o[8] = (double)g.shadow_span; o[9] = g.t_geom; o[10] = g.t_alloc; o[11] = g.t_launch;
     }
+    return DR_OK;
+}
+
+int dr_debug_serve_inject(int32_t server, int32_t kind, int32_t count, uint64_t* failed) {
+    Server* S = find_server(server);
+    if (!S) return DR_ERR_HANDLE;
+    if (count < 0 || (kind != DR_INJECT_ADMIT_NOMEM && kind != DR_INJECT_WAVE_NOMEM && kind != 0)) {
+        set_error("dr_debug_serve_inject: unknown kind or negative count");
+        return DR_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (kind == DR_INJECT_ADMIT_NOMEM) S->inject_admit = (uint32_t)count;
+    if (kind == DR_INJECT_WAVE_NOMEM) S->inject_wave = (uint32_t)count;
+    if (failed) *failed = S->failed;
+    S->cv.notify_all();
     return DR_OK;
 }
 

@@ -17,6 +17,7 @@
 #include <stdint.h>
 
 #include "../../include/dreams_b200.h"
+#include "debug_check.cuh"
 #include "dr_types.h"
 #include "interp.cuh"
 #include "modarith.cuh"
@@ -47,10 +48,16 @@ struct WalkArgs {
     uint32_t* p_res;
     uint32_t* q_res;
     uint32_t* status;
-    // per-warp shared memory layout, in 32-word rows
+    // per-warp shared memory layout, in 32-word rows; rows_axes rows each for
+    // the axis start values, steps and current values (the launch's most axes)
     uint32_t rows_regs, rows_consts, rows_stage;
     uint32_t rows_per_warp;
+    uint32_t rows_axes;
     unsigned long long* tstamp;   // diagnostics: [start, end] of this launch, or null
+    // sizes of the tables above, for the bounds checks of DR_DEBUG builds
+    uint32_t n_progs, n_walks, n_groups, n_slots;
+    uint64_t n_code, n_consts, n_axis, n_res;
+    uint32_t* dbg;                // DR_DEBUG builds: the first failed check (debug_check.cuh)
 };
 
 struct WarpMem {
@@ -68,9 +75,9 @@ __device__ __forceinline__ WarpMem warp_mem(const WalkArgs& A, uint32_t* smem, i
     w.rf = base;
     w.cst = w.rf + A.rows_regs * 32;
     w.x0 = w.cst + A.rows_consts * 32;
-    w.dx = w.x0 + kMaxAxes * 32;
-    w.cur = w.dx + kMaxAxes * 32;
-    w.stage = w.cur + kMaxAxes * 32;
+    w.dx = w.x0 + A.rows_axes * 32;
+    w.cur = w.dx + A.rows_axes * 32;
+    w.stage = w.cur + A.rows_axes * 32;
     return w;
 }
 
@@ -415,7 +422,7 @@ __device__ __forceinline__ void tile_dense(const WalkArgs& A, const DevTile& T, 
 }
 
 // INTERP: the bytecode is interpreted at every step (reference semantics
-// directly; also the plain one-walk-per-launch baseline).
+// directly).
 template <int M_>
 __device__ __forceinline__ void tile_interp(const WalkArgs& A, const DevTile& T, const DevWalk& W,
                                             const DevProgram& G, const WarpMem& wm, int lane) {
@@ -448,9 +455,49 @@ __device__ __forceinline__ void tile_interp(const WalkArgs& A, const DevTile& T,
     finish_tile<M_>(A, T, W, P, M.one, false, M, lane);
 }
 
+// DR_DEBUG builds: every index the tile takes from the batch's tables, checked
+// before it is used (each lane computes the same answer; lane 0 records).
+static __device__ __noinline__ bool tile_ok(const WalkArgs& A, const DevTile& T, int lane) {
+    uint32_t* d = lane == 0 ? A.dbg : nullptr;
+    if (!dbg_check(d, DBG_TILE_WALK, T.walk, A.n_walks) || !dbg_check(d, DBG_TILE_GROUP, T.group, A.n_groups))
+        return false;
+    const DevWalk& W = A.walks[T.walk];
+    if (!dbg_check(d, DBG_WALK_PROGRAM, W.prog, A.n_progs)) return false;
+    const DevProgram& G = A.progs[W.prog];
+    const DevGroup& Gr = A.groups[T.group];
+    bool ok = dbg_check(d, DBG_TILE_PRIMES, T.nprimes - 1u, 32) &
+              dbg_check(d, DBG_TILE_PRIMES, (uint64_t)T.prime0 + T.nprimes, (uint64_t)W.K + 1);
+    if (Gr.n_chunks > 1 || Gr.state != kNoState) ok &= dbg_check(d, DBG_TILE_SLOT, T.slot, A.n_slots);
+    ok &= dbg_check(d, DBG_WALK_OUTPUT, W.res_off + W.K, A.n_res + 1);
+    if (W.checkpoint) ok &= dbg_check(d, DBG_WALK_OUTPUT, W.cp_res_off + W.K, A.n_res + 1);
+    ok &= dbg_check(d, DBG_WALK_AXES, W.axis_off + 4ull * G.dim, A.n_axis + 1) &
+          dbg_check(d, DBG_OPERAND_AXIS, G.dim, A.rows_axes + 1);
+    ok &= dbg_check(d, DBG_PROGRAM_CODE, (uint64_t)G.op_off + G.n_ops, A.n_code + 1) &
+          dbg_check(d, DBG_PROGRAM_CODE, (uint64_t)G.dop_off + G.dn_ops, A.n_code + 1) &
+          dbg_check(d, DBG_PROGRAM_CONSTS, (uint64_t)G.c_off + G.n_consts, A.n_consts + 1) &
+          dbg_check(d, DBG_OPERAND_CONSTANT, G.n_consts, A.rows_consts + 1);
+    if (!ok) return false;
+    const uint32_t zr = G.zero_reg;
+    ok &= zr == 0xffffffffu || dbg_check(d, DBG_OPERAND_REGISTER, zr, A.rows_regs);
+    ok &= dbg_program(d, A.code + G.op_off, G.n_ops, A.rows_regs, A.rows_consts, G.dim, G.m * G.m) &
+          dbg_program(d, A.code + G.dop_off, G.dn_ops, A.rows_regs, A.rows_consts, G.dim,
+                      G.n_streams ? G.n_streams : G.m * G.m);
+    return ok;
+}
+
 // ---- persistent kernel ----------------------------------------------------
+// DR_WALK_MIN_BLOCKS (a build define; 0 = the compiler's choice) asks for that
+// many resident 128-thread blocks per SM, which caps the registers per thread.
+#ifndef DR_WALK_MIN_BLOCKS
+#define DR_WALK_MIN_BLOCKS 0
+#endif
+#if DR_WALK_MIN_BLOCKS > 0
+#define DR_WALK_BOUNDS __launch_bounds__(128, DR_WALK_MIN_BLOCKS)
+#else
+#define DR_WALK_BOUNDS __launch_bounds__(128)
+#endif
 template <int CLS, int M_, int D>
-__global__ void __launch_bounds__(128) k_walk(const WalkArgs A) {
+__global__ void DR_WALK_BOUNDS k_walk(const WalkArgs A) {
     extern __shared__ uint32_t smem[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -462,6 +509,7 @@ __global__ void __launch_bounds__(128) k_walk(const WalkArgs A) {
         t = __shfl_sync(kFull, t, 0);
         if (t >= A.n_tiles) break;
         const DevTile T = A.tiles[t];
+        if (kDebugChecks && A.dbg && !tile_ok(A, T, lane)) continue;   // recorded; the host reports it
         const DevWalk W = A.walks[T.walk];
         const DevProgram G = A.progs[W.prog];
         if (CLS == CLS_COMPANION) tile_companion<M_, D>(A, T, W, G, wm, lane);

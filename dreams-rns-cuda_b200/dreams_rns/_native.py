@@ -13,7 +13,12 @@ import threading
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_native", "libdreams_b200.so")
+# DREAMS_B200_DEBUG=1 selects the DR_DEBUG build (device bounds checks; built
+# by `python dreams-rns-cuda_b200/build.py --debug`); DREAMS_B200_LIB names
+# another build of the same library explicitly
+LIB_PATH = os.environ.get("DREAMS_B200_LIB") or os.path.join(
+    _HERE, "_native", "libdreams_b200_debug.so"
+    if os.environ.get("DREAMS_B200_DEBUG", "") not in ("", "0") else "libdreams_b200.so")
 
 DR_OK = 0
 DR_ERR_CUDA = -1
@@ -42,6 +47,9 @@ DR_STATUS_CP_CRT_OVERFLOW = 0x10
 DR_ENGINE_AUTO = 0
 DR_ENGINE_INTERP = 1
 DR_ENGINE_PLAIN = 2
+
+DR_INJECT_ADMIT_NOMEM = 1
+DR_INJECT_WAVE_NOMEM = 2
 
 DR_MAX_K = 8192
 
@@ -117,6 +125,7 @@ _SIGNATURES = {
     "dr_last_error": (ctypes.c_char_p, []),
     "dr_version": (ctypes.c_int, []),
     "dr_prime_table": (ctypes.c_int, [ctypes.c_int, _P]),
+    "dr_stage_times": (ctypes.c_int, [_P, _P, _I32, _I32]),
     "dr_program_info": (ctypes.c_int, [ctypes.c_char_p, _U64, _P, _P, _P]),
     "dr_walk_batch": (ctypes.c_int, [_P, _I32, _P, _P, _I32, _P, _U64, _P, _P, _P, _U64, _P, _P]),
     "dr_batch_create": (ctypes.c_int, [_P, _I32, _P, _P, _I32, _P, _U64, _P, _P]),
@@ -135,6 +144,7 @@ _SIGNATURES = {
     "dr_crt_batch_device_noalloc": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _P, _P]),
     "dr_delta_batch": (ctypes.c_int, [_P, _P, _P, _P, _I32, _I32, _P, _P, _P, _I32, _I32, _P]),
     "dr_topk": (ctypes.c_int, [_P, _I32, _I32, _P, _P]),
+    "dr_topk_device": (ctypes.c_int, [_P, _I32, _I32, _P, _P, _P, _P]),
     "dr_serve_open": (ctypes.c_int, [_P, _P]),
     "dr_serve_submit": (ctypes.c_int, [_I32, _P, ctypes.c_char_p, _U64, _P, _P]),
     "dr_serve_poll": (ctypes.c_int, [_I32, _I64, _P, _P, _P, _P, _P]),
@@ -147,6 +157,7 @@ _SIGNATURES = {
     "dr_debug_rescale": (ctypes.c_int, [_P, _P, _I32, _P]),
     "dr_debug_batch_timeline": (ctypes.c_int, [_I32, _I32, _P, _P]),
     "dr_debug_serve_waves": (ctypes.c_int, [_I32, _I32, _P, _P]),
+    "dr_debug_serve_inject": (ctypes.c_int, [_I32, _I32, _I32, _P]),
     "dr_debug_build_phases": (ctypes.c_int, [_P, _I32]),
     "dr_debug_sim_walk": (ctypes.c_int, [ctypes.c_char_p, _U64, _I32, _U64, _U64, _P, _I32, _I64,
                                          _U32, _U64, _I32, _P, _P, _P, _P]),

@@ -30,6 +30,7 @@ __all__ = [
     "CmfCompiler",
     "compile_cmf",
     "compile_cmf_from_dict",
+    "compile_pcf",
 ]
 
 
@@ -308,4 +309,26 @@ def compile_cmf_from_dict(matrix_dict: Dict[Tuple[int, int], str], m: int, dim: 
     comp = CmfCompiler(m=m, dim=dim, directions=directions or [1] * dim)
     for (row, col), text in matrix_dict.items():
         comp.compile_matrix_entry(row, col, sp.sympify(text, locals=local_ns), axis_symbols)
+    return comp.build()
+
+
+def compile_pcf(a_str: str, b_str: str) -> Optional[CmfProgram]:
+    """Companion bytecode of PCF(a, b) (reference runner.py:130-166): n is axis
+    0 with direction 1, entries (0,1)=b, (1,0)=1, (1,1)=a; None for imaginary
+    input.  Pure Python: it needs neither the native library nor a GPU."""
+    import sympy as sp
+    from sympy.abc import n
+
+    a_expr = sp.sympify(a_str)
+    b_expr = sp.sympify(b_str)
+    if a_expr.has(sp.I) or b_expr.has(sp.I):
+        return None
+    s = sp.Symbol("_s")
+    a_expr = a_expr.subs(n, s)
+    b_expr = b_expr.subs(n, s)
+    comp = CmfCompiler(m=2, dim=1, directions=[1])
+    axes = {"_s": 0}
+    comp.compile_matrix_entry(0, 1, b_expr, axes)
+    comp.compile_matrix_entry(1, 0, sp.Integer(1), axes)
+    comp.compile_matrix_entry(1, 1, a_expr, axes)
     return comp.build()

@@ -9,6 +9,8 @@ walks can be re-run with no host work (CUDA-graph replay).
 from __future__ import annotations
 
 import ctypes
+import threading
+import time
 from dataclasses import dataclass, field
 from fractions import Fraction
 from typing import Dict, List, Optional, Sequence, Tuple
@@ -18,7 +20,8 @@ import numpy as np
 from . import _native as N
 from .compiler import CmfProgram
 
-__all__ = ["WalkRequest", "pcf_request", "cmf_request", "run_walks", "WalkBatch", "program_blob"]
+__all__ = ["WalkRequest", "pcf_request", "cmf_request", "run_walks", "WalkBatch", "program_blob",
+           "stage_times"]
 
 
 def program_blob(program) -> bytes:
@@ -223,6 +226,8 @@ class _Packed:
     parameters (then state-vector entries) and the residue offsets."""
 
     def __init__(self, reqs: Sequence[WalkRequest]):
+        global _pack_ms, _pack_calls
+        t0 = time.perf_counter()
         n = len(reqs)
         packed = _pack_ext.pack(reqs) if _pack_ext is not None else _pack_py(reqs)
         self.n_programs, off, blob, desc, res, cp, axis, self.n_axis, self.n_res = packed
@@ -233,6 +238,35 @@ class _Packed:
         self.cp_off = np.frombuffer(cp, dtype=np.int64)[:n]
         self.axis = np.frombuffer(axis, dtype=np.int64)
         self.n = n
+        with _pack_lock:
+            _pack_ms += (time.perf_counter() - t0) * 1e3
+            _pack_calls += 1
+
+
+_pack_ms = 0.0
+_pack_calls = 0
+_pack_lock = threading.Lock()
+_STAGES = ("build", "upload", "run", "read", "device")
+
+
+def stage_times(reset: bool = False) -> dict:
+    """Milliseconds spent per stage of the engine calls since the last reset:
+    request packing (host, this module), then the C ABI's batch build,
+    allocation + upload, run, read-back and the device time of the runs read
+    back (dr_stage_times), each with its number of calls."""
+    global _pack_ms, _pack_calls
+    ms = np.zeros(len(_STAGES), dtype=np.float64)
+    calls = np.zeros(len(_STAGES), dtype=np.uint64)
+    N.check(N.lib().dr_stage_times(N.ptr(ms), N.ptr(calls), len(_STAGES), 1 if reset else 0),
+            "dr_stage_times")
+    with _pack_lock:
+        out = {"pack_ms": _pack_ms, "pack_calls": _pack_calls}
+        if reset:
+            _pack_ms, _pack_calls = 0.0, 0
+    for i, s in enumerate(_STAGES):
+        out[f"{s}_ms"] = float(ms[i])
+        out[f"{s}_calls"] = int(calls[i])
+    return out
 
 
 def _tune(chunk_steps=0, engine=N.DR_ENGINE_AUTO, warps_per_block=0, shadow_buffer_mb=0):

@@ -20,6 +20,7 @@ import numpy as np
 
 from . import _native as N
 from .compiler import CmfCompiler, CmfProgram, Opcode
+from .compiler import compile_pcf as _compile_pcf
 from .engine import pcf_request, run_walks
 
 __all__ = [
@@ -266,22 +267,7 @@ def compute_dreams_delta_exact(p_big: int, q_big: int, target, dps: int = 200):
 def compile_pcf(a_str: str, b_str: str) -> Optional[CmfProgram]:
     """Companion bytecode of PCF(a, b) (runner.py:130-166): n is axis 0 with
     direction 1, entries (0,1)=b, (1,0)=1, (1,1)=a; None for imaginary input."""
-    import sympy as sp
-    from sympy.abc import n
-
-    a_expr = sp.sympify(a_str)
-    b_expr = sp.sympify(b_str)
-    if a_expr.has(sp.I) or b_expr.has(sp.I):
-        return None
-    s = sp.Symbol("_s")
-    a_expr = a_expr.subs(n, s)
-    b_expr = b_expr.subs(n, s)
-    comp = CmfCompiler(m=2, dim=1, directions=[1])
-    axes = {"_s": 0}
-    comp.compile_matrix_entry(0, 1, b_expr, axes)
-    comp.compile_matrix_entry(1, 0, sp.Integer(1), axes)
-    comp.compile_matrix_entry(1, 1, a_expr, axes)
-    return comp.build()
+    return _compile_pcf(a_str, b_str)
 
 
 def pcf_initial_values(a_str: str):

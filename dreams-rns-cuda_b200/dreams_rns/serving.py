@@ -68,6 +68,8 @@ class WalkServer:
                                    ctypes.byref(lat))
         if rc == N.DR_ERR_BUSY:
             return None
+        if rc != N.DR_OK:
+            self._K.pop(rid, None)     # the request ended with an error of its own
         N.check(rc, "dr_serve_poll")
         del self._K[rid]
         if K not in self._primes:
@@ -95,6 +97,18 @@ class WalkServer:
                     raise TimeoutError(f"{len(left)} requests still running")
                 time.sleep(0.0002)
         return out
+
+    def inject_failures(self, admissions: int = 0, waves: int = 0) -> int:
+        """Test hook: the next ``admissions`` admissions and ``waves`` wave
+        launches fail as if their device allocation had failed; the affected
+        requests raise MemoryError from poll/wait and the server serves the
+        rest.  Returns the number of requests that have failed so far."""
+        failed = ctypes.c_uint64()
+        N.check(N.lib().dr_debug_serve_inject(self.handle, N.DR_INJECT_ADMIT_NOMEM, int(admissions),
+                                              ctypes.byref(failed)), "dr_debug_serve_inject")
+        N.check(N.lib().dr_debug_serve_inject(self.handle, N.DR_INJECT_WAVE_NOMEM, int(waves),
+                                              ctypes.byref(failed)), "dr_debug_serve_inject")
+        return failed.value
 
     def cancel(self, rid: int) -> None:
         N.check(N.lib().dr_serve_cancel(self.handle, rid), "dr_serve_cancel")

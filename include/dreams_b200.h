@@ -99,8 +99,12 @@ typedef struct dr_walk_desc {
 #define DR_ENGINE_AUTO    0   /* planned fast path (difference tables), else
                                  the per-step interpreter                    */
 #define DR_ENGINE_INTERP  1   /* per-step bytecode interpreter, chunked      */
-#define DR_ENGINE_PLAIN   2   /* one walk per launch, per-step interpreter,
-                                 no depth chunks (the baseline path)         */
+#define DR_ENGINE_PLAIN   2   /* the baseline path: the same per-class step
+                                 code as AUTO, but no depth chunks and no
+                                 persistent grid -- one single-warp block per
+                                 (walk, block of 32 primes) runs the whole
+                                 depth; a batch of one walk is one walk per
+                                 launch (K/32 warps)                         */
 
 typedef struct dr_tune {
     uint32_t chunk_steps;     /* depth-chunk length; 0 = autotuned           */
@@ -121,6 +125,18 @@ int dr_version(void);
 /* The first K primes below 2^31 in descending order (reference
  * runner.py:33-52 generate_rns_primes). */
 int dr_prime_table(int K, uint32_t *out);
+
+/* Per-stage timers of the calls below, summed since the last reset (no
+ * reference counterpart; the reference only prints wall-clock rates):
+ * ms_out[0] host batch build (planning, tiles, launch geometry), [1]
+ * allocation and upload, [2] run (enqueue; the wait as well in
+ * dr_walk_batch), [3] read-back, [4] device milliseconds of the batch runs
+ * read back (CUDA events).  calls_out (may be NULL) counts each stage's
+ * entries.  Fills min(n, 5) entries; reset != 0 zeroes the sums after
+ * reading them.  The stages are also NVTX ranges ("dr.build", "dr.upload",
+ * "dr.run", "dr.read", "dr.serve.wave") for a profiler's timeline.          */
+#define DR_STAGE_COUNT 5
+int dr_stage_times(double *ms_out, uint64_t *calls_out, int32_t n, int32_t reset);
 
 /* Validate a program blob (reference compiler.py:64-89 layout) and report how
  * the engine will run it: *cls_out = 1 companion polynomial, 2 companion
@@ -257,9 +273,19 @@ int dr_delta_batch(const uint32_t *p_limbs, const int32_t *p_sign, const uint32_
                    const uint32_t *lden_limbs, int32_t l_stride, int32_t per_item_target,
                    double *delta_out);
 
-/* Top-k by delta, highest first, ties by lower index (the reference's
- * threshold filter persistent_kernel.cu:796-841 kept no order). */
+/* Top-k by delta, highest first, NaN last, ties by lower index (the
+ * reference's threshold filter persistent_kernel.cu:796-841 kept no order).
+ * k <= 2048.  From 2^18 values on, a threshold taken from a strided sample
+ * lets one pass over the values keep only the candidates that can rank, so
+ * the values are read once; the result is exact (a count check falls back to
+ * sorting every value when the threshold kept too few or too many).       */
 int dr_topk(const double *delta, int32_t n, int32_t k, int32_t *idx_out, double *val_out);
+/* The same on device memory: delta_d[n] in, idx_d[min(k, n)] and val_d
+ * (either may be NULL) out, on `stream` (NULL: the engine's stream); returns
+ * after synchronising that stream.  *filtered (may be NULL) = 1 when the
+ * threshold filter decided the result.                                     */
+int dr_topk_device(const double *delta_d, int32_t n, int32_t k, int32_t *idx_d, double *val_d,
+                   void *stream, int32_t *filtered);
 
 /* ---- serving: continuous batching of walk requests ---------------------- */
 typedef struct dr_serve_config {

@@ -26,9 +26,10 @@ int dr_debug_sim_walk(const uint8_t *blob, uint64_t size, int32_t K, uint64_t de
  * (class, m, degree) program, or -1 when it runs on the interpreter. */
 int dr_debug_template_degree(int32_t cls, int32_t m, int32_t degree);
 
-/* Integer-pipe issue peak on the current device, lane-instructions per
- * second: kind 0 wide multiply-add, 1 add+min, 2 their 1:2 mix.  The
- * denominator of the walk kernels' roofline. */
+/* Integer-pipe issue peaks on the current device, lane-instructions per
+ * second: kind 0 wide multiply-add (mad.wide.u32), 1 add+min, 2 their 1:2
+ * mix, 3 low multiply-add (mad.lo.u32), 4 unsigned min.  The denominators of
+ * the walk kernels' per-pipe roofline. */
 int dr_bench_int_peak(int32_t kind, double *lane_ops_per_s);
 
 /* One uncaptured run of a prepared batch with its launch groups concurrent
@@ -46,6 +47,16 @@ int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t *n_laun
  * totals over all jobs.  Needs no GPU. */
 int dr_debug_host_pool(int32_t parts, uint64_t n, int32_t repeats, uint64_t *index_sum,
                        uint64_t *visits);
+
+/* *debug_checks = 1 in a DR_DEBUG build (libdreams_b200_debug.so, built by
+ * `python dreams-rns-cuda_b200/build.py --debug`), else 0.  A DR_DEBUG build
+ * re-checks on the device every index a walk tile takes from its batch's
+ * tables (walk, program, group, chunk slot, prime block, outputs, and each
+ * bytecode operand against its register, constant, axis and output rows)
+ * before using it; the first failure is recorded, the tile is skipped, and
+ * the next read of the batch returns DR_ERR_INDEX naming the site, index
+ * and bound.  No reference counterpart (the reference has no checks). */
+int dr_debug_build_info(int32_t *debug_checks);
 
 /* Host milliseconds (cumulative from the start) at the end of each phase of
  * the last dr_batch_create: programs, walks, tiles, shadow lists, launch
@@ -72,6 +83,18 @@ int dr_debug_rescale(const double *x, const double *b, int32_t n, double *out);
  * allocation and upload, and its kernel launches.  n_waves receives the
  * number recorded. */
 int dr_debug_serve_waves(int32_t server, int32_t max_waves, int32_t *n_waves, double *rows);
+
+/* Host-side fault injection in the serving loop (no GPU fault is involved):
+ * DR_INJECT_ADMIT_NOMEM makes the next `count` admissions fail as if
+ * allocating the request's resident state had failed; DR_INJECT_WAVE_NOMEM
+ * makes the next `count` wave launches fail as if growing their device
+ * buffers had failed.  Each affected request ends with DR_ERR_NOMEM from
+ * dr_serve_poll, keeps no slots or admitted bytes, and the server goes on
+ * with the others.  kind 0 changes nothing.  *failed (may be NULL) receives
+ * the number of requests that have ended with an error of their own.     */
+#define DR_INJECT_ADMIT_NOMEM 1
+#define DR_INJECT_WAVE_NOMEM  2
+int dr_debug_serve_inject(int32_t server, int32_t kind, int32_t count, uint64_t *failed);
 
 #ifdef __cplusplus
 }

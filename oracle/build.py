@@ -22,7 +22,7 @@ def build(force: bool = False) -> str:
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= os.path.getmtime(SRC):
         return LIB
     cmd = ["gcc", "-O2", "-std=gnu11", "-fPIC", "-shared", "-ffp-contract=off",
-           SRC, "-o", LIB, "-lm"]
+           SRC, "-o", LIB, "-lm", "-lpthread"]
     subprocess.run(cmd, check=True)
     return LIB
 

@@ -21,11 +21,12 @@ def lib():
         if not os.path.exists(path):
             path = _build.build()
         L = ctypes.CDLL(path)
-        L.oracle_walk.restype = ctypes.c_int
-        L.oracle_walk.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int,
-                                  ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
-                                  ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
-                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.oracle_walk_mt.restype = ctypes.c_int
+        L.oracle_walk_mt.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.c_int,
+                                     ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+                                     ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                     ctypes.c_int]
         _lib = L
     return _lib
 
@@ -34,17 +35,29 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def default_threads() -> int:
+    """Host threads for the prime walks: every core this process may use."""
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except (AttributeError, OSError):
+        return max(1, os.cpu_count() or 1)
+
+
 def walk(blob: bytes, depth: int, K: int, axis: np.ndarray, init: np.ndarray,
-         prow: int, qrow: int, shadow: bool = True):
-    """Residues of P[prow][m-1], P[qrow][m-1] after ``depth`` steps (+ shadow)."""
+         prow: int, qrow: int, shadow: bool = True, threads: Optional[int] = None):
+    """Residues of P[prow][m-1], P[qrow][m-1] after ``depth`` steps (+ shadow).
+    The K prime walks run on ``threads`` host threads (default: all cores);
+    the result does not depend on the thread count."""
     pp = primes(K).astype(np.uint32)
     p_out = np.zeros(K, dtype=np.uint32)
     q_out = np.zeros(K, dtype=np.uint32)
     sh = np.zeros(3, dtype=np.float64)
     axis = np.ascontiguousarray(axis, dtype=np.int64)
     init = np.ascontiguousarray(init, dtype=np.int64)
-    rc = lib().oracle_walk(blob, len(blob), K, _ptr(pp), int(depth), _ptr(axis), _ptr(init),
-                           prow, qrow, _ptr(p_out), _ptr(q_out), _ptr(sh) if shadow else None)
+    nt = default_threads() if threads is None else int(threads)
+    rc = lib().oracle_walk_mt(blob, len(blob), K, _ptr(pp), int(depth), _ptr(axis), _ptr(init),
+                              prow, qrow, _ptr(p_out), _ptr(q_out), _ptr(sh) if shadow else None,
+                              nt)
     if rc:
         raise ValueError(f"oracle_walk failed ({rc})")
     return {"p_residues": p_out.astype(np.int64), "q_residues": q_out.astype(np.int64),
@@ -53,16 +66,16 @@ def walk(blob: bytes, depth: int, K: int, axis: np.ndarray, init: np.ndarray,
 
 
 def pcf_walk(blob: bytes, a0: int, depth: int, K: int = 32, shift: int = 1,
-             shadow: bool = True):
+             shadow: bool = True, threads: Optional[int] = None):
     """Same outputs as ``walk_np.pcf_walk`` (reference runner.py:338-413)."""
     m, dim, _, _, dirs = parse_blob(blob)
     axis = np.array([[shift, 1, d, 1] for d in dirs], dtype=np.int64).reshape(-1)
     init = np.array([[1, a0], [0, 1]], dtype=np.int64)
-    return walk(blob, depth, K, axis, init, 0, 1, shadow)
+    return walk(blob, depth, K, axis, init, 0, 1, shadow, threads)
 
 
 def cmf_walk(blob: bytes, depth: int, K: int, shift_vals, trajectory_vals=None,
-             shadow: bool = True):
+             shadow: bool = True, threads: Optional[int] = None):
     """Same outputs as ``walk_np.cmf_walk`` (reference cmf_walk.py:363-431)."""
     m, dim, _, _, dirs = parse_blob(blob)
     sn, sd = _rationals(shift_vals)
@@ -73,4 +86,4 @@ def cmf_walk(blob: bytes, depth: int, K: int, shift_vals, trajectory_vals=None,
     axis = np.array([[sn[a], sd[a], tn[a], td[a]] for a in range(dim)],
                     dtype=np.int64).reshape(-1)
     init = np.eye(m, dtype=np.int64)
-    return walk(blob, depth, K, axis, init, 0, m - 1, shadow)
+    return walk(blob, depth, K, axis, init, 0, m - 1, shadow, threads)

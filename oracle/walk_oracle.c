@@ -11,6 +11,7 @@
  * Only the tests and the benchmark's CPU legs load this file's library.
  */
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -57,6 +58,32 @@ static int parse(const uint8_t *blob, size_t len, prog_t *p) {
 
 #define MAXR 512
 
+/* One past the highest register index the program names (operands the
+ * interpreter reads or writes), so a step clears only those registers.
+ * Clearing all MAXR registers, as the reference allocates them
+ * (runner.py:217), gives the same values.  0 = some index is >= MAXR (the
+ * reference's register list raises IndexError there). */
+static uint32_t reg_span(const prog_t *pr) {
+    uint32_t hi = 1;
+    for (uint32_t pc = 0; pc < pr->n_ops; ++pc) {
+        const insn_t in = pr->ops[pc];
+        uint32_t r[3] = {0, 0, 0};
+        switch (in.op) {
+        case LOAD_X: case LOAD_C: r[0] = in.a1; break;
+        case LOAD_N: r[0] = in.a0; break;
+        case ADD: case SUB: case MUL: r[0] = in.a0; r[1] = in.a1; r[2] = in.a2; break;
+        case NEG: case POW2: case POW3: case INV: r[0] = in.a0; r[1] = in.a1; break;
+        case STORE: r[0] = in.a0; break;
+        default: break;
+        }
+        for (int i = 0; i < 3; ++i) {
+            if (r[i] >= MAXR) return 0;   /* out of range: the caller reports it */
+            if (r[i] + 1 > hi) hi = r[i] + 1;
+        }
+    }
+    return hi;
+}
+
 /* Residue walk for one prime.  axis: 4 int64 per axis (sn, sd, tn, td).
  * init: m*m int64 initial matrix.  Writes the full final P (m*m) into out. */
 static int walk_prime(const prog_t *pr, uint64_t p, int64_t depth, const int64_t *axis,
@@ -72,8 +99,10 @@ static int walk_prime(const prog_t *pr, uint64_t p, int64_t depth, const int64_t
     }
     for (uint32_t i = 0; i < pr->n_consts; ++i) cst[i] = (uint64_t)mod_i128(pr->consts[i], (int64_t)p);
     for (int i = 0; i < m * m; ++i) P[i] = (uint64_t)mod_i128(init[i], (int64_t)p);
+    const uint32_t nr = reg_span(pr);
+    if (!nr) return -3;
     for (int64_t s = 0; s < depth; ++s) {
-        memset(regs, 0, sizeof(regs));
+        memset(regs, 0, sizeof(uint64_t) * nr);   /* fresh zero registers every step */
         memset(M, 0, sizeof(uint64_t) * m * m);
         for (uint32_t pc = 0; pc < pr->n_ops; ++pc) {
             const insn_t in = pr->ops[pc];
@@ -126,10 +155,12 @@ static int walk_shadow(const prog_t *pr, int64_t depth, const int64_t *axis, con
     const int m = (int)pr->m;
     double P[256], M[256], C[256], regs[MAXR];
     double log_scale = 0.0;
+    const uint32_t nr = reg_span(pr);
+    if (!nr) return -3;
     for (int i = 0; i < m * m; ++i) P[i] = (double)init[i];
     for (int64_t s = 0; s < depth; ++s) {
         memset(M, 0, sizeof(double) * m * m);
-        for (int r = 0; r < MAXR; ++r) regs[r] = 0.0;
+        for (uint32_t r = 0; r < nr; ++r) regs[r] = 0.0;
         for (uint32_t pc = 0; pc < pr->n_ops; ++pc) {
             const insn_t in = pr->ops[pc];
             if (in.op == END) break;
@@ -181,19 +212,66 @@ static int walk_shadow(const prog_t *pr, int64_t depth, const int64_t *axis, con
  * for each of the K primes, and optionally the float shadow.
  * Returns 0, or a negative code for a malformed program.
  */
+typedef struct {
+    const prog_t *pr;
+    const uint32_t *primes;
+    int K, prow, qrow, first, step;
+    int64_t depth;
+    const int64_t *axis, *init;
+    uint32_t *p_out, *q_out;
+    int rc;
+} prime_job_t;
+
+static void *prime_worker(void *arg) {
+    prime_job_t *j = (prime_job_t *)arg;
+    uint64_t P[256];
+    const int m = (int)j->pr->m;
+    j->rc = 0;
+    for (int k = j->first; k < j->K; k += j->step) {
+        int rc = walk_prime(j->pr, j->primes[k], j->depth, j->axis, j->init, P);
+        if (rc) { j->rc = rc; return NULL; }
+        j->p_out[k] = (uint32_t)P[j->prow * m + m - 1];
+        j->q_out[k] = (uint32_t)P[j->qrow * m + m - 1];
+    }
+    return NULL;
+}
+
+/*
+ * oracle_walk_mt: oracle_walk with the primes spread over `threads` POSIX
+ * threads (prime k on thread k mod threads; every prime's walk is
+ * independent, so the outputs do not depend on the thread count).
+ */
+int oracle_walk_mt(const uint8_t *blob, uint64_t blob_len, int K, const uint32_t *primes,
+                   int64_t depth, const int64_t *axis, const int64_t *init, int prow, int qrow,
+                   uint32_t *p_out, uint32_t *q_out, double *shadow_out, int threads) {
+    prog_t pr;
+    if (parse(blob, (size_t)blob_len, &pr)) return -1;
+    if (threads < 1) threads = 1;
+    if (threads > K) threads = K > 0 ? K : 1;
+    if (threads > 256) threads = 256;
+    prime_job_t jobs[256];
+    pthread_t tids[256];
+    int started[256];
+    for (int t = 0; t < threads; ++t) {
+        jobs[t] = (prime_job_t){&pr, primes, K, prow, qrow, t, threads, depth, axis, init,
+                                p_out, q_out, 0};
+        started[t] = (t > 0) && pthread_create(&tids[t], NULL, prime_worker, &jobs[t]) == 0;
+        if (t > 0 && !started[t]) prime_worker(&jobs[t]);   /* no thread: run it here */
+    }
+    int rc_sh = 0;
+    if (shadow_out) rc_sh = walk_shadow(&pr, depth, axis, init, prow, qrow, shadow_out);
+    prime_worker(&jobs[0]);
+    int rc = 0;
+    for (int t = 0; t < threads; ++t) {
+        if (started[t]) pthread_join(tids[t], NULL);
+        if (!rc && jobs[t].rc) rc = jobs[t].rc;
+    }
+    return rc ? rc : rc_sh;
+}
+
 int oracle_walk(const uint8_t *blob, uint64_t blob_len, int K, const uint32_t *primes,
                 int64_t depth, const int64_t *axis, const int64_t *init, int prow, int qrow,
                 uint32_t *p_out, uint32_t *q_out, double *shadow_out) {
-    prog_t pr;
-    if (parse(blob, (size_t)blob_len, &pr)) return -1;
-    uint64_t P[256];
-    const int m = (int)pr.m;
-    for (int k = 0; k < K; ++k) {
-        int rc = walk_prime(&pr, primes[k], depth, axis, init, P);
-        if (rc) return rc;
-        p_out[k] = (uint32_t)P[prow * m + m - 1];
-        q_out[k] = (uint32_t)P[qrow * m + m - 1];
-    }
-    if (shadow_out) return walk_shadow(&pr, depth, axis, init, prow, qrow, shadow_out);
-    return 0;
+    return oracle_walk_mt(blob, blob_len, K, primes, depth, axis, init, prow, qrow, p_out, q_out,
+                          shadow_out, 1);
 }

@@ -1,0 +1,74 @@
+"""The reference's batched GPU entry points (python/dreams_rns/gpu_walk.py:279-489)
+on the B200 engine: same result keys, every walk against the C oracle.
+
+Differences from the reference that are by design: every walk gets its own
+FP64 shadow (the reference reports the first walk's shadow for the whole
+batch, gpu_walk.py:345-363) and INV runs on the device.
+"""
+
+import numpy as np
+import pytest
+
+import dreams_rns as dr
+from oracle import walk_c
+
+pytestmark = pytest.mark.gpu
+
+PCF_KEYS = {"p_residues", "q_residues", "p_float", "q_float", "log_scale", "primes", "shift_val"}
+CMF_KEYS = {"p_residues", "q_residues", "p_float", "q_float", "log_scale", "primes", "shift_vals"}
+
+
+def _close(a, b, rtol=1e-12):
+    return a == b or abs(a - b) <= rtol * max(abs(a), abs(b), 1e-300)
+
+
+def test_run_pcf_walk_batch_gpu_matches_oracle():
+    prog = dr.compile_pcf("3*n + 1", "-2*n**2 + n")
+    shifts = [1, 2, 5, -3, 17, 0]
+    out = dr.run_pcf_walk_batch_gpu(prog, 1, 1500, 48, shift_vals=shifts, batch_size=4)
+    assert len(out) == len(shifts)
+    for sv, r in zip(shifts, out):
+        assert set(r) == PCF_KEYS
+        assert r["shift_val"] == sv
+        assert r["p_residues"].dtype == np.int64 and r["p_residues"].shape == (48,)
+        o = walk_c.pcf_walk(prog.serialize(), 1, 1500, 48, shift=sv)
+        assert list(r["p_residues"]) == list(o["p_residues"]), sv
+        assert list(r["q_residues"]) == list(o["q_residues"]), sv
+        assert list(r["primes"]) == list(o["primes"])
+        assert _close(r["p_float"], o["p_float"]) and _close(r["q_float"], o["q_float"]), sv
+        assert _close(r["log_scale"], o["log_scale"], 1e-13), sv
+    single = dr.run_pcf_walk_gpu(prog, 1, 1500, 48, shift_val=5)
+    assert list(single["p_residues"]) == list(out[2]["p_residues"])
+    with pytest.raises(AssertionError):
+        dr.run_pcf_walk_batch_gpu(dr.compile_cmf_from_dict({(0, 0): "x0"}, 1, 1), 0, 10, 8)
+
+
+def test_run_cmf_walk_batch_gpu_matches_oracle():
+    mat = {(0, 2): "x*y + z", (1, 0): "1", (1, 2): "x - 2*z**2", (2, 1): "1", (2, 2): "x + y + z"}
+    prog = dr.compile_cmf_from_dict(mat, m=3, dim=3, axis_names=["x", "y", "z"])
+    shifts = [[1, 1, 1], [2, -1, 0], [0, 3, -2], [-3, -3, 1]]
+    out = dr.run_cmf_walk_batch_gpu(prog, 900, 40, shift_val_list=shifts, batch_size=2)
+    assert len(out) == len(shifts)
+    for sv, r in zip(shifts, out):
+        assert set(r) == CMF_KEYS
+        assert r["shift_vals"] == sv
+        o = walk_c.cmf_walk(prog.serialize(), 900, 40, sv)
+        assert list(r["p_residues"]) == list(o["p_residues"]), sv
+        assert list(r["q_residues"]) == list(o["q_residues"]), sv
+        assert _close(r["p_float"], o["p_float"]) and _close(r["q_float"], o["q_float"]), sv
+    one = dr.run_cmf_walk_gpu(prog, 900, 40, shifts[1])
+    assert list(one["q_residues"]) == list(out[1]["q_residues"])
+
+
+def test_stage_times_cover_a_sweep():
+    """The per-stage timers see every stage of one sweep() call."""
+    from dreams_rns.engine import pcf_request
+    prog = dr.compile_pcf("2", "n**2")
+    reqs = [pcf_request(prog, 2, 2000, 32, shift_val=s, checkpoint=500) for s in (1, 2, 3, 4)]
+    dr.stage_times(reset=True)
+    out = dr.sweep(reqs, delta="self", topk=2)
+    st = dr.stage_times(reset=True)
+    assert len(out["topk_idx"]) == 2
+    for k in ("pack", "build", "upload", "run", "read", "device"):
+        assert st[f"{k}_calls"] >= 1 and st[f"{k}_ms"] > 0, (k, st)
+    assert dr.stage_times()["build_calls"] == 0

@@ -113,3 +113,60 @@ def test_short_requests_overtake_a_long_one():
     assert np.all(gpu_ms > 0) and np.all(n_req >= 1)
     assert set(np.unique(has_long)) <= {0.0, 1.0} and has_long.max() == 1.0
     assert np.all((slot >= 0) & (slot < 3))
+
+
+def _collect(srv, ids, timeout=120.0):
+    """Poll every request to its end: results, and the ids that raised
+    MemoryError (requests whose allocation failed)."""
+    got, failed = {}, []
+    left = list(ids)
+    t0 = time.monotonic()
+    while left:
+        nxt = []
+        for rid in left:
+            try:
+                r = srv.poll(rid)
+            except MemoryError:
+                failed.append(rid)
+                continue
+            if r is None:
+                nxt.append(rid)
+            else:
+                got[rid] = r
+        left = nxt
+        assert time.monotonic() - t0 < timeout, f"{len(left)} requests still running"
+        time.sleep(0.0005)
+    return got, failed
+
+
+def test_injected_allocation_failures():
+    """Host-side fault injection: admissions and a wave launch whose device
+    allocation fails end their requests with MemoryError; every other
+    request completes with the batch's results, the server keeps serving
+    and its accounting returns to zero."""
+    reqs = _mix(9, n=16)
+    batch = run_walks(reqs)
+    with WalkServer(max_inflight=2) as srv:
+        assert srv.inject_failures(admissions=2) == 0
+        ids = [srv.submit(r) for r in reqs]
+        got, failed = _collect(srv, ids)
+        assert len(failed) == 2
+        for i, rid in enumerate(ids):
+            if rid in got:
+                _same(got[rid], batch[i])
+        st = srv.stats()
+        assert st["admitted_bytes"] == 0 and st["queue_depth"] == 0
+        # a wave whose buffers cannot grow: only its own requests fail
+        srv.inject_failures(waves=1)
+        ids2 = [srv.submit(r) for r in reqs[:8]]
+        got2, failed2 = _collect(srv, ids2)
+        assert len(failed2) >= 1
+        for i, rid in enumerate(ids2):
+            if rid in got2:
+                _same(got2[rid], batch[i])
+        # and the server still serves
+        rid = srv.submit(reqs[0])
+        _same(srv.wait([rid])[rid], batch[0])
+        st = srv.stats()
+        assert st["admitted_bytes"] == 0 and st["queue_depth"] == 0
+        assert srv.inject_failures() == 2 + len(failed2)

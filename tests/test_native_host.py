@@ -280,3 +280,32 @@ def test_read_pipeline_limb_stride_from_descriptors(monkeypatch):
         assert len(out["p"]) == len(out["cp_q"]) == 3
     finally:
         b.handle = 0
+
+
+def test_stage_timers_need_no_gpu(L):
+    """dr_stage_times reads and resets the per-stage sums without a device;
+    a batch call that fails before building adds nothing to them."""
+    ms = (ctypes.c_double * 5)()
+    calls = (ctypes.c_uint64 * 5)()
+    L.dr_stage_times.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32]
+    assert L.dr_stage_times(ms, calls, 5, 1) == 0
+    assert L.dr_stage_times(ms, calls, 5, 0) == 0
+    assert list(calls) == [0] * 5 and list(ms) == [0.0] * 5
+    assert L.dr_stage_times(None, None, 5, 0) != 0          # null output
+    assert L.dr_stage_times(ms, None, -1, 0) != 0           # negative count
+    assert L.dr_stage_times(ms, None, 2, 0) == 0            # a prefix is fine
+
+
+def test_debug_build_exports_the_same_symbols():
+    """The DR_DEBUG library (build.py --debug) offers the same C ABI and
+    reports its checks; the normal one reports none."""
+    dbg = os.path.join(os.path.dirname(native_lib_path()), "libdreams_b200_debug.so")
+    if not os.path.exists(dbg):
+        pytest.skip("debug library not built")
+    names = _declared("dreams_b200.h") + _declared("dreams_b200_debug.h")
+    D = ctypes.CDLL(dbg)
+    assert [n for n in names if not hasattr(D, n)] == []
+    flag = ctypes.c_int32(-1)
+    assert D.dr_debug_build_info(ctypes.byref(flag)) == 0 and flag.value == 1
+    R = ctypes.CDLL(native_lib_path())
+    assert R.dr_debug_build_info(ctypes.byref(flag)) == 0 and flag.value == 0
