@@ -269,9 +269,9 @@ class ClockSampler:
 
 def companion_op_split(D: int, m: int):
     """Integer lane-instructions one prime-step of the difference-table
-    companion step needs, by the pipe that can execute them on B200 (ncu
-    assigns mad.wide.u32 to the ALU pipe and the low multiply to the FMA pipe,
-    profiles/int_pipes_microbench.md):
+    companion step needs, by the pipe that can execute them on B200 (ncu's
+    pipe counters on the dr_bench_int_peak kernels put mad.wide.u32 on the ALU
+    pipe and the low multiply mad.lo.u32 on the FMA pipe):
       wide  m+1 per last-column entry: its m products and the Montgomery
             reduction's q*p (ALU only)
       low   1 per entry: the reduction's quotient q = t*(-p^-1) (FMA only)

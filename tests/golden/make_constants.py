@@ -11,7 +11,9 @@ import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_constants.py <reference checkout>")
+ref = sys.argv[1]
 sys.path.insert(0, os.path.join(ref, "python"))
 from dreams_rns import constants as C  # noqa: E402  (the reference package)
 

@@ -12,7 +12,9 @@ import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_estimate_k.py <reference checkout>")
+ref = sys.argv[1]
 sys.path.insert(0, os.path.join(ref, "python"))
 spec = importlib.util.spec_from_file_location(
     "euler2ai_full_verify", os.path.join(ref, "python", "euler2ai_full_verify.py"))

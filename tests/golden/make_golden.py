@@ -2,7 +2,7 @@
 
 Run in a container where the reference checkout is mounted read-only::
 
-    python tests/golden/make_golden.py /root/reference/python
+    python tests/golden/make_golden.py <reference checkout>/python
 
 It imports the reference ``dreams_rns`` package (numpy / sympy / mpmath only)
 and records, for seeded and hand-picked inputs, what the reference computes:
@@ -289,4 +289,6 @@ def main(ref_python: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/python")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <reference checkout>/python")
+    main(sys.argv[1])
