@@ -232,7 +232,7 @@ void devcache_put(void* p, size_t bytes) {
 }
 
 Batch::Batch() {
-    for (DevBuf* b : {&progs, &code, &consts, &walks, &axis, &tiles, &groups, &group_done, &chunkP,
+    for (DevBuf* b : {&tables, &progs, &code, &consts, &walks, &axis, &tiles, &groups, &group_done, &chunkP,
                       &chunkSig, &shadow_list, &queues, &res, &shadow, &status, &mf, &eval_items,
                       &shadow_state, &tstamps, &crt_in, &crt_out, &limbs, &signs, &delta, &tgt_num,
                       &tgt_den, &tgt_sign, &tk_keys[0], &tk_keys[1], &tk_idx[0], &tk_idx[1],
@@ -332,8 +332,12 @@ uint32_t chunk_policy(uint64_t total_group_steps, uint64_t n_groups, int sms, co
 
 }  // namespace
 
-// host time of the phases of the last batch_build (diagnostics)
-static double g_build_ms[8];
+// host time of the phases of the last batch_build (diagnostics): plan
+// lookup, descriptors, code copy, walks, workload shape, tile count, tile
+// fill, tile order, shadow lists, geometry, table copy, buffers and
+// events, final sync
+constexpr int kBuildPhases = 13;
+static double g_build_ms[kBuildPhases];
 static std::chrono::steady_clock::time_point g_build_t0;
 static void build_mark(int i) {
     const auto t = std::chrono::steady_clock::now();
@@ -428,6 +432,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         else plan_range(0, 0, (size_t)n_programs);
         if ((rc = first_error(perr))) return rc;
     }
+    build_mark(1);
     // descriptors and offsets (serial, cheap); programs with the same
     // instruction streams share one copy of them
     std::vector<uint8_t> copy_code(n_programs, 0);     // first program of its code_id
@@ -470,6 +475,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         set_error("programs too large: more than 2^32 instructions or constants");
         return DR_ERR_UNSUPPORTED;
     }
+    build_mark(2);
     // the instruction streams (Insn and uint4 are both four 32-bit words) and
     // constants, copied on the host pool
     static_assert(sizeof(Insn) == sizeof(uint4), "instruction layout");
@@ -493,7 +499,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         else copy_range(0, 0, (size_t)n_programs);
     }
 
-    build_mark(1);
+    build_mark(3);
     // ---- walks
     std::vector<DevWalk> dwalks(n_walks);
     uint64_t total_group_steps = 0, n_groups = 0;
@@ -592,7 +598,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         }
     }
 
-    build_mark(2);
+    build_mark(4);
     // ---- tiles and groups
     const bool plain = engine == DR_ENGINE_PLAIN;
     // workload shape for the autotuner: per launch key, log2 buckets of the
@@ -625,6 +631,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
                    std::to_string(lg(kv.second.second));
         B->signature = sig;
     }
+    build_mark(5);
     // an autotuned choice for this shape applies unless the caller fixed one
     uint32_t tuned_chunk = 0, tuned_wpb = 0;
     if (!plain && !(tune && (tune->chunk_steps || tune->warps_per_block))) {
@@ -694,6 +701,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     };
     if (tparts > 1) host_pool().run(tparts, (size_t)n_walks, count_range);
     else count_range(0, 0, (size_t)n_walks);
+    build_mark(6);
     std::map<LaunchKey, std::vector<DevTile>> tile_sets;
     std::map<LaunchKey, Rows> key_rows;
     uint64_t n_group_total = 0, slots64 = 0;
@@ -782,6 +790,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     };
     if (tparts > 1) host_pool().run(tparts, (size_t)n_walks, fill_range);
     else fill_range(0, 0, (size_t)n_walks);
+    build_mark(7);
     size_t n_tiles_est = 0;
     for (auto& kv : tile_sets) n_tiles_est += kv.second.size();
     std::vector<DevTile> tiles;
@@ -809,7 +818,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     B->n_tiles = (uint32_t)tiles.size();
     B->n_groups = (uint32_t)groups.size();
 
-    build_mark(3);
+    build_mark(8);
     // ---- shadow work lists
     std::map<LaunchKey, std::vector<uint32_t>> shadow_sets;
     {
@@ -881,7 +890,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         B->launches.push_back(L);
     }
 
-    build_mark(4);
+    build_mark(9);
     // ---- launch geometry
     // expected duration of the walk kernels: algorithmic lane-ops per
     // prime-step (difference-table streams, product, reduction; the bytecode
@@ -959,22 +968,55 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     }
     B->n_queues = q;
 
-    build_mark(5);
+    build_mark(10);
     nvtx_build.end();
     NvtxRange nvtx_upload("dr.upload");
     const auto t_upload0 = std::chrono::steady_clock::now();
     // ---- upload
     cudaStream_t st = C.stream;
-    if ((rc = upload(B->progs, dprogs, st))) return rc;
-    if ((rc = upload(B->code, code, st))) return rc;
-    if ((rc = upload(B->consts, consts, st))) return rc;
-    if ((rc = upload(B->walks, dwalks, st))) return rc;
-    std::vector<int64_t> ax(axis, axis + n_axis);
-    if ((rc = upload(B->axis, ax, st))) return rc;
-    if ((rc = upload(B->tiles, tiles, st))) return rc;
-    if ((rc = upload(B->groups, groups, st))) return rc;
-    if ((rc = upload(B->shadow_list, shadow_list, st))) return rc;
-    if ((rc = upload(B->eval_items, eval_items, st))) return rc;
+    // The tables go up as one copy from the context's pinned staging buffer
+    // (pageable copies cost a staging pass and a call each); the batch's
+    // buffers are views into one device allocation.  stage_mu stays held
+    // until the stream sync below, which the copy must pass before the
+    // buffer is refilled.
+    std::unique_lock<std::mutex> stage_lk(C.stage_mu);
+    {
+        struct Part { DevBuf* b; const void* src; size_t n; };
+        const Part parts[] = {
+            {&B->progs, dprogs.data(), sizeof(DevProgram) * dprogs.size()},
+            {&B->code, code.data(), sizeof(uint4) * code.size()},
+            {&B->consts, consts.data(), sizeof(int64_t) * consts.size()},
+            {&B->walks, dwalks.data(), sizeof(DevWalk) * dwalks.size()},
+            {&B->axis, axis, sizeof(int64_t) * n_axis},
+            {&B->tiles, tiles.data(), sizeof(DevTile) * tiles.size()},
+            {&B->groups, groups.data(), sizeof(DevGroup) * groups.size()},
+            {&B->shadow_list, shadow_list.data(), sizeof(DevShadowSeg) * shadow_list.size()},
+            {&B->eval_items, eval_items.data(), sizeof(uint32_t) * eval_items.size()},
+        };
+        constexpr size_t kParts = sizeof(parts) / sizeof(parts[0]);
+        constexpr size_t kAlign = 256;
+        size_t offs[kParts], total = 0;
+        for (size_t i = 0; i < kParts; ++i) {
+            offs[i] = total;
+            total += (std::max<size_t>(parts[i].n, 16) + kAlign - 1) / kAlign * kAlign;
+        }
+        DR_CUDA(B->tables.alloc(total));
+        if (C.stage_bytes < total) {
+            if (C.stage_host) DR_CUDA(cudaFreeHost(C.stage_host));
+            C.stage_host = nullptr;
+            C.stage_bytes = 0;
+            const size_t cap = std::max<size_t>(total + total / 4, 1u << 20);
+            DR_CUDA(cudaMallocHost(&C.stage_host, cap));
+            C.stage_bytes = cap;
+        }
+        uint8_t* h = static_cast<uint8_t*>(C.stage_host);
+        for (size_t i = 0; i < kParts; ++i)
+            if (parts[i].n) std::memcpy(h + offs[i], parts[i].src, parts[i].n);
+        DR_CUDA(cudaMemcpyAsync(B->tables.p, h, total, cudaMemcpyHostToDevice, st));
+        uint8_t* d = static_cast<uint8_t*>(B->tables.p);
+        for (size_t i = 0; i < kParts; ++i) parts[i].b->set_view(d + offs[i], std::max<size_t>(parts[i].n, 16));
+    }
+    build_mark(11);
     DR_CUDA(B->mf.alloc(8ull * std::max<uint64_t>(mf_doubles, 1)));
     DR_CUDA(B->shadow_state.alloc(8ull * kShadowStateStride * std::max<uint32_t>(state_slots, 1)));
     DR_CUDA(B->group_done.alloc(4ull * std::max<uint32_t>(B->n_groups, 1)));
@@ -1017,9 +1059,9 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         if (B->launches[i].kind == 1 || (B->launches[i].kind == 2 && !B->launches[i].lean))
             DR_CUDA(cudaEventCreateWithFlags(&B->evals[i], cudaEventDisableTiming));
     for (auto& e : B->joins) DR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    build_mark(6);
+    build_mark(12);
     DR_CUDA(cudaStreamSynchronize(st));
-    build_mark(7);
+    build_mark(13);
     {
         using ms = std::chrono::duration<double, std::milli>;
         const auto t_end = std::chrono::steady_clock::now();
@@ -1344,6 +1386,9 @@ static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, Shado
     unsigned long long* ts = B.stamping ? B.tstamps.as<unsigned long long>() + 4 * (&L - B.launches.data()) : nullptr;
     wa.tstamp = ts;
     sa.tstamp = ts;
+    sa.item_log = (B.stamping && L.kind == 2)
+                      ? B.item_log.as<unsigned long long>() + 4ull * B.item_log_off[&L - B.launches.data()]
+                      : nullptr;
     if (L.kind == 0) {
         wa.tiles = B.tiles.as<DevTile>() + L.off;
         wa.n_tiles = L.count;
@@ -1399,15 +1444,19 @@ static int enqueue_batch(Batch& B, cudaStream_t st, std::vector<cudaEvent_t>* en
     size_t k_lo = 0, k_hi = 0;
     cudaStream_t prev = nullptr;
     int rc = DR_OK;
-    for (int pass = 0; pass < 2 && rc == DR_OK; ++pass) {
+    // Launch order: the integer-difference chains first (their blocks claim
+    // whole SMs, so they must be placed before the evaluation kernel fills
+    // the GPU), then the interpreted shadows, then the walks.
+    for (int pass = 0; pass < 3 && rc == DR_OK; ++pass) {
+        const int kind = pass == 0 ? 2 : pass == 1 ? 1 : 0;
         for (const LaunchSpec& L : B.launches) {
-            if ((L.items == 0 && L.items2 == 0) || (pass == 0) != (L.kind != 0)) continue;
+            if ((L.items == 0 && L.items2 == 0) || L.kind != kind) continue;
             cudaStream_t s = prev;
             if (!L.follow || !prev) {
-                s = pass == 0 ? take(C.hpool, k_hi) : take(C.pool, k_lo);
+                s = pass < 2 ? take(C.hpool, k_hi) : take(C.pool, k_lo);
                 // walks start once the step matrices are evaluated, so the
                 // shadow chains (high priority) are placed before them
-                if (s && pass == 1)
+                if (s && pass == 2)
                     for (size_t j = 0; j < B.launches.size(); ++j)
                         if ((B.launches[j].kind == 1 ||
                              (B.launches[j].kind == 2 && chain_first() && !B.launches[j].lean)) &&
@@ -1509,14 +1558,37 @@ int batch_timeline(Batch& B, std::vector<float>* out) {
     }
     DR_CUDA(B.tstamps.alloc(8 * h.size()));
     DR_CUDA(cudaMemcpy(B.tstamps.p, h.data(), 8 * h.size(), cudaMemcpyHostToDevice));
+    // per chain item of the integer-difference launches: 4 words each
+    B.item_log_off.assign(n, 0);
+    uint32_t n_items = 0;
+    for (size_t i = 0; i < n; ++i) {
+        B.item_log_off[i] = n_items;
+        if (B.launches[i].kind == 2) n_items += B.launches[i].items;
+    }
+    DR_CUDA(B.item_log.alloc(32ull * std::max<uint32_t>(n_items, 1)));
+    DR_CUDA(cudaMemset(B.item_log.p, 0, 32ull * std::max<uint32_t>(n_items, 1)));
     B.stamping = true;
     int rc = enqueue_batch(B, st);
     B.stamping = false;
     if (rc) return rc;
     DR_CUDA(cudaStreamSynchronize(st));
     DR_CUDA(cudaMemcpy(h.data(), B.tstamps.p, 8 * h.size(), cudaMemcpyDeviceToHost));
+    std::vector<unsigned long long> il(4ull * n_items);
+    if (n_items) DR_CUDA(cudaMemcpy(il.data(), B.item_log.p, 8 * il.size(), cudaMemcpyDeviceToHost));
     unsigned long long t0 = ~0ull;
     for (size_t i = 0; i < 2 * n; ++i) t0 = std::min(t0, h[2 * i]);
+    // items: launch, start, tables built, end (ms after t0), re-run chunks, exact steps
+    B.item_rows.clear();
+    for (size_t i = 0; i < n; ++i) {
+        if (B.launches[i].kind != 2) continue;
+        for (uint32_t k = 0; k < B.launches[i].items; ++k) {
+            const unsigned long long* r = &il[4ull * (B.item_log_off[i] + k)];
+            if (!r[0] || r[0] < t0) continue;
+            B.item_rows.insert(B.item_rows.end(),
+                               {(float)i, (float)((r[0] - t0) * 1e-6), (float)((r[1] - t0) * 1e-6),
+                                (float)((r[2] - t0) * 1e-6), (float)(r[3] >> 32), (float)(r[3] & 0xffffffffu)});
+        }
+    }
     out->assign(4 * n, -1.f);
     for (size_t i = 0; i < 2 * n; ++i)
         if (h[2 * i] != ~0ull) {
@@ -2064,7 +2136,7 @@ int dr_debug_host_pool(int32_t parts, uint64_t n, int32_t repeats, uint64_t* ind
 }
 
 int dr_debug_build_phases(double* ms, int32_t n) {
-    for (int i = 0; i < n && i < 7; ++i) ms[i] = g_build_ms[i];
+    for (int i = 0; i < n && i < kBuildPhases; ++i) ms[i] = g_build_ms[i];
     return DR_OK;
 }
 
@@ -2085,6 +2157,17 @@ int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t* n_laun
     if (n_launches) *n_launches = (int32_t)(t.size() / 4);
     for (int i = 0; i < (int)t.size() && i < 4 * max_launches; ++i)
         if (spans) spans[i] = t[i];
+    return DR_OK;
+}
+
+int dr_debug_chain_items(int32_t batch, int32_t max_items, int32_t* n_items, float* rows) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    Batch* B = find_batch(batch);
+    if (!B) return DR_ERR_HANDLE;
+    if (n_items) *n_items = (int32_t)(B->item_rows.size() / 6);
+    for (size_t i = 0; i < B->item_rows.size() && i < 6ull * std::max(max_items, 0); ++i)
+        if (rows) rows[i] = B->item_rows[i];
     return DR_OK;
 }
 

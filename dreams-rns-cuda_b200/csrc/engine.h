@@ -5,6 +5,7 @@
 #include <atomic>
 #include <condition_variable>
 #include <cstdint>
+#include <cstring>
 #include <functional>
 #include <map>
 #include <memory>
@@ -36,17 +37,25 @@ struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
     bool pooled = false;
+    bool view = false;   // p points into another buffer, which owns the memory
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) {
+        if (p && !view) {
             if (pooled) devcache_put(p, bytes);
             else cudaFree(p);
         }
         p = nullptr;
         bytes = 0;
+        view = false;
+    }
+    void set_view(void* q, size_t n) {
+        release();
+        p = q;
+        bytes = n;
+        view = true;
     }
     cudaError_t alloc(size_t n) {
         if (n <= bytes && p) return cudaSuccess;
@@ -96,6 +105,30 @@ class HostPool {
 // The context's pool (created on first use).
 HostPool& host_pool();
 
+// Hash of a program blob for the plan cache: eight bytes per round
+// (multiply, xor-shift), then the tail; several times faster than a
+// byte-wise string hash on the kilobyte-sized blobs a batch looks up.
+struct BlobHash {
+    size_t operator()(std::string_view s) const noexcept {
+        const uint64_t kMul = 0x9E3779B97F4A7C15ull;
+        uint64_t h = 0x243F6A8885A308D3ull ^ (uint64_t)s.size();
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(s.data());
+        size_t n = s.size();
+        while (n >= 8) {
+            uint64_t w;
+            std::memcpy(&w, p, 8);
+            h = (h ^ w) * kMul;
+            h ^= h >> 29;
+            p += 8;
+            n -= 8;
+        }
+        uint64_t w = 0;
+        std::memcpy(&w, p, n);
+        h = (h ^ w) * kMul;
+        return (size_t)(h ^ (h >> 32));
+    }
+};
+
 struct CrtSet {
     int K = 0, L = 0;
     DevBuf moduli, pinv, r2, ginv, Mlimbs, Mtotal;
@@ -113,7 +146,7 @@ struct Context {
     // plan cache keyed by program bytes (views into each Plan's own copy);
     // plan_mu guards it and code_ids (lookups shared, inserts exclusive)
     std::shared_mutex plan_mu;
-    std::unordered_map<std::string_view, std::shared_ptr<Plan>> plan_cache;
+    std::unordered_map<std::string_view, std::shared_ptr<Plan>, BlobHash> plan_cache;
     // interned instruction streams: programs that differ only in their
     // constants share one copy of device code in a batch
     std::unordered_map<std::string, uint32_t> code_ids;
@@ -123,6 +156,11 @@ struct Context {
     std::mutex cache_mu;
     std::multimap<size_t, void*> cache;   // free device blocks by size
     size_t cached_bytes = 0;
+    // pinned staging of a batch's tables: one host-to-device copy per build.
+    // stage_mu is held from filling it until the build's stream sync.
+    std::mutex stage_mu;
+    void* stage_host = nullptr;
+    size_t stage_bytes = 0;
 };
 
 Context* ctx();           // nullptr before dr_init
@@ -207,6 +245,7 @@ struct Batch {
     uint64_t n_code = 0, n_consts = 0, n_axis = 0;
     DevBuf dbg;                                   // DR_DEBUG builds: first failed device check
     uint32_t chunk_stride = 0;   // words per chunk-product slot
+    DevBuf tables;   // one copy of progs, code, consts, walks, axis, tiles, groups, shadow_list, eval_items
     DevBuf progs, code, consts, walks, axis, tiles, groups, group_done, chunkP, chunkSig;
     DevBuf shadow_list, queues, res, shadow, status;   // res: p residues then q residues
     DevBuf mf, eval_items, shadow_state;               // interpreted shadow
@@ -232,6 +271,9 @@ struct Batch {
     std::vector<cudaEvent_t> evals;     // per launch: its step-matrix evaluation is done
     DevBuf tstamps;                     // diagnostics: 4 timestamps per launch
     bool stamping = false;
+    DevBuf item_log;                    // diagnostics: per chain item of kind-2 launches
+    std::vector<uint32_t> item_log_off; // first item of each launch in item_log
+    std::vector<float> item_rows;       // last timeline's items (see dr_debug_chain_items)
     float last_ms = 0.f;
     bool has_shadow = false;
     std::string signature;              // autotuner cache key (workload shape)

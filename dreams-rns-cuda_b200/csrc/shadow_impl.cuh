@@ -70,6 +70,9 @@ struct ShadowArgs {
     uint32_t rows_regs;         // per-warp smem: doubles, 32 per row
     uint32_t rows_per_warp;
     uint32_t lean;              // chains co-located with walks: exact steps only
+    // diagnostics, integer-difference chains: per item [start ns, tables
+    // built ns, end ns, exact chunk re-runs << 32 | exact single steps], or null
+    unsigned long long* item_log;
 };
 
 constexpr int kShadowStateStride = 72;   // m*m <= 64 entries, then mantissa, exponent, nan flag
@@ -813,6 +816,9 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
         if (it >= A.n_items) break;
         const uint32_t first = it * 32;
         const uint32_t count = min(32u, A.n_list - first);
+        unsigned long long* ilog = A.item_log ? A.item_log + 4ull * it : nullptr;
+        uint32_t reruns = 0, exact_steps = 0;
+        if (ilog && lane == 0) ilog[0] = global_ns();
         // difference tables: lane j evaluates segment w's walk at step s0 + j
         for (uint32_t w = 0; w < count; ++w) {
             const DevShadowSeg g = A.segs[first + w];
@@ -830,8 +836,13 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
             }
             __syncwarp();
         }
+        // Lanes past the item's walks run a copy of lane 0's walk (same
+        // table, same steps) and drop its results.  Left at their start
+        // state, they made the whole warp of a partial item ~1.6x slower
+        // per step than the warps of full items.
         const bool active = (uint32_t)lane < count;
-        const DevShadowSeg g = A.segs[first + (active ? lane : 0)];
+        const int src = active ? lane : 0;
+        const DevShadowSeg g = A.segs[first + src];
         const uint32_t wi = g.walk;
         const DevWalk W = A.walks[wi];
         const DevProgram G = A.progs[W.prog];
@@ -839,7 +850,7 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
 #pragma unroll
         for (int j = 0; j <= D; ++j)
 #pragma unroll
-            for (int i = 0; i < NS; ++i) st.fd[i][j] = ((uint32_t)j <= G.degree && active) ? stage[(j * NS + i) * 32 + lane] : 0;
+            for (int i = 0; i < NS; ++i) st.fd[i][j] = ((uint32_t)j <= G.degree) ? stage[(j * NS + i) * 32 + src] : 0;
 #pragma unroll
         for (int lvl = 1; lvl <= D; ++lvl)
 #pragma unroll
@@ -848,7 +859,9 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
 #pragma unroll
                     for (int i = 0; i < NS; ++i) st.fd[i][j] -= st.fd[i][j - 1];
         st.ch.begin(W, g, A.state, A.axis);
-        const uint64_t s_end = active ? g.s1 : g.s0;
+        if (ilog && lane == 0) ilog[1] = global_ns();
+        const uint64_t s_end = g.s1;
+        const uint64_t cp_step = active ? W.checkpoint : 0;   // copies write no checkpoint
         double* cp_out = A.shadow + 3 * ((size_t)A.n_walks + wi);
         // Chunks of kFdChunk fast steps while every lane that still has steps
         // has a whole chunk left with no checkpoint inside it; a chunk where a
@@ -873,7 +886,7 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
                 for (int i = 0; i < NS; ++i)
 #pragma unroll
                     for (int j = 0; j < D; ++j) st.fd[i][j] += st.fd[i][j + 1];
-                if (W.checkpoint && s + 1 == W.checkpoint) st.ch.write(cp_out, W);
+                if (cp_step && s + 1 == cp_step) st.ch.write(cp_out, W);
             }
         }
         if (!LEAN) {
@@ -903,18 +916,27 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
                             for (int j = 0; j < D; ++j) st.fd[i][j] += st.fd[i][j + 1];
                     }
                     st.ch.renorm();
-                    if (__any_sync(0xffffffffu, out && left))
+                    if (__any_sync(0xffffffffu, out && left)) {
                         st = intfd_exact<CLS, M_, NS, D>(saved, kFdChunk, s, 0, cp_out, A.walks + wi);
+                        ++reruns;
+                    }
                     if (left) s += kFdChunk;
                     else st = saved;      // lanes without steps keep their state
-                } else if (left) {
-                    st = intfd_exact<CLS, M_, NS, D>(st, 1, s, W.checkpoint, cp_out, A.walks + wi);
-                    ++s;
+                } else {
+                    if (left) {
+                        st = intfd_exact<CLS, M_, NS, D>(st, 1, s, cp_step, cp_out, A.walks + wi);
+                        ++s;
+                    }
+                    ++exact_steps;
                 }
             }
         }
         const FChain<M_>& ch = st.ch;
         if (active) ch.end(W, g, A.state, A.shadow, A.status, wi);
+        if (ilog && lane == 0) {
+            ilog[2] = global_ns();
+            ilog[3] = ((unsigned long long)reruns << 32) | exact_steps;
+        }
         __syncwarp();
     }
     stamp_end(A.tstamp);

@@ -156,6 +156,7 @@ _SIGNATURES = {
     "dr_debug_host_pool": (ctypes.c_int, [_I32, _U64, _I32, _P, _P]),
     "dr_debug_rescale": (ctypes.c_int, [_P, _P, _I32, _P]),
     "dr_debug_batch_timeline": (ctypes.c_int, [_I32, _I32, _P, _P]),
+    "dr_debug_chain_items": (ctypes.c_int, [_I32, _I32, _P, _P]),
     "dr_debug_serve_waves": (ctypes.c_int, [_I32, _I32, _P, _P]),
     "dr_debug_serve_inject": (ctypes.c_int, [_I32, _I32, _I32, _P]),
     "dr_debug_build_phases": (ctypes.c_int, [_P, _I32]),

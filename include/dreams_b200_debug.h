@@ -41,6 +41,12 @@ int dr_bench_int_peak(int32_t kind, double *lane_ops_per_s);
 int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t *n_launches,
                             float *spans);
 
+/* The chain items of the integer-difference shadow launches (32 walks on one
+ * warp each) from the last dr_debug_batch_timeline of the batch: 6 floats per
+ * item, [launch group, start, difference tables built, end, chunks re-run
+ * exactly, exact single steps], times in ms on the timeline's scale. */
+int dr_debug_chain_items(int32_t batch, int32_t max_items, int32_t *n_items, float *rows);
+
 /* Exercises the host thread pool the batch build runs on: `repeats` jobs
  * over [0, n) with 1..parts parts each; every index must be visited exactly
  * once per job (else DR_ERR_INDEX).  index_sum and visits receive the
@@ -59,8 +65,10 @@ int dr_debug_host_pool(int32_t parts, uint64_t n, int32_t repeats, uint64_t *ind
 int dr_debug_build_info(int32_t *debug_checks);
 
 /* Host milliseconds (cumulative from the start) at the end of each phase of
- * the last dr_batch_create: programs, walks, tiles, shadow lists, launch
- * geometry, allocation and upload, final synchronisation (7 values). */
+ * the last dr_batch_create (13 values): plan lookup, program descriptors,
+ * code copy, walk validation, workload shape, tile count, tile fill, tile
+ * order, shadow lists, launch geometry, table copy, buffers and events,
+ * final synchronisation. */
 int dr_debug_build_phases(double *ms, int32_t n);
 
 /* Latency floor of the FP64 shadow chain for m = 2: one warp runs `steps`
