@@ -1386,7 +1386,7 @@ static cudaError_t launch_one(Batch& B, const LaunchSpec& L, WalkArgs& wa, Shado
     unsigned long long* ts = B.stamping ? B.tstamps.as<unsigned long long>() + 4 * (&L - B.launches.data()) : nullptr;
     wa.tstamp = ts;
     sa.tstamp = ts;
-    sa.item_log = (B.stamping && L.kind == 2)
+    sa.item_log = (B.stamping && L.kind != 0)
                       ? B.item_log.as<unsigned long long>() + 4ull * B.item_log_off[&L - B.launches.data()]
                       : nullptr;
     if (L.kind == 0) {
@@ -1564,6 +1564,7 @@ int batch_timeline(Batch& B, std::vector<float>* out) {
     for (size_t i = 0; i < n; ++i) {
         B.item_log_off[i] = n_items;
         if (B.launches[i].kind == 2) n_items += B.launches[i].items;
+        if (B.launches[i].kind == 1) n_items += B.launches[i].items2;
     }
     DR_CUDA(B.item_log.alloc(32ull * std::max<uint32_t>(n_items, 1)));
     DR_CUDA(cudaMemset(B.item_log.p, 0, 32ull * std::max<uint32_t>(n_items, 1)));
@@ -1580,8 +1581,9 @@ int batch_timeline(Batch& B, std::vector<float>* out) {
     // items: launch, start, tables built, end (ms after t0), re-run chunks, exact steps
     B.item_rows.clear();
     for (size_t i = 0; i < n; ++i) {
-        if (B.launches[i].kind != 2) continue;
-        for (uint32_t k = 0; k < B.launches[i].items; ++k) {
+        if (B.launches[i].kind == 0) continue;
+        const uint32_t items = B.launches[i].kind == 2 ? B.launches[i].items : B.launches[i].items2;
+        for (uint32_t k = 0; k < items; ++k) {
             const unsigned long long* r = &il[4ull * (B.item_log_off[i] + k)];
             if (!r[0] || r[0] < t0) continue;
             B.item_rows.insert(B.item_rows.end(),

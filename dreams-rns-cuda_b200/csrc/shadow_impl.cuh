@@ -70,8 +70,8 @@ struct ShadowArgs {
     uint32_t rows_regs;         // per-warp smem: doubles, 32 per row
     uint32_t rows_per_warp;
     uint32_t lean;              // chains co-located with walks: exact steps only
-    // diagnostics, integer-difference chains: per item [start ns, tables
-    // built ns, end ns, exact chunk re-runs << 32 | exact single steps], or null
+    // diagnostics, chain launches: per item [start ns, tables built / state
+    // loaded ns, end ns, exact chunk re-runs << 32 | exact steps or chunks], or null
     unsigned long long* item_log;
 };
 
@@ -662,11 +662,15 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
         if (it >= A.n_items) break;
         const uint32_t first = it * 32;
         const uint32_t count = min(32u, A.n_list - first);
+        unsigned long long* ilog = A.item_log ? A.item_log + 4ull * it : nullptr;
+        uint32_t reruns = 0, exact_chunks = 0;
+        if (ilog && lane == 0) ilog[0] = global_ns();
         const bool active = (uint32_t)lane < count;
         const DevShadowSeg g = A.segs[first + (active ? lane : 0)];
         const DevWalk W = A.walks[g.walk];
         Chain ch;
         ch.begin(W, g, A.state, A.axis);
+        if (ilog && lane == 0) ilog[1] = global_ns();
         const uint64_t len = active ? g.s1 - g.s0 : 0;
         // lanes past the item's segments stream lane 0's step matrices (their
         // results are dropped): stale shared memory could hold values that
@@ -746,14 +750,22 @@ __global__ void __launch_bounds__(256) k_shadow_chain(const ShadowArgs A) {
                     for (int e = 0; e < NE; ++e) X[e] = Y[e];
                 }
                 ch.renorm();
-                if (__any_sync(0xffffffffu, out && active)) ch = chain_chunk_exact<M_, COMP, Chain, CS>(saved, buf, lane);
+                if (__any_sync(0xffffffffu, out && active)) {
+                    ch = chain_chunk_exact<M_, COMP, Chain, CS>(saved, buf, lane);
+                    ++reruns;
+                }
             } else {
                 ch = chain_chunk_partial<M_, COMP, Chain, CS>(ch, buf, lane, base, len, cp_rel,
                                                                A.shadow + 3 * ((size_t)A.n_walks + g.walk), A.walks + g.walk);
+                ++exact_chunks;
             }
         }
         cp_async_wait<0>();
         if (active) ch.end(W, g, A.state, A.shadow, A.status, g.walk);
+        if (ilog && lane == 0) {
+            ilog[2] = global_ns();
+            ilog[3] = ((unsigned long long)reruns << 32) | exact_chunks;
+        }
     }
     stamp_end(A.tstamp);
 }

@@ -41,10 +41,12 @@ int dr_bench_int_peak(int32_t kind, double *lane_ops_per_s);
 int dr_debug_batch_timeline(int32_t batch, int32_t max_launches, int32_t *n_launches,
                             float *spans);
 
-/* The chain items of the integer-difference shadow launches (32 walks on one
- * warp each) from the last dr_debug_batch_timeline of the batch: 6 floats per
- * item, [launch group, start, difference tables built, end, chunks re-run
- * exactly, exact single steps], times in ms on the timeline's scale. */
+/* The chain items of the shadow launches (32 walks on one warp each) from the
+ * last dr_debug_batch_timeline of the batch: 6 floats per item, [launch group,
+ * start, difference tables built (integer-difference chains) or state loaded
+ * (interpreted chains), end, chunks re-run exactly, exact single steps
+ * (integer-difference) or exact chunks (interpreted)], times in ms on the
+ * timeline's scale. */
 int dr_debug_chain_items(int32_t batch, int32_t max_items, int32_t *n_items, float *rows);
 
 /* Exercises the host thread pool the batch build runs on: `repeats` jobs
