@@ -653,8 +653,19 @@ def main():
     ap.add_argument("--walks", type=int, default=N_WALKS,
                     help="PCFs per GPU (default 4096, the benchmark workload; smaller values "
                          "give the same workload shape for profiler captures)")
+    ap.add_argument("--stage", choices=["crt", "topk"],
+                    help="measure one pipeline stage alone on HBM-resident inputs (CRT of 2^20 "
+                         "K=32 residue vectors, or top-256 of 2^24 deltas) and print its JSON")
     args = ap.parse_args()
     N_WALKS = args.walks
+    if args.stage:
+        _use_repo_package()
+        import torch
+        from dreams_rns import _native as N
+        N.init(int(os.environ.get("LOCAL_RANK", "0")))
+        fn = bench_crt_stage if args.stage == "crt" else bench_topk_stage
+        print(json.dumps({"stage": args.stage, **fn(torch)}), flush=True)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
