@@ -239,6 +239,7 @@ __global__ void __launch_bounds__(128) k_crt(const uint32_t* __restrict__ residu
 // (lanes differ in the column) and the coalesced load/store of one value's
 // row (lanes differ in the row) are free of bank conflicts.
 constexpr int kCrtPitch = 33;
+constexpr int kCrtCols = 4;   // digit columns per group (interleaved Montgomery chains)
 
 __host__ __device__ inline size_t crt_lanes_warp_words(int K, int L) {
     return (size_t)kCrtPitch * ((K > L ? K : L) + L);
@@ -275,22 +276,50 @@ __global__ void __launch_bounds__(128) k_crt_lanes(const uint32_t* __restrict__ 
             for (int k = lane; k < K; k += 32) D[k * kCrtPitch + v] = __ldg(a + k);
         }
         __syncwarp();
-        // digits, column by column: digit k needs the final digits i < k
+        // digits: digit k takes rows i = 0 .. k-1 in order, each needing the
+        // final digit i.  Columns go in groups of kCrtCols: the rows below a
+        // group update its columns independently (interleaved Montgomery
+        // chains, kCrtCols times the instruction-level parallelism), then
+        // the group's own rows finish it column by column.
         const uint32_t t0 = D[lane];                 // raw, as the reference starts from it
-        for (int k = 1; k < K; ++k) {
-            const uint32_t p = sp[k];
-            const Mont M{p, spi[k], 0u, 0u};
-            uint32_t d = D[k * kCrtPitch + lane];
-            d = umin32(d, d - 2u * p);               // a_k < 2^32 < 4p: reduce mod p
-            d = umin32(d, d - p);
-            uint32_t t = umin32(t0, t0 - 2u * p);    // t_0 < 2^32: t_0 mod p
-            t = umin32(t, t - p);
-            d = mmul(subm(d, t, p), __ldg(T.garner + k), M);              // row i = 0
-            for (int i = 1; i < k; ++i) {
-                const uint32_t ti = D[i * kCrtPitch + lane];              // < p_i < 2p
-                d = mmul(subm(d, umin32(ti, ti - p), p), __ldg(T.garner + (size_t)i * K + k), M);
+        for (int k = 1; k < K; k += kCrtCols) {
+            uint32_t d[kCrtCols], pc[kCrtCols], pic[kCrtCols];
+#pragma unroll
+            for (int c = 0; c < kCrtCols; ++c) {
+                const int kk = k + c < K ? k + c : K - 1;   // past K: a duplicate, never stored
+                const uint32_t p = sp[kk];
+                pc[c] = p;
+                pic[c] = spi[kk];
+                uint32_t x = D[kk * kCrtPitch + lane];
+                x = umin32(x, x - 2u * p);           // a_k < 2^32 < 4p: reduce mod p
+                x = umin32(x, x - p);
+                uint32_t t = umin32(t0, t0 - 2u * p);   // t_0 < 2^32: t_0 mod p
+                t = umin32(t, t - p);
+                d[c] = mmul(subm(x, t, p), __ldg(T.garner + kk), Mont{p, pic[c], 0u, 0u});   // row 0
             }
-            D[k * kCrtPitch + lane] = d;
+            for (int i = 1; i < k; ++i) {
+                const uint32_t ti = D[i * kCrtPitch + lane];                 // < p_i < 2 p_k
+                const uint32_t* g = T.garner + (size_t)i * K;
+#pragma unroll
+                for (int c = 0; c < kCrtCols; ++c) {
+                    const int kk = k + c < K ? k + c : K - 1;
+                    const uint32_t p = pc[c];
+                    d[c] = mmul(subm(d[c], umin32(ti, ti - p), p), __ldg(g + kk), Mont{p, pic[c], 0u, 0u});
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < kCrtCols; ++c) {
+                if (k + c >= K) break;
+                // row k + c: digit k + c is final; it updates the later columns
+#pragma unroll
+                for (int c2 = c + 1; c2 < kCrtCols; ++c2) {
+                    if (k + c2 >= K) break;
+                    const uint32_t p = pc[c2];
+                    d[c2] = mmul(subm(d[c2], umin32(d[c], d[c] - p), p),
+                                 __ldg(T.garner + (size_t)(k + c) * K + (k + c2)), Mont{p, pic[c2], 0u, 0u});
+                }
+                D[(k + c) * kCrtPitch + lane] = d[c];
+            }
         }
         // x = t_0 + p_0 (t_1 + p_1 (t_2 + ...)): Horner from the top digit;
         // the limb count grows when some lane's carry needs a new limb

@@ -225,47 +225,114 @@ __device__ __forceinline__ bool ranks_before(uint64_t ka, uint32_t ia, uint64_t 
 
 constexpr int kTopkTile = 4096;
 
-// Sort one tile of (key, index) pairs in shared memory, keep the first k.
+// Compare-exchange of the pair (a, b) of one bitonic stage, a the lower
+// index: a takes the better one in an ascending ("best first") segment.
+__device__ __forceinline__ void cmpx_pair(uint64_t& ka, uint32_t& ia, uint64_t& kb, uint32_t& ib, bool up) {
+    const bool sw = up ? ranks_before(kb, ib, ka, ia) : ranks_before(ka, ia, kb, ib);
+    if (sw) {
+        const uint64_t tk = ka; ka = kb; kb = tk;
+        const uint32_t ti = ia; ia = ib; ib = ti;
+    }
+}
+
+// Register stage of stride RS * 1024: both elements of a pair live in one
+// thread (elements e = r * 1024 + tid, r < 4).
+template <int RS>
+__device__ __forceinline__ void topk_reg_stage(uint64_t (&K)[4], uint32_t (&I)[4], int tid, int size) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+        if ((r & RS) == 0) cmpx_pair(K[r], I[r], K[r | RS], I[r | RS], ((r * 1024 + tid) & size) == 0);
+}
+
+// Sort one tile of 4096 (key, index) pairs, keep the first k.  Bitonic
+// network, 1024 threads holding 4 elements each (element e = r * 1024 +
+// tid): strides of 1024 and 2048 pair elements of one thread (registers),
+// strides below 32 pair lanes of one warp (shuffles), and only strides 32 to
+// 512 go through shared memory, so one SM's shared-memory bandwidth no longer
+// bounds the tile.  The order is total (key, then index), so the result is
+// the same as any other correct sort's.
 __global__ void __launch_bounds__(1024) k_topk_tile(const double* __restrict__ vals,
                                                     const uint64_t* __restrict__ in_keys,
                                                     const uint32_t* __restrict__ in_idx, int n,
                                                     int k, uint64_t* __restrict__ out_keys,
                                                     uint32_t* __restrict__ out_idx) {
+    static_assert(kTopkTile == 4096, "4 elements per thread of a 1024-thread block");
     __shared__ uint64_t sk[kTopkTile];
     __shared__ uint32_t si[kTopkTile];
+    const int tid = threadIdx.x;
     const int base = blockIdx.x * kTopkTile;
-    for (int i = threadIdx.x; i < kTopkTile; i += blockDim.x) {
-        const int g = base + i;
+    uint64_t K[4];
+    uint32_t I[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int g = base + r * 1024 + tid;
         if (g < n) {
-            sk[i] = in_keys ? in_keys[g] : desc_key(vals[g]);
-            si[i] = in_idx ? in_idx[g] : (uint32_t)g;
+            K[r] = in_keys ? in_keys[g] : desc_key(vals[g]);
+            I[r] = in_idx ? in_idx[g] : (uint32_t)g;
         } else {
-            sk[i] = 0ull;
-            si[i] = 0xffffffffu;
+            K[r] = 0ull;
+            I[r] = 0xffffffffu;
         }
     }
-    __syncthreads();
     for (int size = 2; size <= kTopkTile; size <<= 1) {
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < kTopkTile; i += blockDim.x) {
-                const int j = i ^ stride;
-                if (j > i) {
-                    const bool up = (i & size) == 0;   // segment sorted "best first" when up
-                    const bool sw = up ? ranks_before(sk[j], si[j], sk[i], si[i])
-                                       : ranks_before(sk[i], si[i], sk[j], si[j]);
-                    if (sw) {
-                        const uint64_t tk = sk[i]; sk[i] = sk[j]; sk[j] = tk;
-                        const uint32_t ti = si[i]; si[i] = si[j]; si[j] = ti;
-                    }
-                }
+        int stride = size >> 1;
+        if (stride == 2048) { topk_reg_stage<2>(K, I, tid, size); stride >>= 1; }
+        if (stride == 1024) { topk_reg_stage<1>(K, I, tid, size); stride >>= 1; }
+        if (stride >= 32) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                sk[r * 1024 + tid] = K[r];
+                si[r * 1024 + tid] = I[r];
             }
             __syncthreads();
+            for (; stride >= 32; stride >>= 1) {
+                for (int i = tid; i < kTopkTile; i += 1024) {
+                    const int j = i ^ stride;
+                    if (j > i) {
+                        uint64_t ka = sk[i], kb = sk[j];
+                        uint32_t ia = si[i], ib = si[j];
+                        const bool up = (i & size) == 0;
+                        const bool sw = up ? ranks_before(kb, ib, ka, ia) : ranks_before(ka, ia, kb, ib);
+                        if (sw) {
+                            sk[i] = kb; sk[j] = ka;
+                            si[i] = ib; si[j] = ia;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                K[r] = sk[r * 1024 + tid];
+                I[r] = si[r * 1024 + tid];
+            }
+            __syncthreads();   // the next size writes sk / si again
+        }
+        for (; stride > 0; stride >>= 1) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int e = r * 1024 + tid;
+                const uint64_t pk = __shfl_xor_sync(0xffffffffu, K[r], stride);
+                const uint32_t pi = __shfl_xor_sync(0xffffffffu, I[r], stride);
+                // the lower element of the pair keeps the better one in an
+                // ascending segment; the higher keeps it in a descending one
+                const bool keep_better = ((e & stride) == 0) == ((e & size) == 0);
+                const bool partner_better = ranks_before(pk, pi, K[r], I[r]);
+                if (partner_better == keep_better) {
+                    K[r] = pk;
+                    I[r] = pi;
+                }
+            }
         }
     }
     const int keep = k < kTopkTile ? k : kTopkTile;
-    for (int i = threadIdx.x; i < keep; i += blockDim.x) {
-        out_keys[(size_t)blockIdx.x * keep + i] = sk[i];
-        out_idx[(size_t)blockIdx.x * keep + i] = si[i];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int e = r * 1024 + tid;
+        if (e < keep) {
+            out_keys[(size_t)blockIdx.x * keep + e] = K[r];
+            out_idx[(size_t)blockIdx.x * keep + e] = I[r];
+        }
     }
 }
 

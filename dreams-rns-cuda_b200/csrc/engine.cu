@@ -2335,7 +2335,7 @@ static int topk_tiles(const double* vals, const uint64_t* in_keys, const uint32_
 // threshold filter (delta_topk.cu) reads them once.
 constexpr int kTopkFilterMin = 1 << 18;
 constexpr int kTopkSample = 1 << 16;
-constexpr int kTopkCand = 1 << 16;
+constexpr int kTopkCand = 1 << 16;   // largest candidate buffer
 
 // Top-k (k <= 2048) of n device doubles, highest first, NaN last, ties by
 // lower index: idx_d[j], val_d[j] (device pointers; either may be null) for
@@ -2355,30 +2355,36 @@ int topk_device(const double* vals, int n, int k, int32_t* idx_d, double* val_d,
         const int s = kTopkSample;
         const int r = std::min(topk_tile_size() / 2,
                                (int)(4 * (((int64_t)k * s + n - 1) / n)) + 8);
+        // candidates: about r * n / s values reach the threshold; the
+        // buffer holds twice that (a power of two, 4096 .. kTopkCand), and
+        // an overflow falls back to sorting everything
+        const int64_t expect = (int64_t)r * ((n + s - 1) / s);
+        int cand = 4096;
+        while (cand < kTopkCand && cand < 2 * expect) cand <<= 1;
         DevBuf skeys, sidx, ckeys, cidx, count;
         skeys.pooled = sidx.pooled = ckeys.pooled = cidx.pooled = count.pooled = true;
         DR_CUDA(skeys.alloc(8ull * s));
         DR_CUDA(sidx.alloc(4ull * s));
-        DR_CUDA(ckeys.alloc(8ull * kTopkCand));
-        DR_CUDA(cidx.alloc(4ull * kTopkCand));
+        DR_CUDA(ckeys.alloc(8ull * cand));
+        DR_CUDA(cidx.alloc(4ull * cand));
         DR_CUDA(count.alloc(16));
         DR_CUDA(launch_topk_sample(vals, stride, s, skeys.as<uint64_t>(), sidx.as<uint32_t>(), st));
         DevBuf sk[2], si[2];
         int sb = 0;
         if ((rc = topk_tiles(nullptr, skeys.as<uint64_t>(), sidx.as<uint32_t>(), s, r, sk, si, st, &sb))) return rc;
         const uint64_t* thr = sk[sb].as<uint64_t>() + (r - 1);
-        DR_CUDA(cudaMemsetAsync(ckeys.p, 0, 8ull * kTopkCand, st));      // key 0, index ~0: rank last
-        DR_CUDA(cudaMemsetAsync(cidx.p, 0xff, 4ull * kTopkCand, st));
+        DR_CUDA(cudaMemsetAsync(ckeys.p, 0, 8ull * cand, st));      // key 0, index ~0: rank last
+        DR_CUDA(cudaMemsetAsync(cidx.p, 0xff, 4ull * cand, st));
         DR_CUDA(cudaMemsetAsync(count.p, 0, 16, st));
-        DR_CUDA(launch_topk_filter(vals, n, thr, ckeys.as<uint64_t>(), cidx.as<uint32_t>(), kTopkCand,
+        DR_CUDA(launch_topk_filter(vals, n, thr, ckeys.as<uint64_t>(), cidx.as<uint32_t>(), cand,
                                    count.as<unsigned int>(), g_ctx->sms, st));
-        if ((rc = topk_tiles(nullptr, ckeys.as<uint64_t>(), cidx.as<uint32_t>(), kTopkCand, k, keys, idx, st, &out)))
+        if ((rc = topk_tiles(nullptr, ckeys.as<uint64_t>(), cidx.as<uint32_t>(), cand, k, keys, idx, st, &out)))
             return rc;
         DR_CUDA(launch_topk_gather(vals, idx[out].as<uint32_t>(), keep, val_d, idx_d, st));
         unsigned int cnt = 0;
         DR_CUDA(cudaMemcpyAsync(&cnt, count.p, sizeof(cnt), cudaMemcpyDeviceToHost, st));
         DR_CUDA(cudaStreamSynchronize(st));
-        if (cnt >= (unsigned)keep && cnt <= (unsigned)kTopkCand) {
+        if (cnt >= (unsigned)keep && cnt <= (unsigned)cand) {
             if (filtered) *filtered = true;
             return DR_OK;
         }
