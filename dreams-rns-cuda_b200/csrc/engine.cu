@@ -337,8 +337,9 @@ uint32_t chunk_policy(uint64_t total_group_steps, uint64_t n_groups, int sms, co
 // fill, tile order, shadow lists, geometry, table copy, buffers and
 // events, final sync
 constexpr int kBuildPhases = 13;
-static double g_build_ms[kBuildPhases];
-static std::chrono::steady_clock::time_point g_build_t0;
+// (per thread: batches may be built on several threads at once)
+static thread_local double g_build_ms[kBuildPhases];
+static thread_local std::chrono::steady_clock::time_point g_build_t0;
 static void build_mark(int i) {
     const auto t = std::chrono::steady_clock::now();
     if (i == 0) g_build_t0 = t;
@@ -1836,6 +1837,23 @@ int dr_batch_run(int32_t batch, void* stream) {
     if (B->n_walks == 0) return DR_OK;
     StageScope sc(STAGE_RUN, "dr.run");
     return batch_run(*B, static_cast<cudaStream_t>(stream));
+}
+
+int dr_stream_create(void** stream_out) {
+    int rc = ensure_ctx();
+    if (rc) return rc;
+    if (!stream_out) return DR_ERR_ARG;
+    cudaStream_t s = nullptr;
+    DR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    *stream_out = s;
+    return DR_OK;
+}
+
+int dr_stream_destroy(void* stream) {
+    if (!stream) return DR_ERR_ARG;
+    DR_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    DR_CUDA(cudaStreamDestroy(static_cast<cudaStream_t>(stream)));
+    return DR_OK;
 }
 
 int dr_batch_read(int32_t batch, uint32_t* p_res, uint32_t* q_res, uint64_t n_res, double* shadow,

@@ -12,7 +12,7 @@ exact delta run in hand-written CUDA behind libdreams_b200.so.
 
 from .compiler import CmfCompiler, CmfProgram, Instruction, Opcode, compile_cmf, compile_cmf_from_dict
 from .engine import (WalkBatch, WalkRequest, autotune, cmf_request, pcf_request, run_walks,
-                     stage_times, sweep, vec_request)
+                     stage_times, sweep, sweep_many, vec_request)
 from .gpu_walk import (gpu_available, run_cmf_walk_batch_gpu, run_cmf_walk_gpu,
                        run_pcf_walk_batch_gpu, run_pcf_walk_gpu)
 from .runner import (WalkConfig, centered, compile_pcf, compute_dreams_delta_exact,
@@ -30,6 +30,6 @@ __all__ = [
     "pcf_initial_values", "run_pcf_walk", "verify_pcf",
     "gpu_available", "run_pcf_walk_gpu", "run_pcf_walk_batch_gpu", "run_cmf_walk_gpu",
     "run_cmf_walk_batch_gpu", "run_cmf_walk", "run_cmf_walk_vec", "vec_request", "compile_cmf_spec",
-    "WalkBatch", "WalkRequest", "pcf_request", "cmf_request", "run_walks", "sweep", "autotune", "crt_batch",
+    "WalkBatch", "WalkRequest", "pcf_request", "cmf_request", "run_walks", "sweep", "sweep_many", "autotune", "crt_batch",
     "delta_batch", "estimate_K", "crt_overflowed", "stage_times",
 ]

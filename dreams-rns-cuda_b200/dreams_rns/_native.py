@@ -130,6 +130,8 @@ _SIGNATURES = {
     "dr_walk_batch": (ctypes.c_int, [_P, _I32, _P, _P, _I32, _P, _U64, _P, _P, _P, _U64, _P, _P]),
     "dr_batch_create": (ctypes.c_int, [_P, _I32, _P, _P, _I32, _P, _U64, _P, _P]),
     "dr_batch_run": (ctypes.c_int, [_I32, _P]),
+    "dr_stream_create": (ctypes.c_int, [_P]),
+    "dr_stream_destroy": (ctypes.c_int, [_P]),
     "dr_batch_read": (ctypes.c_int, [_I32, _P, _P, _U64, _P, _P]),
     "dr_batch_stats": (ctypes.c_int, [_I32, _P, _P, _P, _P]),
     "dr_batch_destroy": (ctypes.c_int, [_I32]),

@@ -8,12 +8,13 @@ walks can be re-run with no host work (CUDA-graph replay).
 
 from __future__ import annotations
 
+import collections
 import ctypes
 import threading
 import time
 from dataclasses import dataclass, field
 from fractions import Fraction
-from typing import Dict, List, Optional, Sequence, Tuple
+from typing import Dict, Iterable, Iterator, List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -350,6 +351,67 @@ def sweep(reqs: Sequence[WalkRequest], delta: Optional[str] = None,
         return out
     finally:
         b.close()
+
+
+def sweep_many(batches: Iterable[Sequence[WalkRequest]], delta: Optional[str] = None,
+               target: Optional[Tuple[int, int]] = None, topk: int = 0, values: bool = False,
+               chunk_steps: int = 0, bank=None, lookahead: int = 2) -> Iterator[dict]:
+    """sweep() over a sequence of request lists, yielding each list's result
+    dict in order.  While the device walks one list, up to ``lookahead``
+    threads pack, build and upload the next ones (the batch build runs in C
+    with the GIL released), and every run goes to one stream of its own, so a
+    long sweep is bound by the slower of the host and the device instead of
+    their sum.  Results equal sweep()'s for each list."""
+    from concurrent.futures import ThreadPoolExecutor
+    N.init()
+    lookahead = max(1, int(lookahead))
+    piped = bool(delta) or topk > 0 or values
+    stream = ctypes.c_void_p()
+    N.check(N.lib().dr_stream_create(ctypes.byref(stream)), "dr_stream_create")
+
+    def prepare(reqs):
+        b = WalkBatch(reqs, chunk_steps=chunk_steps)
+        try:
+            if piped:
+                b.set_pipeline(delta=delta, target=target, topk=topk)
+            if bank:
+                b.set_bank(bank)
+            b.run(stream.value)
+        except BaseException:
+            b.close()
+            raise
+        return b
+
+    def collect(b):
+        try:
+            out = b.read_arrays()
+            if piped:
+                out.update(b.read_pipeline(values=values))
+            if bank and topk > 0:
+                out.update(b.read_bank())
+            return out
+        finally:
+            b.close()
+
+    pool = ThreadPoolExecutor(max_workers=lookahead)
+    pending: collections.deque = collections.deque()
+    try:
+        for reqs in batches:
+            pending.append(pool.submit(prepare, list(reqs)))
+            if len(pending) > lookahead:
+                yield collect(pending.popleft().result())
+        while pending:
+            yield collect(pending.popleft().result())
+    finally:
+        # batches prepared but not collected (early close, or an error)
+        while pending:
+            f = pending.popleft()
+            try:
+                f.result().close()
+            except Exception:  # noqa: BLE001 - its error was or will be raised elsewhere
+                pass
+        pool.shutdown(wait=True)
+        N.lib().dr_stream_destroy(stream)
 
 
 def autotune(reqs: Sequence[WalkRequest]) -> dict:

@@ -166,6 +166,13 @@ int dr_batch_create(const dr_walk_desc *walks, int32_t n_walks,
                     const int64_t *axis_params, uint64_t n_axis_params,
                     const dr_tune *tune, int32_t *batch_out);
 int dr_batch_run(int32_t batch, void *stream);
+/* A non-blocking CUDA stream for dr_batch_run, owned by the caller.  No
+ * reference counterpart (the reference runs one batch at a time).  Batch
+ * builds order their uploads on the engine's own stream and wait for it, so
+ * runs of batches built while others are running belong on a stream like this
+ * one (dreams_rns.sweep_many). */
+int dr_stream_create(void **stream_out);
+int dr_stream_destroy(void *stream);
 int dr_batch_read(int32_t batch, uint32_t *p_res, uint32_t *q_res, uint64_t n_res,
                   double *shadow, uint32_t *status);
 int dr_batch_stats(int32_t batch, uint64_t *prime_steps, uint32_t *n_tiles,

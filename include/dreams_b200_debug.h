@@ -67,7 +67,7 @@ int dr_debug_host_pool(int32_t parts, uint64_t n, int32_t repeats, uint64_t *ind
 int dr_debug_build_info(int32_t *debug_checks);
 
 /* Host milliseconds (cumulative from the start) at the end of each phase of
- * the last dr_batch_create (13 values): plan lookup, program descriptors,
+ * the calling thread's last dr_batch_create (13 values): plan lookup, program descriptors,
  * code copy, walk validation, workload shape, tile count, tile fill, tile
  * order, shadow lists, launch geometry, table copy, buffers and events,
  * final synchronisation. */

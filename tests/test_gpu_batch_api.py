@@ -72,3 +72,30 @@ def test_stage_times_cover_a_sweep():
     for k in ("pack", "build", "upload", "run", "read", "device"):
         assert st[f"{k}_calls"] >= 1 and st[f"{k}_ms"] > 0, (k, st)
     assert dr.stage_times()["build_calls"] == 0
+
+
+def test_sweep_many_equals_sweep_per_list():
+    """sweep_many over several lists (the next lists built while the device
+    walks the current one) gives each list what sweep() gives it, in order;
+    closing the generator early releases the batches it had prepared."""
+    from dreams_rns.engine import pcf_request
+    progs = [dr.compile_pcf("2", "n**2"), dr.compile_pcf("3*n + 1", "-2*n**2 + n"),
+             dr.compile_pcf("n + 5", "n**3 - 7")]
+    lists = []
+    for j in range(5):
+        lists.append([pcf_request(progs[(j + i) % 3], 1 + i, 1200 + 300 * j, 32, shift_val=1 + i,
+                                  checkpoint=400) for i in range(6 + 2 * j)])
+    want = [dr.sweep(r, delta="self", topk=3) for r in lists]
+    got = list(dr.sweep_many(lists, delta="self", topk=3, lookahead=2))
+    assert len(got) == len(lists)
+    for w, g in zip(want, got):
+        for key in ("p_residues", "q_residues", "topk_idx"):
+            assert np.array_equal(np.asarray(w[key]), np.asarray(g[key])), key
+        assert np.array_equal(w["shadow"], g["shadow"])
+        assert np.array_equal(w["delta"], g["delta"], equal_nan=True)
+    gen = dr.sweep_many(lists, delta="self", topk=3, lookahead=3)
+    first = next(gen)
+    assert np.array_equal(np.asarray(first["topk_idx"]), np.asarray(want[0]["topk_idx"]))
+    gen.close()
+    assert np.array_equal(np.asarray(dr.sweep(lists[1], delta="self", topk=3)["p_residues"]),
+                          np.asarray(want[1]["p_residues"]))
