@@ -266,10 +266,24 @@ struct LaunchKey {
 // Appends v to out longest first, keeping the input order among equal lengths
 // (a stable sort).  Tile lengths usually take a handful of values, which a
 // counting sort places in two passes over v; more than 64 distinct lengths
-// fall back to std::stable_sort.
+// fall back to std::stable_sort.  Lengths within 1/64 of each other (equal
+// splits of equal depths) are appended as they are: the order only balances
+// the queue's tail, and there it changes nothing.  (Skipping the sort for
+// lengths within a factor of two, a checkpoint's shorter chunks among the
+// others, made the benchmark's walk kernels 2% slower.)
 template <class T, class Len>
 static void append_longest_first(std::vector<T>& out, std::vector<T>& v, Len len) {
     constexpr uint32_t kMaxKeys = 64;
+    uint64_t lo = UINT64_MAX, hi = 0;
+    for (const T& t : v) {
+        const uint64_t l = len(t);
+        lo = std::min(lo, l);
+        hi = std::max(hi, l);
+    }
+    if (v.empty() || hi - lo <= hi / 64) {
+        out.insert(out.end(), v.begin(), v.end());
+        return;
+    }
     uint64_t keys[kMaxKeys];
     uint32_t nk = 0, last = 0;
     for (const T& t : v) {
@@ -504,17 +518,25 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     // ---- walks
     std::vector<DevWalk> dwalks(n_walks);
     uint64_t total_group_steps = 0, n_groups = 0;
+    std::map<LaunchKey, std::pair<uint64_t, uint64_t>> shape;   // workload shape, merged from the parts
+    uint64_t longest = 0;
     {
         // validation and device descriptors on the host pool; per-part sums
         struct WalkAcc {
             uint64_t group_steps = 0, groups = 0, prime_steps = 0;
             bool shadow = false;
+            // workload shape (see below): per launch key, (walk, prime block)
+            // count and their steps, and the longest walk
+            std::map<LaunchKey, std::pair<uint64_t, uint64_t>> shape;
+            uint64_t longest = 0;
         };
         const int parts = build_parts((size_t)n_walks);
         std::vector<BuildErr> perr(parts);
         std::vector<WalkAcc> accs(parts);
         auto walk_range = [&](int part, size_t w_lo, size_t w_hi) {
             WalkAcc& acc = accs[part];
+            LaunchKey shape_prev{-1, 0, 0, 0};
+            std::pair<uint64_t, uint64_t>* shape_cur = nullptr;
             for (size_t wi = w_lo; wi < w_hi; ++wi) {
                 const int32_t w = (int32_t)wi;
                 auto fail = [&](int code, const char* msg) { perr[part] = {(int64_t)w, code, msg}; };
@@ -586,6 +608,18 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
                 acc.group_steps += nb * std::max<uint64_t>(W.depth, 1);
                 acc.groups += nb;
                 acc.prime_steps += (uint64_t)W.K * W.depth;
+                {
+                    const Plan& P = *plans[W.program];
+                    LaunchKey key{0, G.cls, G.m, 0};
+                    if (G.cls != CLS_INTERP) key.D = (uint32_t)template_degree(P.cls, P.m, P.degree);
+                    if (!shape_cur || key < shape_prev || shape_prev < key) {
+                        shape_cur = &acc.shape[key];
+                        shape_prev = key;
+                    }
+                    shape_cur->first += nb;
+                    shape_cur->second += nb * W.depth;
+                    acc.longest = std::max<uint64_t>(acc.longest, W.depth);
+                }
             }
         };
         if (parts > 1) host_pool().run(parts, (size_t)n_walks, walk_range);
@@ -596,6 +630,12 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             n_groups += a.groups;
             B->prime_steps += a.prime_steps;
             B->has_shadow |= a.shadow;
+            for (const auto& kv : a.shape) {
+                auto& e = shape[kv.first];
+                e.first += kv.second.first;
+                e.second += kv.second.second;
+            }
+            longest = std::max(longest, a.longest);
         }
     }
 
@@ -604,26 +644,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     const bool plain = engine == DR_ENGINE_PLAIN;
     // workload shape for the autotuner: per launch key, log2 buckets of the
     // (walk, prime block) count and of their steps, plus the longest walk
+    // (summed per part in the walk pass above)
     {
-        std::map<LaunchKey, std::pair<uint64_t, uint64_t>> shape;
-        uint64_t longest = 0;
-        LaunchKey prev{-1, 0, 0, 0};
-        std::pair<uint64_t, uint64_t>* cur = nullptr;   // shape entry of prev
-        for (int32_t w = 0; w < n_walks; ++w) {
-            const DevWalk& W = dwalks[w];
-            const DevProgram& G = dprogs[W.prog];
-            const Plan& P = *plans[W.prog];
-            LaunchKey key{0, G.cls, G.m, 0};
-            if (G.cls != CLS_INTERP) key.D = (uint32_t)template_degree(P.cls, P.m, P.degree);
-            if (!cur || key < prev || prev < key) {
-                cur = &shape[key];
-                prev = key;
-            }
-            const uint64_t nb = (W.K + 31) / 32;
-            cur->first += nb;
-            cur->second += nb * W.depth;
-            longest = std::max<uint64_t>(longest, W.depth);
-        }
         auto lg = [](uint64_t v) { int b = 0; while (v > 1) { v >>= 1; ++b; } return b; };
         std::string sig = std::to_string(lg(longest)) + (B->has_shadow ? "s" : "n");
         for (auto& kv : shape)
@@ -850,9 +872,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     for (auto& d : dprogs) max_dim = std::max(max_dim, d.dim);
     for (auto& kv : shadow_sets) {
         auto& v = kv.second;
-        std::stable_sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) {
-            return dwalks[a].depth > dwalks[b].depth;
-        });
+        auto deeper = [&](uint32_t a, uint32_t b) { return dwalks[a].depth > dwalks[b].depth; };
+        if (!std::is_sorted(v.begin(), v.end(), deeper)) std::stable_sort(v.begin(), v.end(), deeper);
         uint32_t rr = 1;
         for (uint32_t w : v) {
             const DevProgram& G = dprogs[dwalks[w].prog];
@@ -1011,8 +1032,22 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             C.stage_bytes = cap;
         }
         uint8_t* h = static_cast<uint8_t*>(C.stage_host);
+        // into the staging buffer in 256 KB pieces, on the host pool when large
+        constexpr size_t kPiece = 256u << 10;
+        std::vector<std::pair<size_t, size_t>> pieces;   // (part, byte offset)
         for (size_t i = 0; i < kParts; ++i)
-            if (parts[i].n) std::memcpy(h + offs[i], parts[i].src, parts[i].n);
+            for (size_t o = 0; o < parts[i].n; o += kPiece) pieces.emplace_back(i, o);
+        auto copy_pieces = [&](int, size_t lo, size_t hi) {
+            for (size_t k = lo; k < hi; ++k) {
+                const Part& P = parts[pieces[k].first];
+                const size_t o = pieces[k].second;
+                std::memcpy(h + offs[pieces[k].first] + o, static_cast<const uint8_t*>(P.src) + o,
+                            std::min(kPiece, P.n - o));
+            }
+        };
+        const int cparts = std::min<int>(host_pool().threads(), (int)pieces.size());
+        if (cparts > 2) host_pool().run(cparts, pieces.size(), copy_pieces);
+        else copy_pieces(0, 0, pieces.size());
         DR_CUDA(cudaMemcpyAsync(B->tables.p, h, total, cudaMemcpyHostToDevice, st));
         uint8_t* d = static_cast<uint8_t*>(B->tables.p);
         for (size_t i = 0; i < kParts; ++i) parts[i].b->set_view(d + offs[i], std::max<size_t>(parts[i].n, 16));
