@@ -811,8 +811,8 @@ def main():
     chain_ns = chain_ms * 1e6 / DEPTH
     shadow_chain = {"bound": "latency", "achieved_ns_per_step": chain_ns, "floor_ns_per_step": floor.value,
                     "frac": floor.value / chain_ns, "chain_ms": chain_ms, "steps": DEPTH,
-                    "kernel": "k_shadow_chain<2,1>" if chain_p["kind"] == 1
-                    else f"k_shadow_intfd<1,2,{chain_p['degree']},0>",
+                    "kernel": (f"k_shadow_split<1,2,{chain_p['degree']}>" if chain_p["degree"] else "k_shadow_chain<2,1>")
+                    if chain_p["kind"] == 1 else f"k_shadow_intfd<1,2,{chain_p['degree']},0>",
                     "floor_source": "dr_bench_chain_step: the same fast step on one warp, "
                                     "step matrices computed in registers"}
 

@@ -360,6 +360,19 @@ static void build_mark(int i) {
     else g_build_ms[i - 1] = std::chrono::duration<double, std::milli>(t - g_build_t0).count();
 }
 
+// Split shadows: walks with at least this many integer-exact head steps (and
+// twice as many in all) run the head on integer differences.
+// DREAMS_B200_SPLIT_SHADOW=0 turns it off (every such walk then takes the
+// interpreted shadow).
+constexpr uint64_t kSplitMin = 256;
+static bool split_shadow_on() {
+    static const bool on = [] {
+        const char* v = std::getenv("DREAMS_B200_SPLIT_SHADOW");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
 // Host-pool use in batch construction: parts for n items (one part below
 // kPoolMin items; about kPoolGrain items per part otherwise).
 constexpr size_t kPoolMin = 1024, kPoolGrain = 512;
@@ -517,6 +530,10 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     build_mark(3);
     // ---- walks
     std::vector<DevWalk> dwalks(n_walks);
+    // split shadow: the head length of walks whose float intermediates are
+    // integer-exact only over their first steps (0: not split)
+    std::vector<uint64_t> split_at(n_walks, 0);
+    const bool split_shadow = split_shadow_on();
     uint64_t total_group_steps = 0, n_groups = 0;
     std::map<LaunchKey, std::pair<uint64_t, uint64_t>> shape;   // workload shape, merged from the parts
     uint64_t longest = 0;
@@ -598,8 +615,27 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
                     const Plan& P = *plans[W.program];
                     const int Dt = template_degree(P.cls, P.m, P.degree);
                     if (G.shadow_fd && G.cls != CLS_INTERP && Dt > 0 && !(W.flags & DR_WALK_VEC)) {
-                        const double b = float_bound_log2(P, axis + W.axis_offset, W.depth + 1);
-                        if (b < 53.0 && b + Dt < 61.0) d.shadow_mode = SHADOW_INTFD;
+                        const int64_t* ax = axis + W.axis_offset;
+                        auto exact_to = [&](uint64_t steps) {   // integer-exact float intermediates over [0, steps)
+                            const double b = float_bound_log2(P, ax, steps + 1);
+                            return b < 53.0 && b + Dt < 61.0;
+                        };
+                        if (exact_to(W.depth)) {
+                            d.shadow_mode = SHADOW_INTFD;
+                        } else if (split_shadow && G.fcomp && shadow_split_supported(G.cls, G.m, (uint32_t)Dt) &&
+                                   W.depth >= 2 * kSplitMin && exact_to(kSplitMin)) {
+                            // exact over a head of the walk: the split shadow
+                            // runs the head on integer differences (the bound
+                            // is monotone in the step count; 8 halvings place
+                            // the head within depth/256 of the largest)
+                            uint64_t lo = kSplitMin, hi = W.depth;
+                            for (int it = 0; it < 8 && hi - lo > 32; ++it) {
+                                const uint64_t mid = lo + (hi - lo) / 2;
+                                if (exact_to(mid)) lo = mid;
+                                else hi = mid;
+                            }
+                            split_at[w] = lo;
+                        }
                     }
                     acc.shadow = true;
                 }
@@ -852,8 +888,10 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             if (W.shadow_mode == SHADOW_NONE) continue;
             const DevProgram& G = dprogs[W.prog];
             const Plan& P = *plans[W.prog];
+            // kind 0 here: split shadows (integer-difference head, interpreted tail)
             const LaunchKey key = W.shadow_mode == SHADOW_INTFD
                 ? LaunchKey{2, P.cls, P.m, (uint32_t)template_degree(P.cls, P.m, P.degree)}
+                : split_at[w] ? LaunchKey{0, P.cls, P.m, (uint32_t)template_degree(P.cls, P.m, P.degree)}
                 : LaunchKey{1, G.fcomp | ((W.flags & DR_WALK_VEC) ? 2u : 0u), G.m, 0};
             if (!set || key < prev || prev < key) {
                 set = &shadow_sets[key];
@@ -872,6 +910,40 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     for (auto& d : dprogs) max_dim = std::max(max_dim, d.dim);
     for (auto& kv : shadow_sets) {
         auto& v = kv.second;
+        if (kv.first.kind == 0) {
+            // split shadows: walks by head length, shortest first (the longest
+            // items first); an item switches at its shortest head
+            std::stable_sort(v.begin(), v.end(), [&](uint32_t a, uint32_t b) { return split_at[a] < split_at[b]; });
+            uint32_t rr_eval = 1, rr_head = 1;
+            uint64_t need = 0;
+            std::vector<DevShadowSeg> segs;
+            segs.reserve(v.size());
+            for (size_t k = 0; k < v.size(); ++k) {
+                const uint32_t w = v[k];
+                const DevProgram& G = dprogs[dwalks[w].prog];
+                rr_eval = std::max(rr_eval, G.n_regs);
+                rr_head = std::max(rr_head, G.dn_regs);
+                const uint64_t sw = split_at[v[k / 32 * 32]];
+                segs.push_back(DevShadowSeg{w, kNoState, sw, dwalks[w].depth, 0, 0, 0});
+                need += (dwalks[w].depth - sw) * shadow_entries(kv.first.m, true);
+            }
+            if (need > cap_doubles) {
+                // the tails' step matrices would not fit: interpreted shadows
+                const DevProgram& G0 = dprogs[dwalks[v[0]].prog];
+                auto& interp = shadow_sets[LaunchKey{1, G0.fcomp, kv.first.m, 0}];
+                interp.insert(interp.end(), v.begin(), v.end());
+                continue;
+            }
+            const size_t l0 = B->launches.size();
+            mf_doubles += shadow_interp_plan(B->launches, shadow_list, eval_items, segs, kv.first.m, 1u, rr_eval,
+                                             mf_doubles, UINT64_MAX, state_slots);
+            for (size_t i = l0; i < B->launches.size(); ++i) {
+                B->launches[i].split_cls = kv.first.cls;
+                B->launches[i].split_D = kv.first.D;
+                B->launches[i].split_rows_regs = rr_head;
+            }
+            continue;
+        }
         auto deeper = [&](uint32_t a, uint32_t b) { return dwalks[a].depth > dwalks[b].depth; };
         if (!std::is_sorted(v.begin(), v.end(), deeper)) std::stable_sort(v.begin(), v.end(), deeper);
         uint32_t rr = 1;
@@ -942,6 +1014,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             L.queue2 = q++;
             if ((rc = shadow_interp_geometry(L, max_dim, C.sms, shadow_list.data() + L.off, true, walk_ns)))
                 return rc;
+            if (L.split_D && (rc = shadow_split_geometry(L, C.sms))) return rc;
             continue;
         }
         if (L.kind == 2) {
@@ -1240,6 +1313,47 @@ int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevSh
     return DR_OK;
 }
 
+// The chain launch of a split shadow: one item per warp (items are 32 walks
+// of about equal length, and the longest go first), kChainWarps warps per
+// block claiming a whole SM; per warp the head's rows or the tail's staging
+// buffers, whichever is larger.
+int shadow_split_geometry(LaunchSpec& L, int sms) {
+    const uint32_t ns = (uint32_t)std::max(streams_for(L.split_cls, L.m), 1);
+    const uint32_t head_rows = L.split_rows_regs + kMaxAxes + (L.split_D + 1) * ns + ns;
+    const uint32_t tail_rows = (uint32_t)(shadow_chain_smem(L.m, true) / (32 * sizeof(double)));
+    L.split_rows_per_warp = std::max(head_rows, tail_rows);
+    const size_t per_warp = (size_t)L.split_rows_per_warp * 32 * sizeof(double);
+    int cw = kChainWarps;
+    while (cw > 1 && per_warp * cw > 227 * 1024) cw /= 2;
+    if (per_warp * cw > 227 * 1024) {
+        set_error("program needs more shared memory per warp than a block offers");
+        return DR_ERR_UNSUPPORTED;
+    }
+    L.lean = false;
+    L.block2 = 32 * cw;
+    L.smem2 = std::max(per_warp * cw, chain_hog_smem());
+    ShadowArgs sa{};
+    int occ = 0;
+    cudaError_t e = shadow_split_dispatch(L.split_cls, L.m, L.split_D, 0, L.block2, L.smem2, nullptr, sa, &occ);
+    if (e != cudaSuccess) return cuda_fail(e, "occupancy query");
+    if (occ < 1) {
+        set_error("kernel cannot be resident with this shared memory size");
+        return DR_ERR_UNSUPPORTED;
+    }
+    L.grid2 = std::max(1, std::min((int)((L.items2 + cw - 1) / cw), occ * sms));
+    return DR_OK;
+}
+
+// The chain launch of an interpreted (or split) shadow group.
+static cudaError_t interp_chain_dispatch(const LaunchSpec& L, ShadowArgs sa, cudaStream_t s) {
+    if (L.split_D) {
+        sa.rows_regs = L.split_rows_regs;
+        sa.rows_per_warp = L.split_rows_per_warp;
+        return shadow_split_dispatch(L.split_cls, L.m, L.split_D, L.grid2, L.block2, L.smem2, s, sa, nullptr);
+    }
+    return shadow_chain_dispatch(L.m, L.cls, L.grid2, L.block2, L.smem2, s, sa, nullptr);
+}
+
 cudaError_t launch_shadow_interp(const LaunchSpec& L, ShadowArgs sa, uint32_t* queues,
                                  const uint32_t* eval_items, cudaStream_t s, cudaEvent_t evaluated) {
     sa.eval_items = eval_items + L.eoff;
@@ -1257,7 +1371,7 @@ cudaError_t launch_shadow_interp(const LaunchSpec& L, ShadowArgs sa, uint32_t* q
     sa.n_items = L.items2;
     sa.queue = queues + L.queue2;
     if (sa.tstamp) sa.tstamp += 2;
-    return shadow_chain_dispatch(L.m, L.cls, L.grid2, L.block2, L.smem2, s, sa, nullptr);
+    return interp_chain_dispatch(L, sa, s);
 }
 
 static CrtTables tables_of(const CrtSet& S);
@@ -1559,7 +1673,7 @@ int batch_profile(Batch& B, std::vector<float>* ms, std::vector<float>* ms2) {
             if (e == cudaSuccess) {
                 sa.n_items = L.items2;
                 sa.queue = B.queues.as<uint32_t>() + L.queue2;
-                e = shadow_chain_dispatch(L.m, L.cls, L.grid2, L.block2, L.smem2, st, sa, nullptr);
+                e = interp_chain_dispatch(L, sa, st);
             }
         } else {
             if (L.items) e = launch_one(B, L, wa, sa, st);
@@ -2243,7 +2357,7 @@ int dr_batch_profile(int32_t batch, int32_t max_launches, int32_t* n_launches, i
         if (kind) kind[i] = L.kind;
         if (cls) cls[i] = (int32_t)L.cls;
         if (m) m[i] = (int32_t)L.m;
-        if (degree) degree[i] = (int32_t)L.D;
+        if (degree) degree[i] = (int32_t)(L.kind == 1 ? L.split_D : L.D);
         if (items) items[i] = L.items;
         if (ms) ms[i] = t[i];
         if (ms2) ms2[i] = t2[i];

@@ -193,6 +193,10 @@ struct LaunchSpec {
     bool lean = false;         // shadow chains co-located with the walks: exact steps, which
                                // skip the rescale work on the steps without one (fewest
                                // instructions, as they share issue slots with the walks)
+    // kind 1 with split_D > 0: a split shadow, whose chain launch is
+    // k_shadow_split (integer-difference head of class split_cls and depth
+    // split_D, then the interpreted tail); the head's rows per warp
+    uint32_t split_cls = 0, split_D = 0, split_rows_regs = 0, split_rows_per_warp = 0;
 };
 
 // Interpreted-shadow launch geometry shared by batches and serving waves:
@@ -202,6 +206,8 @@ struct LaunchSpec {
 // whose walks run beside them); serving waves request only what they use.
 int shadow_interp_geometry(LaunchSpec& L, uint32_t max_dim, int sms, const DevShadowSeg* segs,
                            bool whole_sm = true, double walk_ns = 0.0);
+// The chain launch geometry of a split shadow group (LaunchSpec::split_D).
+int shadow_split_geometry(LaunchSpec& L, int sms);
 
 // FP64 chain kernels (interpreted chain, integer-difference shadow) run as
 // blocks of kChainWarps warps that claim a whole SM's shared memory, so no

@@ -19,4 +19,10 @@
     X(2, 1) X(2, 2) X(2, 3) X(2, 4) X(2, 6) X(2, 8) X(2, 12) X(2, 16) \
     X(3, 1) X(3, 2) X(3, 3) X(3, 4) X(3, 6)
 
+// split shadow (integer-difference head + interpreted tail): companion PCFs and
+// CMFs of m <= 3 with difference depths up to 8
+#define DR_SPLIT_INSTANCES(X) \
+    X(2, 1) X(2, 2) X(2, 3) X(2, 4) X(2, 6) X(2, 8) \
+    X(3, 1) X(3, 2) X(3, 3) X(3, 4) X(3, 6) X(3, 8)
+
 #define DR_INTERP_INSTANCES(X) X(1, 0) X(2, 0) X(3, 0) X(4, 0) X(5, 0) X(6, 0) X(7, 0) X(8, 0)

@@ -84,6 +84,11 @@ cudaError_t shadow_eval_dispatch(uint32_t U, int grid, int block, size_t smem, c
 cudaError_t shadow_chain_dispatch(uint32_t m, uint32_t flags, int grid, int block, size_t smem,
                                   cudaStream_t st, const ShadowArgs& a, int* occ);
 size_t shadow_chain_smem(uint32_t m, bool comp);
+// Split shadow (integer-difference head, then the interpreted chain's tail):
+// the (class, m, D) it is built for, and its launch.
+bool shadow_split_supported(uint32_t cls, uint32_t m, uint32_t D);
+cudaError_t shadow_split_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block, size_t smem,
+                                  cudaStream_t st, const ShadowArgs& a, int* occ);
 cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block,
                                size_t smem, cudaStream_t st, const ShadowArgs& a, int* occ);
 

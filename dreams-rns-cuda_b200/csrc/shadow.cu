@@ -68,6 +68,28 @@ cudaError_t shadow_fd_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, i
     return cudaErrorInvalidValue;
 }
 
+bool shadow_split_supported(uint32_t cls, uint32_t m, uint32_t D) {
+    if (cls != CLS_COMPANION) return false;
+    switch (m * 100 + D) {
+#define DR_X(M_, D_) case M_ * 100 + D_: return true;
+        DR_SPLIT_INSTANCES(DR_X)
+#undef DR_X
+        default: return false;
+    }
+}
+
+cudaError_t shadow_split_dispatch(uint32_t cls, uint32_t m, uint32_t D, int grid, int block, size_t smem,
+                                  cudaStream_t st, const ShadowArgs& a, int* occ) {
+    if (cls != CLS_COMPANION) return cudaErrorInvalidValue;
+    switch (m * 100 + D) {
+#define DR_X(M_, D_) \
+    case M_ * 100 + D_: return run_kernel(k_shadow_split<CLS_COMPANION, M_, D_>, grid, block, smem, st, a, occ, true);
+        DR_SPLIT_INSTANCES(DR_X)
+#undef DR_X
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 }  // namespace dr
 
 namespace dr {

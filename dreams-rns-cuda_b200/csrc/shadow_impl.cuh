@@ -954,4 +954,203 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
     stamp_end(A.tstamp);
 }
 
+
+// Split shadow: walks whose float intermediates stay below 2^53 only over
+// their first steps (a quartic b(n) with large coefficients, say).  A lane
+// runs one walk: the integer-difference chain of k_shadow_intfd (exact int64
+// forward differences, bit-identical to the float evaluation while every
+// intermediate is an integer below 2^53) from step 0 up to the item's switch
+// step g.s0, then the same FChain goes on with the step matrices that
+// k_shadow_eval wrote for steps g.s0 .. g.s1, as k_shadow_chain does.  The
+// host sorts the walks by their bound, so the 32 walks of an item have
+// nearly the same switch step (the smallest of theirs).  Nothing crosses a
+// launch: the head costs the integer chain's step, only the tail the
+// interpreted chain's.  Shared memory per warp: the head's rows, reused by
+// the tail's staging buffers once the head is done.
+template <int CLS, int M_, int D>
+__global__ void __launch_bounds__(256) k_shadow_split(const ShadowArgs A) {
+    constexpr int NS = (CLS == CLS_COMPANION) ? M_ : M_ * M_;
+    constexpr bool COMP = CLS == CLS_COMPANION;
+    constexpr int NE = COMP ? M_ : M_ * M_;
+    constexpr int CS = chain_chunk_steps(NE);
+    constexpr int NB = chain_buffers(NE);
+    using Chain = FChain<M_>;
+    extern __shared__ double dsm[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    double* wbase = dsm + (size_t)warp * A.rows_per_warp * 32;
+    int64_t* rf = reinterpret_cast<int64_t*>(wbase);
+    int64_t* axv = rf + A.rows_regs * 32;
+    int64_t* stage = axv + kMaxAxes * 32;      // [(j*NS + i)][32 walks]
+    int64_t* outv = stage + (D + 1) * NS * 32; // [stream][32 steps]
+    double* sbuf = wbase;                      // tail staging, after the head
+    // a programmatic dependent of the evaluation kernel: its step matrices
+    // are complete and visible past this point
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    stamp_begin(A.tstamp);
+    for (;;) {
+        uint32_t it = 0;
+        if (lane == 0) it = atomicAdd(A.queue, 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= A.n_items) break;
+        const uint32_t first = it * 32;
+        const uint32_t count = min(32u, A.n_list - first);
+        unsigned long long* ilog = A.item_log ? A.item_log + 4ull * it : nullptr;
+        uint32_t reruns = 0, exact = 0;
+        if (ilog && lane == 0) ilog[0] = global_ns();
+        // head tables: lane j evaluates segment w's walk at step j
+        for (uint32_t w = 0; w < count; ++w) {
+            const DevShadowSeg g = A.segs[first + w];
+            const DevWalk W = A.walks[g.walk];
+            const DevProgram G = A.progs[W.prog];
+            const int64_t* ax = A.axis + W.axis_off;
+            const int64_t s = lane;
+            for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = ax[0 + 4 * a] + s * ax[2 + 4 * a];
+            __syncwarp();
+            interp_i64(A.code + G.dop_off, G.dn_ops, rf, A.consts + G.c_off, axv, s, outv, lane);
+            __syncwarp();
+            if ((uint32_t)lane <= G.degree) {
+#pragma unroll
+                for (int i = 0; i < NS; ++i) stage[(lane * NS + i) * 32 + w] = outv[i * 32 + lane];
+            }
+            __syncwarp();
+        }
+        // lanes past the item's walks run a copy of lane 0's walk and drop
+        // its results (as in k_shadow_intfd)
+        const bool active = (uint32_t)lane < count;
+        const int srcl = active ? lane : 0;
+        const DevShadowSeg g = A.segs[first + srcl];
+        const uint32_t wi = g.walk;
+        const DevWalk W = A.walks[wi];
+        const DevProgram G = A.progs[W.prog];
+        FdChain<M_, NS, D> st;
+#pragma unroll
+        for (int j = 0; j <= D; ++j)
+#pragma unroll
+            for (int i = 0; i < NS; ++i) st.fd[i][j] = ((uint32_t)j <= G.degree) ? stage[(j * NS + i) * 32 + srcl] : 0;
+#pragma unroll
+        for (int lvl = 1; lvl <= D; ++lvl)
+#pragma unroll
+            for (int j = D; j >= lvl; --j)
+                if ((uint32_t)j <= G.degree)
+#pragma unroll
+                    for (int i = 0; i < NS; ++i) st.fd[i][j] -= st.fd[i][j - 1];
+        st.ch.init(W);
+        if (ilog && lane == 0) ilog[1] = global_ns();
+        const uint64_t s_sw = g.s0;                              // the same on every lane of the item
+        const uint64_t cp_step = active ? W.checkpoint : 0;      // copies write no checkpoint
+        double* cp_out = A.shadow + 3 * ((size_t)A.n_walks + wi);
+        constexpr int kFdChunk = 32;
+        uint64_t s = 0;
+        while (s < s_sw) {
+            const bool cp_in = W.checkpoint > s && W.checkpoint <= s + kFdChunk;
+            if (__all_sync(0xffffffffu, s + kFdChunk <= s_sw && !cp_in)) {
+                const FdChain<M_, NS, D> saved = st;
+                bool out = false;
+#pragma unroll 8
+                for (int t = 0; t < kFdChunk; ++t) {
+                    if (CLS == CLS_COMPANION) {
+                        double c[M_];
+#pragma unroll
+                        for (int i = 0; i < M_; ++i) c[i] = __ll2double_rn(st.fd[i][0]);
+                        st.ch.step_companion_fast(c, out);
+                    } else {
+                        double X[M_][M_];
+#pragma unroll
+                        for (int e = 0; e < M_ * M_; ++e) X[e / M_][e % M_] = __ll2double_rn(st.fd[e][0]);
+                        st.ch.step_fast(X, out);
+                    }
+#pragma unroll
+                    for (int i = 0; i < NS; ++i)
+#pragma unroll
+                        for (int j = 0; j < D; ++j) st.fd[i][j] += st.fd[i][j + 1];
+                }
+                st.ch.renorm();
+                if (__any_sync(0xffffffffu, out)) {
+                    st = intfd_exact<CLS, M_, NS, D>(saved, kFdChunk, s, 0, cp_out, A.walks + wi);
+                    ++reruns;
+                }
+                s += kFdChunk;
+            } else {
+                st = intfd_exact<CLS, M_, NS, D>(st, 1, s, cp_step, cp_out, A.walks + wi);
+                ++s;
+                ++exact;
+            }
+        }
+        // tail: steps s_sw .. g.s1 from the step-matrix buffer
+        Chain ch = st.ch;
+        __syncwarp();            // the head's rows are no longer read: the staging reuses them
+        const uint64_t len = active ? g.s1 - g.s0 : 0;
+        const uint64_t load_len = g.s1 - g.s0;
+        const double* src = A.mf + g.mf_off;
+        unsigned long long mlen = len;
+        unsigned long long minlen = active ? len : ~0ull;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mlen = max(mlen, __shfl_xor_sync(0xffffffffu, mlen, o));
+            minlen = min(minlen, __shfl_xor_sync(0xffffffffu, minlen, o));
+        }
+        const uint64_t cp_rel = (active && W.checkpoint > g.s0 && W.checkpoint <= g.s1)
+                                    ? W.checkpoint - g.s0 - 1 : ~0ull;
+        const uint64_t nch = (mlen + CS - 1) / CS;
+        auto issue = [&](uint64_t c) {
+            double* buf = sbuf + (size_t)(c % NB) * CS * NE * 32;
+#pragma unroll 1
+            for (int t = 0; t < CS; ++t) {
+                const uint64_t rel = c * CS + t;
+                if (rel < load_len)
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) cp_async8(buf + (t * NE + e) * 32 + lane, src + rel * NE + e);
+            }
+        };
+#pragma unroll 1
+        for (int c0 = 0; c0 + 1 < NB; ++c0) {
+            if ((uint64_t)c0 < nch) issue(c0);
+            cp_async_commit();
+        }
+        for (uint64_t c = 0; c < nch; ++c) {
+            if (c + NB - 1 < nch) issue(c + NB - 1);
+            cp_async_commit();
+            cp_async_wait<NB - 1>();
+            const double* buf = sbuf + (size_t)(c % NB) * CS * NE * 32;
+            const uint64_t base = c * CS;
+            const bool cp_here = __any_sync(0xffffffffu, cp_rel >= base && cp_rel < base + CS);
+            if (base + CS <= minlen && !cp_here) {
+                const Chain saved = ch;
+                bool out = false;
+                double X[NE];
+#pragma unroll
+                for (int e = 0; e < NE; ++e) X[e] = buf[e * 32 + lane];
+#pragma unroll
+                for (int t = 0; t < CS; ++t) {
+                    double Y[NE];
+                    const int tn = t + 1 < CS ? t + 1 : t;
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) Y[e] = buf[(tn * NE + e) * 32 + lane];
+                    chain_step_fast<M_, COMP, Chain>(ch, X, out);
+#pragma unroll
+                    for (int e = 0; e < NE; ++e) X[e] = Y[e];
+                }
+                ch.renorm();
+                if (__any_sync(0xffffffffu, out && active)) {
+                    ch = chain_chunk_exact<M_, COMP, Chain, CS>(saved, buf, lane);
+                    ++reruns;
+                }
+            } else {
+                ch = chain_chunk_partial<M_, COMP, Chain, CS>(ch, buf, lane, base, len, cp_rel, cp_out,
+                                                               A.walks + wi);
+                ++exact;
+            }
+        }
+        cp_async_wait<0>();
+        __syncwarp();            // every lane's copies have landed before the next item's tables
+        if (active) ch.end(W, g, A.state, A.shadow, A.status, wi);
+        if (ilog && lane == 0) {
+            ilog[2] = global_ns();
+            ilog[3] = ((unsigned long long)reruns << 32) | exact;
+        }
+    }
+    stamp_end(A.tstamp);
+}
+
 }  // namespace dr

@@ -232,8 +232,10 @@ int dr_autotune(const dr_walk_desc *walks, int32_t n_walks, const uint8_t *blobs
 /* Where a batch's time goes: runs every launch group of the batch alone, one
  * after another, timing each with CUDA events (walk kernels: kind 0; FP64
  * shadow: kind 1 interpreted, kind 2 integer differences).  ms: the launch
- * (kind 1: its step-matrix evaluation), ms2: kind 1's chain kernel.  No
- * reference counterpart (the reference has no profiling hooks). */
+ * (kind 1: its step-matrix evaluation), ms2: kind 1's chain kernel.  degree:
+ * the difference depth (kind 1: that of a split shadow's integer-difference
+ * head, 0 for a plain interpreted shadow).  No reference counterpart (the
+ * reference has no profiling hooks). */
 int dr_batch_profile(int32_t batch, int32_t max_launches, int32_t *n_launches, int32_t *kind,
                      int32_t *cls, int32_t *m, int32_t *degree, uint32_t *items, float *ms,
                      float *ms2);
