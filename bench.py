@@ -805,7 +805,14 @@ def main():
     # on one warp with its step matrices computed in registers.
     prof = batch.profile()
     chains = [(p["ms2"] if p["kind"] == 1 else p["ms"], p) for p in prof if p["kind"] in (1, 2)]
-    chain_ms, chain_p = max(chains, key=lambda x: x[0])
+    # integer-difference launches the tuner packs two chain warps per
+    # scheduler (chain_pack_depth) are slower by design, to give the walks
+    # their SMs; the latency figure is over the one-warp-per-scheduler ones
+    pack = int((tuned or {}).get("chain_pack_depth", 0))
+    def _packed(p):
+        return p["kind"] == 2 and pack and p["degree"] <= pack
+    solo = [c for c in chains if not _packed(c[1])] or chains
+    chain_ms, chain_p = max(solo, key=lambda x: x[0])
     floor = ctypes.c_double()
     N.check(N.lib().dr_bench_chain_step(DEPTH, ctypes.byref(floor)), "chain floor")
     chain_ns = chain_ms * 1e6 / DEPTH
@@ -814,7 +821,9 @@ def main():
                     "kernel": (f"k_shadow_split<1,2,{chain_p['degree']}>" if chain_p["degree"] else "k_shadow_chain<2,1>")
                     if chain_p["kind"] == 1 else f"k_shadow_intfd<1,2,{chain_p['degree']},0>",
                     "floor_source": "dr_bench_chain_step: the same fast step on one warp, "
-                                    "step matrices computed in registers"}
+                                    "step matrices computed in registers",
+                    "packed_launches": [{"kernel": f"k_shadow_intfd<1,2,{p['degree']},0>", "ms": c,
+                                         "warps_per_scheduler": 2} for c, p in chains if _packed(p)]}
 
     # ---- end to end through the public API with host buffers: one sweep()
     # call per step packs the requests, uploads descriptors and programs,

@@ -213,6 +213,7 @@ cudaError_t launch_delta(const DeltaArgs& D, int sms, cudaStream_t st) {
 // Keys order doubles descending (+inf first, NaN last); ties by lower index.
 __device__ __forceinline__ uint64_t desc_key(double d) {
     if (d != d) return 0ull;                                   // NaN last
+    if (d == 0.0) d = 0.0;                                     // -0 equals +0: a tie, by index
     uint64_t b = (uint64_t)__double_as_longlong(d);
     b = (b >> 63) ? ~b : (b | 0x8000000000000000ull);          // ascending order key
     return b;                                                  // larger = better

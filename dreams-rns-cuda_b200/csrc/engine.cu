@@ -692,12 +692,17 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     }
     build_mark(5);
     // an autotuned choice for this shape applies unless the caller fixed one
-    uint32_t tuned_chunk = 0, tuned_wpb = 0;
+    uint32_t tuned_chunk = 0, tuned_wpb = 0, tuned_pack = 0;
     if (!plain && !(tune && (tune->chunk_steps || tune->warps_per_block))) {
         std::lock_guard<std::mutex> lk(C.cache_mu);
         auto it = C.tuned.find(B->signature);
-        if (it != C.tuned.end()) std::tie(tuned_chunk, tuned_wpb) = it->second;
+        if (it != C.tuned.end()) {
+            tuned_chunk = it->second.chunk;
+            tuned_wpb = it->second.wpb;
+            tuned_pack = it->second.pack;
+        }
     }
+    const uint32_t chain_pack = (tune && tune->chain_pack_depth) ? tune->chain_pack_depth : tuned_pack;
     const uint32_t chunk = plain ? 0xffffffffu
                          : tuned_chunk ? tuned_chunk
                          : chunk_policy(total_group_steps, n_groups, C.sms, tune);
@@ -1021,8 +1026,11 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             const size_t per_warp = (size_t)L.rows_per_warp * 32 * 8;
             const bool coloc = chain_colocate(shadow_list.data() + L.off, L.count, L.m, walk_ns);
             L.lean = coloc;
-            L.block = coloc ? 32 : 32 * kChainWarps;
-            L.smem = coloc ? per_warp : std::max(per_warp * kChainWarps, chain_hog_smem());
+            // two chain warps per scheduler for the packed depths (the tuner's
+            // choice: each chain is slower, the walks get the SMs)
+            const int cw = (chain_pack && L.D <= chain_pack) ? 2 * kChainWarps : kChainWarps;
+            L.block = coloc ? 32 : 32 * cw;
+            L.smem = coloc ? per_warp : std::max(per_warp * cw, chain_hog_smem());
             if (per_warp * (L.block / 32) > L.smem || L.smem > 227 * 1024) {
                 set_error("program needs more shared memory per warp than a block offers");
                 return DR_ERR_UNSUPPORTED;
@@ -1036,7 +1044,7 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
                 return DR_ERR_UNSUPPORTED;
             }
             L.grid = coloc ? std::min((int)L.items, occ * C.sms)
-                           : std::min(chain_blocks(shadow_list.data() + L.off, L.count, L.m, walk_ns),
+                           : std::min(chain_blocks(shadow_list.data() + L.off, L.count, L.m, walk_ns, cw),
                                       occ * C.sms);
             continue;
         }
@@ -2268,12 +2276,24 @@ int dr_autotune(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             }
         }
     }
+    // then two chain warps per scheduler for the integer-difference shadows of
+    // depth up to d: worth it when those chains end before the walks do
+    for (uint32_t d : {2u, 3u, 4u, 16u}) {
+        dr_tune cand = bt;
+        cand.chain_pack_depth = d;
+        float ms = 0.f;
+        rc = time_one(cand, &ms, nullptr, nullptr);
+        if (rc == DR_ERR_UNSUPPORTED) continue;
+        if (rc) return rc;
+        if (ms < 0.98f * bms) { bms = ms; bt = cand; }
+    }
     {
         std::lock_guard<std::mutex> lk(C.cache_mu);
-        C.tuned[sig] = {bt.chunk_steps, bt.warps_per_block};
+        C.tuned[sig] = {bt.chunk_steps, bt.warps_per_block, bt.chain_pack_depth};
     }
     best->chunk_steps = bt.chunk_steps;
     best->warps_per_block = bt.warps_per_block;
+    best->chain_pack_depth = bt.chain_pack_depth;
     if (best_ms) *best_ms = bms;
     return DR_OK;
 }

@@ -152,7 +152,8 @@ struct Context {
     std::unordered_map<std::string, uint32_t> code_ids;
     uint32_t next_code_id = 1;   // never reused, so a cleared table cannot alias
     std::map<int, std::shared_ptr<CrtSet>> crt_std;  // CRT tables of the standard primes
-    std::map<std::string, std::pair<uint32_t, uint32_t>> tuned;   // signature -> (chunk, warps/block)
+    struct TunedShape { uint32_t chunk, wpb, pack; };   // chunk steps, warps/block, chain pack depth
+    std::map<std::string, TunedShape> tuned;              // by workload signature
     std::mutex cache_mu;
     std::multimap<size_t, void*> cache;   // free device blocks by size
     size_t cached_bytes = 0;

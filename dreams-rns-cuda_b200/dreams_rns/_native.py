@@ -83,7 +83,8 @@ assert WALK_DTYPE.itemsize == ctypes.sizeof(WalkDesc)
 
 class Tune(ctypes.Structure):
     _fields_ = [("chunk_steps", ctypes.c_uint32), ("warps_per_block", ctypes.c_uint32),
-                ("engine", ctypes.c_uint32), ("shadow_buffer_mb", ctypes.c_uint32)]
+                ("engine", ctypes.c_uint32), ("shadow_buffer_mb", ctypes.c_uint32),
+                ("chain_pack_depth", ctypes.c_uint32)]
 
 
 class Pipeline(ctypes.Structure):

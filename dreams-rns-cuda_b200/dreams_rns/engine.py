@@ -425,7 +425,8 @@ def autotune(reqs: Sequence[WalkRequest]) -> dict:
     N.check(N.lib().dr_autotune(N.ptr(pk.desc), pk.n, N.ptr(pk.blobs), N.ptr(pk.offsets),
                                 pk.n_programs, N.ptr(pk.axis), pk.n_axis, ctypes.byref(t),
                                 ctypes.byref(ms)), "dr_autotune")
-    return {"chunk_steps": t.chunk_steps, "warps_per_block": t.warps_per_block, "ms": ms.value}
+    return {"chunk_steps": t.chunk_steps, "warps_per_block": t.warps_per_block,
+            "chain_pack_depth": t.chain_pack_depth, "ms": ms.value}
 
 
 class WalkBatch:

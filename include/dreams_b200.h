@@ -114,6 +114,12 @@ typedef struct dr_tune {
                                  buffer per launch group; 0 = default
                                  (2048); walks beyond it run their shadow in
                                  rounds with resident state                 */
+    uint32_t chain_pack_depth;/* integer-difference shadow launches of
+                                 difference depth <= this run two chain warps
+                                 per scheduler (8 per SM instead of 4): each
+                                 chain is slower, but the walks get their SMs;
+                                 0 = the autotuned choice for the workload's
+                                 shape, else none                           */
 } dr_tune;
 
 /* ---- context ---------------------------------------------------------- */
@@ -220,7 +226,9 @@ int dr_batch_destroy(int32_t batch);
  * (best of three, CUDA events), and returns the fastest in *best (its engine
  * and shadow_buffer_mb fields are inputs); a candidate replaces the built-in
  * policy only when it is at least 2% faster, since shorter chunks cost host
- * build time on every batch.  The choice is remembered for the
+ * build time on every batch.  With the chosen shape it then tries packing
+ * the integer-difference shadow chains of depth <= 2, 3, 4 or 16 two warps
+ * per scheduler (chain_pack_depth), kept by the same 2% rule.  The choice is remembered for the
  * workload's shape (per launch class: log2 of the (walk, prime block) count
  * and of their steps, longest walk), so later batches of that shape built
  * with a zero chunk_steps and warps_per_block use it.  No reference

@@ -131,3 +131,25 @@ def test_topk_device_reports_the_filter():
     want = _ref_topk(h, k)
     assert list(idx.cpu().numpy()) == list(want)
     assert np.array_equal(val.cpu().numpy(), h[want])
+
+
+@pytest.mark.parametrize("n", [1, 7, 100, 4096, 8192])
+def test_topk_small_inputs_with_ties(n):
+    """Small inputs (the tile sort): the order of a full sort -- value
+    descending, NaN last, ties by lower index, -0.0 equal to +0.0 -- with heavy
+    ties, NaNs and infinities, and k above n."""
+    rng = np.random.default_rng(n)
+    d = np.round(rng.normal(0, 1, size=n), 1)          # many ties
+    d[rng.integers(0, n, size=max(1, n // 50))] = np.nan
+    d[rng.integers(0, n, size=max(1, n // 200))] = np.inf
+    d[rng.integers(0, n, size=max(1, n // 200))] = -np.inf
+    if n > 100:
+        d[: n // 4] = 0.5                              # a block of equal values near the top
+    for k in (1, 5, 100, 2048):
+        keep = min(k, n)
+        idx = np.zeros(keep, dtype=np.int32)
+        val = np.zeros(keep, dtype=np.float64)
+        N.check(N.lib().dr_topk(N.ptr(d), n, k, N.ptr(idx), N.ptr(val)), "dr_topk")
+        want = _ref_topk(d, keep)
+        assert list(idx) == list(want), (n, k)
+        assert np.array_equal(val, d[want], equal_nan=True)
