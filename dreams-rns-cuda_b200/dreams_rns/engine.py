@@ -270,12 +270,14 @@ def stage_times(reset: bool = False) -> dict:
     return out
 
 
-def _tune(chunk_steps=0, engine=N.DR_ENGINE_AUTO, warps_per_block=0, shadow_buffer_mb=0):
+def _tune(chunk_steps=0, engine=N.DR_ENGINE_AUTO, warps_per_block=0, shadow_buffer_mb=0,
+          chain_pack_depth=0):
     t = N.Tune()
     t.chunk_steps = chunk_steps
     t.engine = engine
     t.warps_per_block = warps_per_block
     t.shadow_buffer_mb = shadow_buffer_mb
+    t.chain_pack_depth = chain_pack_depth
     return t
 
 
@@ -433,11 +435,12 @@ class WalkBatch:
     """A batch of walks prepared once and resident on the device."""
 
     def __init__(self, reqs: Sequence[WalkRequest], chunk_steps: int = 0,
-                 engine: int = N.DR_ENGINE_AUTO, warps_per_block: int = 0, shadow_buffer_mb: int = 0):
+                 engine: int = N.DR_ENGINE_AUTO, warps_per_block: int = 0, shadow_buffer_mb: int = 0,
+                 chain_pack_depth: int = 0):
         N.init()
         self.reqs = list(reqs)
         self.pk = _Packed(self.reqs)
-        t = _tune(chunk_steps, engine, warps_per_block, shadow_buffer_mb)
+        t = _tune(chunk_steps, engine, warps_per_block, shadow_buffer_mb, chain_pack_depth)
         h = ctypes.c_int32(0)
         N.check(N.lib().dr_batch_create(N.ptr(self.pk.desc), self.pk.n, N.ptr(self.pk.blobs),
                                         N.ptr(self.pk.offsets), self.pk.n_programs,

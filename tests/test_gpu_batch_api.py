@@ -99,3 +99,21 @@ def test_sweep_many_equals_sweep_per_list():
     gen.close()
     assert np.array_equal(np.asarray(dr.sweep(lists[1], delta="self", topk=3)["p_residues"]),
                           np.asarray(want[1]["p_residues"]))
+
+
+def test_chain_packing_changes_no_result():
+    """Two integer-difference chain warps per scheduler (dr_tune.chain_pack_depth)
+    is a launch-shape choice: residues, shadows and statuses are the same."""
+    from dreams_rns.engine import WalkBatch, pcf_request
+    progs = [dr.compile_pcf("3*n + 1", "-2*n**2 + n"), dr.compile_pcf("n + 2", "n**3 + 5*n")]
+    reqs = [pcf_request(progs[i % 2], 1 + i % 3, 3000 + 97 * i, 32, shift_val=1 + i, checkpoint=700)
+            for i in range(70)]
+    out = []
+    for pack in (0, 16):
+        b = WalkBatch(reqs, chain_pack_depth=pack)
+        b.run()
+        out.append(b.read_arrays())
+        b.close()
+    for key in ("p_residues", "q_residues"):
+        assert np.array_equal(out[0][key], out[1][key]), key
+    assert np.array_equal(out[0]["shadow"], out[1]["shadow"])
