@@ -117,3 +117,22 @@ def test_chain_packing_changes_no_result():
     for key in ("p_residues", "q_residues"):
         assert np.array_equal(out[0][key], out[1][key]), key
     assert np.array_equal(out[0]["shadow"], out[1]["shadow"])
+
+
+def test_sweep_many_reports_a_bad_list_and_recovers():
+    """An invalid list (a walk with K = 0) raises from sweep_many when its turn
+    comes; the lists before it were yielded, the batches prepared after it are
+    released, and the engine keeps working."""
+    from dreams_rns.engine import pcf_request
+    prog = dr.compile_pcf("2", "n**2")
+    good = [pcf_request(prog, 2, 1500, 32, shift_val=s, checkpoint=300) for s in (1, 2, 3)]
+    bad = [pcf_request(prog, 2, 1500, 32)]
+    bad[0].K = 0
+    gen = dr.sweep_many([good, bad, good, good], delta="self", topk=2)
+    first = next(gen)
+    with pytest.raises((ValueError, RuntimeError)):
+        next(gen)
+    gen.close()
+    again = dr.sweep(good, delta="self", topk=2)
+    assert np.array_equal(np.asarray(first["topk_idx"]), np.asarray(again["topk_idx"]))
+    assert np.array_equal(first["p_residues"], again["p_residues"])
