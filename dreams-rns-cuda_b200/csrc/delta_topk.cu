@@ -236,37 +236,39 @@ __device__ __forceinline__ void cmpx_pair(uint64_t& ka, uint32_t& ia, uint64_t& 
     }
 }
 
-// Register stage of stride RS * 1024: both elements of a pair live in one
-// thread (elements e = r * 1024 + tid, r < 4).
-template <int RS>
+// Register stage of stride RS * T (T threads): both elements of a pair live
+// in one thread (elements e = r * T + tid, r < 4).
+template <int RS, int T>
 __device__ __forceinline__ void topk_reg_stage(uint64_t (&K)[4], uint32_t (&I)[4], int tid, int size) {
 #pragma unroll
     for (int r = 0; r < 4; ++r)
-        if ((r & RS) == 0) cmpx_pair(K[r], I[r], K[r | RS], I[r | RS], ((r * 1024 + tid) & size) == 0);
+        if ((r & RS) == 0) cmpx_pair(K[r], I[r], K[r | RS], I[r | RS], ((r * T + tid) & size) == 0);
 }
 
-// Sort one tile of 4096 (key, index) pairs, keep the first k.  Bitonic
-// network, 1024 threads holding 4 elements each (element e = r * 1024 +
-// tid): strides of 1024 and 2048 pair elements of one thread (registers),
-// strides below 32 pair lanes of one warp (shuffles), and only strides 32 to
-// 512 go through shared memory, so one SM's shared-memory bandwidth no longer
+// Sort one tile of TILE (key, index) pairs, keep the first k.  Bitonic
+// network, TILE / 4 threads holding 4 elements each (element e = r * T +
+// tid): strides of T and 2T pair elements of one thread (registers), strides
+// below 32 pair lanes of one warp (shuffles), and only strides from 32 to T/2
+// go through shared memory, so one SM's shared-memory bandwidth no longer
 // bounds the tile.  The order is total (key, then index), so the result is
-// the same as any other correct sort's.
-__global__ void __launch_bounds__(1024) k_topk_tile(const double* __restrict__ vals,
-                                                    const uint64_t* __restrict__ in_keys,
-                                                    const uint32_t* __restrict__ in_idx, int n,
-                                                    int k, uint64_t* __restrict__ out_keys,
-                                                    uint32_t* __restrict__ out_idx) {
-    static_assert(kTopkTile == 4096, "4 elements per thread of a 1024-thread block");
-    __shared__ uint64_t sk[kTopkTile];
-    __shared__ uint32_t si[kTopkTile];
+// the same as any other correct sort's, whatever the tile size.
+template <int TILE>
+__global__ void __launch_bounds__(TILE / 4) k_topk_tile(const double* __restrict__ vals,
+                                                        const uint64_t* __restrict__ in_keys,
+                                                        const uint32_t* __restrict__ in_idx, int n,
+                                                        int k, uint64_t* __restrict__ out_keys,
+                                                        uint32_t* __restrict__ out_idx) {
+    constexpr int T = TILE / 4;
+    static_assert(T >= 64 && (T & (T - 1)) == 0, "a power-of-two block of at least two warps");
+    __shared__ uint64_t sk[TILE];
+    __shared__ uint32_t si[TILE];
     const int tid = threadIdx.x;
-    const int base = blockIdx.x * kTopkTile;
+    const int base = blockIdx.x * TILE;
     uint64_t K[4];
     uint32_t I[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const int g = base + r * 1024 + tid;
+        const int g = base + r * T + tid;
         if (g < n) {
             K[r] = in_keys ? in_keys[g] : desc_key(vals[g]);
             I[r] = in_idx ? in_idx[g] : (uint32_t)g;
@@ -275,19 +277,19 @@ __global__ void __launch_bounds__(1024) k_topk_tile(const double* __restrict__ v
             I[r] = 0xffffffffu;
         }
     }
-    for (int size = 2; size <= kTopkTile; size <<= 1) {
+    for (int size = 2; size <= TILE; size <<= 1) {
         int stride = size >> 1;
-        if (stride == 2048) { topk_reg_stage<2>(K, I, tid, size); stride >>= 1; }
-        if (stride == 1024) { topk_reg_stage<1>(K, I, tid, size); stride >>= 1; }
+        if (stride == 2 * T) { topk_reg_stage<2, T>(K, I, tid, size); stride >>= 1; }
+        if (stride == T) { topk_reg_stage<1, T>(K, I, tid, size); stride >>= 1; }
         if (stride >= 32) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                sk[r * 1024 + tid] = K[r];
-                si[r * 1024 + tid] = I[r];
+                sk[r * T + tid] = K[r];
+                si[r * T + tid] = I[r];
             }
             __syncthreads();
             for (; stride >= 32; stride >>= 1) {
-                for (int i = tid; i < kTopkTile; i += 1024) {
+                for (int i = tid; i < TILE; i += T) {
                     const int j = i ^ stride;
                     if (j > i) {
                         uint64_t ka = sk[i], kb = sk[j];
@@ -304,15 +306,15 @@ __global__ void __launch_bounds__(1024) k_topk_tile(const double* __restrict__ v
             }
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                K[r] = sk[r * 1024 + tid];
-                I[r] = si[r * 1024 + tid];
+                K[r] = sk[r * T + tid];
+                I[r] = si[r * T + tid];
             }
             __syncthreads();   // the next size writes sk / si again
         }
         for (; stride > 0; stride >>= 1) {
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
-                const int e = r * 1024 + tid;
+                const int e = r * T + tid;
                 const uint64_t pk = __shfl_xor_sync(0xffffffffu, K[r], stride);
                 const uint32_t pi = __shfl_xor_sync(0xffffffffu, I[r], stride);
                 // the lower element of the pair keeps the better one in an
@@ -326,10 +328,10 @@ __global__ void __launch_bounds__(1024) k_topk_tile(const double* __restrict__ v
             }
         }
     }
-    const int keep = k < kTopkTile ? k : kTopkTile;
+    const int keep = k < TILE ? k : TILE;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-        const int e = r * 1024 + tid;
+        const int e = r * T + tid;
         if (e < keep) {
             out_keys[(size_t)blockIdx.x * keep + e] = K[r];
             out_idx[(size_t)blockIdx.x * keep + e] = I[r];
@@ -337,10 +339,19 @@ __global__ void __launch_bounds__(1024) k_topk_tile(const double* __restrict__ v
     }
 }
 
+// Small inputs sort in tiles of 1024 (256 threads each, several blocks at
+// once), larger ones in tiles of 4096.
+constexpr int kTopkSmallTile = 1024;
+int topk_tile_for(int n, int k) { return (n <= 16384 && 2 * k <= kTopkSmallTile) ? kTopkSmallTile : kTopkTile; }
+
 cudaError_t launch_topk_tile(const double* vals, const uint64_t* in_keys, const uint32_t* in_idx,
                              int n, int k, uint64_t* out_keys, uint32_t* out_idx, cudaStream_t st) {
-    const int tiles = (n + kTopkTile - 1) / kTopkTile;
-    k_topk_tile<<<tiles, 1024, 0, st>>>(vals, in_keys, in_idx, n, k, out_keys, out_idx);
+    const int tile = topk_tile_for(n, k);
+    const int tiles = (n + tile - 1) / tile;
+    if (tile == kTopkSmallTile)
+        k_topk_tile<kTopkSmallTile><<<tiles, kTopkSmallTile / 4, 0, st>>>(vals, in_keys, in_idx, n, k, out_keys, out_idx);
+    else
+        k_topk_tile<kTopkTile><<<tiles, kTopkTile / 4, 0, st>>>(vals, in_keys, in_idx, n, k, out_keys, out_idx);
     return cudaGetLastError();
 }
 

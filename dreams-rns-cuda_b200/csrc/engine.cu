@@ -1028,7 +1028,8 @@ int batch_build(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
             L.lean = coloc;
             // two chain warps per scheduler for the packed depths (the tuner's
             // choice: each chain is slower, the walks get the SMs)
-            const int cw = (chain_pack && L.D <= chain_pack) ? 2 * kChainWarps : kChainWarps;
+            int cw = (chain_pack && L.D <= chain_pack) ? 2 * kChainWarps : kChainWarps;
+            if (per_warp * cw > 227 * 1024) cw = kChainWarps;   // no room for the packed block
             L.block = coloc ? 32 : 32 * cw;
             L.smem = coloc ? per_warp : std::max(per_warp * cw, chain_hog_smem());
             if (per_warp * (L.block / 32) > L.smem || L.smem > 227 * 1024) {
@@ -2113,11 +2114,11 @@ int dr_batch_set_pipeline(int32_t batch, const dr_pipeline* pl) {
     }
     B->tk_counts.clear();
     if (pl->topk > 0 && n > 0) {
-        const int tile = topk_tile_size();
         int cnt = (int)n;
         size_t cap = 16;
         do {
             B->tk_counts.push_back(cnt);
+            const int tile = topk_tile_for(cnt, pl->topk);
             cnt = ((cnt + tile - 1) / tile) * std::min(pl->topk, tile);
             cap = std::max(cap, (size_t)cnt);
         } while (cnt > pl->topk);
@@ -2496,8 +2497,8 @@ namespace dr {
 // returns the buffer pair holding the sorted best k (at least min(k, n)).
 static int topk_tiles(const double* vals, const uint64_t* in_keys, const uint32_t* in_idx, int n, int k,
                       DevBuf (&keys)[2], DevBuf (&idx)[2], cudaStream_t st, int* out_buf) {
-    const int tile = topk_tile_size();
-    const size_t cap = (size_t)((n + tile - 1) / tile) * k + 16;
+    const int tile0 = topk_tile_for(n, k);
+    const size_t cap = (size_t)((n + tile0 - 1) / tile0) * k + 16;
     for (int b = 0; b < 2; ++b) {
         keys[b].pooled = idx[b].pooled = true;
         DR_CUDA(keys[b].alloc(8 * cap));
@@ -2506,8 +2507,9 @@ static int topk_tiles(const double* vals, const uint64_t* in_keys, const uint32_
     int cnt = n, cur = 0;
     cudaError_t e = launch_topk_tile(vals, in_keys, in_idx, cnt, k, keys[0].as<uint64_t>(), idx[0].as<uint32_t>(), st);
     if (e != cudaSuccess) return cuda_fail(e, "topk");
-    cnt = ((cnt + tile - 1) / tile) * std::min(k, tile);
+    cnt = ((cnt + tile0 - 1) / tile0) * std::min(k, tile0);
     while (cnt > k) {
+        const int tile = topk_tile_for(cnt, k);
         e = launch_topk_tile(nullptr, keys[cur].as<uint64_t>(), idx[cur].as<uint32_t>(), cnt, k,
                              keys[cur ^ 1].as<uint64_t>(), idx[cur ^ 1].as<uint32_t>(), st);
         if (e != cudaSuccess) return cuda_fail(e, "topk");

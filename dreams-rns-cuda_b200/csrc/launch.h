@@ -66,6 +66,8 @@ cudaError_t launch_crt_check(const uint32_t* limbs, const int32_t* signs, int L,
 cudaError_t launch_topk_tile(const double* vals, const uint64_t* in_keys, const uint32_t* in_idx,
                              int n, int k, uint64_t* out_keys, uint32_t* out_idx, cudaStream_t st);
 int topk_tile_size();
+// the tile of a launch_topk_tile pass over n values keeping k per tile
+int topk_tile_for(int n, int k);
 // threshold-filter top-k of large arrays (delta_topk.cu)
 cudaError_t launch_topk_sample(const double* vals, int64_t stride, int s, uint64_t* keys, uint32_t* idx,
                                cudaStream_t st);
