@@ -270,9 +270,17 @@ __global__ void __launch_bounds__(128) k_crt_lanes(const uint32_t* __restrict__ 
     for (int g = blockIdx.x * wpb + warp; g < groups; g += gridDim.x * wpb) {
         const int j0 = g * 32;
         const int cnt = min(32, n - j0);
+        // every lane loads one value's input offset and output row; the rows
+        // then go around by shuffles, so the warp's residue loads (and limb
+        // stores) are independent of one another instead of each waiting for
+        // its own offset load
+        const int jl = j0 + (lane < cnt ? lane : 0);
+        const uint64_t my_in = in_off ? in_off[jl] : (uint64_t)jl * K;
+        const uint32_t my_row = out_idx ? out_idx[jl] : (uint32_t)jl;
         // residues of the warp's values, one value's row at a time (coalesced)
+#pragma unroll 4
         for (int v = 0; v < cnt; ++v) {
-            const uint32_t* a = residues + (in_off ? in_off[j0 + v] : (uint64_t)(j0 + v) * K);
+            const uint32_t* a = residues + __shfl_sync(0xffffffffu, my_in, v);
             for (int k = lane; k < K; k += 32) D[k * kCrtPitch + v] = __ldg(a + k);
         }
         __syncwarp();
@@ -339,7 +347,7 @@ __global__ void __launch_bounds__(128) k_crt_lanes(const uint32_t* __restrict__ 
         __syncwarp();
         if (ulimbs)
             for (int v = 0; v < cnt; ++v) {
-                uint32_t* uo = ulimbs + (size_t)(out_idx ? out_idx[j0 + v] : (uint32_t)(j0 + v)) * stride;
+                uint32_t* uo = ulimbs + (size_t)__shfl_sync(0xffffffffu, my_row, v) * stride;
                 for (int l = lane; l < stride; l += 32) uo[l] = l < L ? X[l * kCrtPitch + v] : 0u;
             }
         // centring (runner.py:79-81): x - M if x > M // 2, else x.  d = M - x;
@@ -378,12 +386,11 @@ __global__ void __launch_bounds__(128) k_crt_lanes(const uint32_t* __restrict__ 
         }
         __syncwarp();
         if (lane < cnt) {
-            const uint32_t row = out_idx ? out_idx[j0 + lane] : (uint32_t)(j0 + lane);
-            sign_out[row] = nl ? (neg ? -1 : 1) : 0;
-            if (nlimbs_out) nlimbs_out[row] = nl;
+            sign_out[my_row] = nl ? (neg ? -1 : 1) : 0;
+            if (nlimbs_out) nlimbs_out[my_row] = nl;
         }
         for (int v = 0; v < cnt; ++v) {
-            uint32_t* out = limbs + (size_t)(out_idx ? out_idx[j0 + v] : (uint32_t)(j0 + v)) * stride;
+            uint32_t* out = limbs + (size_t)__shfl_sync(0xffffffffu, my_row, v) * stride;
             for (int l = lane; l < stride; l += 32) out[l] = l < L ? X[l * kCrtPitch + v] : 0u;
         }
         __syncwarp();
