@@ -819,7 +819,7 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
     int64_t* rf = base;
     int64_t* axv = rf + A.rows_regs * 32;
     int64_t* stage = axv + kMaxAxes * 32;      // [(j*NS + i)][32 walks]
-    int64_t* outv = stage + (D + 1) * NS * 32; // [stream][32 steps]
+    int64_t* outv = stage + (D + 1) * NS * 32; // [stream][32 walks]
     stamp_begin(A.tstamp);
     for (;;) {
         uint32_t it = 0;
@@ -831,23 +831,6 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
         unsigned long long* ilog = A.item_log ? A.item_log + 4ull * it : nullptr;
         uint32_t reruns = 0, exact_steps = 0;
         if (ilog && lane == 0) ilog[0] = global_ns();
-        // difference tables: lane j evaluates segment w's walk at step s0 + j
-        for (uint32_t w = 0; w < count; ++w) {
-            const DevShadowSeg g = A.segs[first + w];
-            const DevWalk W = A.walks[g.walk];
-            const DevProgram G = A.progs[W.prog];
-            const int64_t* ax = A.axis + W.axis_off;
-            const int64_t s = (int64_t)g.s0 + lane;
-            for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = ax[0 + 4 * a] + s * ax[2 + 4 * a];
-            __syncwarp();
-            interp_i64(A.code + G.dop_off, G.dn_ops, rf, A.consts + G.c_off, axv, s, outv, lane);
-            __syncwarp();
-            if ((uint32_t)lane <= G.degree) {
-#pragma unroll
-                for (int i = 0; i < NS; ++i) stage[(lane * NS + i) * 32 + w] = outv[i * 32 + lane];
-            }
-            __syncwarp();
-        }
         // Lanes past the item's walks run a copy of lane 0's walk (same
         // table, same steps) and drop its results.  Left at their start
         // state, they made the whole warp of a partial item ~1.6x slower
@@ -858,11 +841,25 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
         const uint32_t wi = g.walk;
         const DevWalk W = A.walks[wi];
         const DevProgram G = A.progs[W.prog];
+        // difference tables: every lane evaluates its own walk at steps
+        // s0 .. s0 + degree (the 32 walks at once, each in its own column of
+        // the register file; lanes with the same program structure run in
+        // lockstep, others only diverge on the opcode)
+        {
+            const int64_t* ax = A.axis + W.axis_off;
+            for (uint32_t j = 0; j <= G.degree; ++j) {
+                const int64_t s = (int64_t)g.s0 + j;
+                for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = ax[0 + 4 * a] + s * ax[2 + 4 * a];
+                interp_i64(A.code + G.dop_off, G.dn_ops, rf, A.consts + G.c_off, axv, s, outv, lane);
+#pragma unroll
+                for (int i = 0; i < NS; ++i) stage[(j * NS + i) * 32 + lane] = outv[i * 32 + lane];
+            }
+        }
         FdChain<M_, NS, D> st;
 #pragma unroll
         for (int j = 0; j <= D; ++j)
 #pragma unroll
-            for (int i = 0; i < NS; ++i) st.fd[i][j] = ((uint32_t)j <= G.degree) ? stage[(j * NS + i) * 32 + src] : 0;
+            for (int i = 0; i < NS; ++i) st.fd[i][j] = ((uint32_t)j <= G.degree) ? stage[(j * NS + i) * 32 + lane] : 0;
 #pragma unroll
         for (int lvl = 1; lvl <= D; ++lvl)
 #pragma unroll
@@ -982,7 +979,7 @@ __global__ void __launch_bounds__(256) k_shadow_split(const ShadowArgs A) {
     int64_t* rf = reinterpret_cast<int64_t*>(wbase);
     int64_t* axv = rf + A.rows_regs * 32;
     int64_t* stage = axv + kMaxAxes * 32;      // [(j*NS + i)][32 walks]
-    int64_t* outv = stage + (D + 1) * NS * 32; // [stream][32 steps]
+    int64_t* outv = stage + (D + 1) * NS * 32; // [stream][32 walks]
     double* sbuf = wbase;                      // tail staging, after the head
     // a programmatic dependent of the evaluation kernel: its step matrices
     // are complete and visible past this point
@@ -998,23 +995,6 @@ __global__ void __launch_bounds__(256) k_shadow_split(const ShadowArgs A) {
         unsigned long long* ilog = A.item_log ? A.item_log + 4ull * it : nullptr;
         uint32_t reruns = 0, exact = 0;
         if (ilog && lane == 0) ilog[0] = global_ns();
-        // head tables: lane j evaluates segment w's walk at step j
-        for (uint32_t w = 0; w < count; ++w) {
-            const DevShadowSeg g = A.segs[first + w];
-            const DevWalk W = A.walks[g.walk];
-            const DevProgram G = A.progs[W.prog];
-            const int64_t* ax = A.axis + W.axis_off;
-            const int64_t s = lane;
-            for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = ax[0 + 4 * a] + s * ax[2 + 4 * a];
-            __syncwarp();
-            interp_i64(A.code + G.dop_off, G.dn_ops, rf, A.consts + G.c_off, axv, s, outv, lane);
-            __syncwarp();
-            if ((uint32_t)lane <= G.degree) {
-#pragma unroll
-                for (int i = 0; i < NS; ++i) stage[(lane * NS + i) * 32 + w] = outv[i * 32 + lane];
-            }
-            __syncwarp();
-        }
         // lanes past the item's walks run a copy of lane 0's walk and drop
         // its results (as in k_shadow_intfd)
         const bool active = (uint32_t)lane < count;
@@ -1023,11 +1003,23 @@ __global__ void __launch_bounds__(256) k_shadow_split(const ShadowArgs A) {
         const uint32_t wi = g.walk;
         const DevWalk W = A.walks[wi];
         const DevProgram G = A.progs[W.prog];
+        // head tables: every lane evaluates its own walk at steps 0 .. degree
+        // (as in k_shadow_intfd)
+        {
+            const int64_t* ax = A.axis + W.axis_off;
+            for (uint32_t j = 0; j <= G.degree; ++j) {
+                const int64_t s = j;
+                for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = ax[0 + 4 * a] + s * ax[2 + 4 * a];
+                interp_i64(A.code + G.dop_off, G.dn_ops, rf, A.consts + G.c_off, axv, s, outv, lane);
+#pragma unroll
+                for (int i = 0; i < NS; ++i) stage[(j * NS + i) * 32 + lane] = outv[i * 32 + lane];
+            }
+        }
         FdChain<M_, NS, D> st;
 #pragma unroll
         for (int j = 0; j <= D; ++j)
 #pragma unroll
-            for (int i = 0; i < NS; ++i) st.fd[i][j] = ((uint32_t)j <= G.degree) ? stage[(j * NS + i) * 32 + srcl] : 0;
+            for (int i = 0; i < NS; ++i) st.fd[i][j] = ((uint32_t)j <= G.degree) ? stage[(j * NS + i) * 32 + lane] : 0;
 #pragma unroll
         for (int lvl = 1; lvl <= D; ++lvl)
 #pragma unroll
