@@ -532,8 +532,9 @@ def bench_cmf3(stream, torch, n_walks=16384):
     plain_rate = plain_steps / (plain_ms * 1e-3)
     # integer-pipe roofline of the walk kernels on this sweep (no shadow)
     import ctypes
+    # at the launch shape the timed sweep runs with (the tuner's choice)
     walk_only = WalkBatch([cmf_request(kb[w.program_key], w.depth, w.K, w.shifts, w.trajectory, shadow=False)
-                           for w in ws])
+                           for w in ws], chunk_steps=tuned["chunk_steps"], warps_per_block=tuned["warps_per_block"])
     walk_ms = _time_batch(walk_only, stream, torch, reps=5)
     walk_only.close()
     infos = {k: N.program_info(b) for k, b in kb.items()}
@@ -773,8 +774,11 @@ def main():
     pipe = batch.read_pipeline()
 
     # ---- roofline: the walk kernels alone (no shadow, no pipeline)
+    # at the launch shape the timed batch runs with (the tuner's choice)
     walk_only = WalkBatch([pcf_request(b, w.a0, DEPTH, K, checkpoint=CHECKPOINT, shadow=False)
-                           for b, w in zip(blobs, ws)])
+                           for b, w in zip(blobs, ws)],
+                          chunk_steps=(tuned or {}).get("chunk_steps", 0),
+                          warps_per_block=(tuned or {}).get("warps_per_block", 0))
     for _ in range(3):
         walk_only.run(stream.cuda_stream)
     wt = []
@@ -796,7 +800,7 @@ def main():
     import ctypes
     peaks = int_peaks(N)
     roofline = walk_roofline(splits, walk_ms, peaks,
-                             "k_walk<COMPANION, 2, D> (D = 1..4), walk-only batch, median of 5")
+                             "k_walk<COMPANION, 2, D> (D = 1..4), walk-only batch at the timed batch's launch shape, median of 5")
     walk_only.close()
 
     # ---- the step's critical path: the FP64 shadow chains, serial recurrences
