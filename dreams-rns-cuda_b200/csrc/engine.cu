@@ -2278,15 +2278,17 @@ int dr_autotune(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         }
     }
     // then two chain warps per scheduler for the integer-difference shadows of
-    // depth up to d: worth it when those chains end before the walks do
-    for (uint32_t d : {2u, 3u, 4u, 16u}) {
+    // depth up to d: worth it when those chains end before the walks do.
+    // Packing costs the host nothing, so 1% (above the replays' spread of
+    // ~0.5% for a best of 3) is enough to keep it
+    for (uint32_t d : {1u, 2u, 3u, 4u, 16u}) {
         dr_tune cand = bt;
         cand.chain_pack_depth = d;
         float ms = 0.f;
         rc = time_one(cand, &ms, nullptr, nullptr);
         if (rc == DR_ERR_UNSUPPORTED) continue;
         if (rc) return rc;
-        if (ms < 0.98f * bms) { bms = ms; bt = cand; }
+        if (ms < 0.99f * bms) { bms = ms; bt = cand; }
     }
     {
         std::lock_guard<std::mutex> lk(C.cache_mu);

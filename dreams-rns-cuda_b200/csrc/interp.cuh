@@ -150,35 +150,58 @@ __device__ __forceinline__ void interp_f64(const uint4* __restrict__ code, uint3
 }
 
 // Exact int64 interpreter for programs without INV whose values the host has
-// bounded below 2^53 (integer-valued float shadow).
-__device__ __forceinline__ void interp_i64(const uint4* __restrict__ code, uint32_t n,
-                                           int64_t* __restrict__ rf,
-                                           const int64_t* __restrict__ consts,
-                                           const int64_t* __restrict__ axv, int64_t step,
-                                           int64_t* __restrict__ out, int lane) {
+// bounded below 2^53 (integer-valued float shadow), with one program per lane
+// (the exception to the uniform dispatch above: the lanes evaluate 32
+// different walks, whose programs differ in their op sequences).  Every lane
+// fetches its own instruction and the opcode selects the result and its
+// destination instead of a jump, so the warp stays converged however the
+// programs differ.  nmax = the warp's
+// longest program; a lane past its own n writes nothing.  Operand rows are
+// read at row 0 where the opcode has no such operand, so every access stays
+// inside the register file and axis rows.  The instructions (and the
+// constants they load) come in batches of kBatch independent loads: with the
+// chain kernels' shared memory taking most of the SM, the lanes' 32 programs
+// do not stay in L1, and one fetch at a time waited on L2 for every op.
+__device__ __forceinline__ void interp_i64_lanes(const uint4* __restrict__ code, uint32_t n, uint32_t nmax,
+                                                 int64_t* __restrict__ rf,
+                                                 const int64_t* __restrict__ consts,
+                                                 const int64_t* __restrict__ axv, int64_t step,
+                                                 int64_t* __restrict__ out, int lane) {
+    constexpr int kBatch = 8;
 #pragma unroll 1
-    for (uint32_t pc = 0; pc < n; ++pc) {
-        const uint4 in = __ldg(code + pc);
-        switch (in.x) {
-            case OP_LOAD_X: rf[in.z * 32 + lane] = axv[in.y * 32 + lane]; break;
-            case OP_LOAD_C: rf[in.z * 32 + lane] = __ldg(consts + in.y); break;
-            case OP_LOAD_N: rf[in.y * 32 + lane] = step; break;
-            case OP_ADD: rf[in.w * 32 + lane] = rf[in.y * 32 + lane] + rf[in.z * 32 + lane]; break;
-            case OP_SUB: rf[in.w * 32 + lane] = rf[in.y * 32 + lane] - rf[in.z * 32 + lane]; break;
-            case OP_MUL: rf[in.w * 32 + lane] = rf[in.y * 32 + lane] * rf[in.z * 32 + lane]; break;
-            case OP_NEG: rf[in.z * 32 + lane] = -rf[in.y * 32 + lane]; break;
-            case OP_POW2: {
-                const int64_t v = rf[in.y * 32 + lane];
-                rf[in.z * 32 + lane] = v * v;
-                break;
-            }
-            case OP_POW3: {
-                const int64_t v = rf[in.y * 32 + lane];
-                rf[in.z * 32 + lane] = v * v * v;
-                break;
-            }
-            case OP_STORE: out[in.z * 32 + lane] = rf[in.y * 32 + lane]; break;
-            default: break;
+    for (uint32_t pc0 = 0; pc0 < nmax; pc0 += kBatch) {
+        uint4 ins[kBatch];
+        int64_t cv[kBatch];
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k)
+            ins[k] = pc0 + k < n ? __ldg(code + pc0 + k) : make_uint4(OP_NOP, 0u, 0u, 0u);
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            cv[k] = 0;
+            if (ins[k].x == OP_LOAD_C) cv[k] = __ldg(consts + ins[k].y);
+        }
+#pragma unroll
+        for (int k = 0; k < kBatch; ++k) {
+            const uint4 in = ins[k];
+            const uint32_t op = in.x;
+            const bool bin = op == OP_ADD || op == OP_SUB || op == OP_MUL;
+            const bool un = op == OP_NEG || op == OP_POW2 || op == OP_POW3;
+            const int64_t a = rf[((bin || un || op == OP_STORE) ? in.y : 0u) * 32 + lane];
+            const int64_t b = rf[(bin ? in.z : 0u) * 32 + lane];
+            const int64_t x = axv[(op == OP_LOAD_X ? in.y : 0u) * 32 + lane];
+            const int64_t sq = a * a;
+            const int64_t r = op == OP_ADD ? a + b
+                            : op == OP_SUB ? a - b
+                            : op == OP_MUL ? a * b
+                            : op == OP_NEG ? -a
+                            : op == OP_POW2 ? sq
+                            : op == OP_POW3 ? sq * a
+                            : op == OP_LOAD_X ? x
+                            : op == OP_LOAD_C ? cv[k]
+                            : step;                                  // OP_LOAD_N
+            const uint32_t dst = bin ? in.w : op == OP_LOAD_N ? in.y : in.z;
+            if (bin || un || op == OP_LOAD_X || op == OP_LOAD_C || op == OP_LOAD_N) rf[dst * 32 + lane] = r;
+            if (op == OP_STORE) out[in.z * 32 + lane] = a;
         }
     }
 }

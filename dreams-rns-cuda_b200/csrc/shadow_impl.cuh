@@ -843,14 +843,14 @@ __global__ void __launch_bounds__(256) k_shadow_intfd(const ShadowArgs A) {
         const DevProgram G = A.progs[W.prog];
         // difference tables: every lane evaluates its own walk at steps
         // s0 .. s0 + degree (the 32 walks at once, each in its own column of
-        // the register file; lanes with the same program structure run in
-        // lockstep, others only diverge on the opcode)
+        // the register file, the programs' opcodes applied by selection)
         {
             const int64_t* ax = A.axis + W.axis_off;
+            const uint32_t nmax = __reduce_max_sync(0xffffffffu, G.dn_ops);
             for (uint32_t j = 0; j <= G.degree; ++j) {
                 const int64_t s = (int64_t)g.s0 + j;
                 for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = ax[0 + 4 * a] + s * ax[2 + 4 * a];
-                interp_i64(A.code + G.dop_off, G.dn_ops, rf, A.consts + G.c_off, axv, s, outv, lane);
+                interp_i64_lanes(A.code + G.dop_off, G.dn_ops, nmax, rf, A.consts + G.c_off, axv, s, outv, lane);
 #pragma unroll
                 for (int i = 0; i < NS; ++i) stage[(j * NS + i) * 32 + lane] = outv[i * 32 + lane];
             }
@@ -1007,10 +1007,11 @@ __global__ void __launch_bounds__(256) k_shadow_split(const ShadowArgs A) {
         // (as in k_shadow_intfd)
         {
             const int64_t* ax = A.axis + W.axis_off;
+            const uint32_t nmax = __reduce_max_sync(0xffffffffu, G.dn_ops);
             for (uint32_t j = 0; j <= G.degree; ++j) {
                 const int64_t s = j;
                 for (uint32_t a = 0; a < G.dim; ++a) axv[a * 32 + lane] = ax[0 + 4 * a] + s * ax[2 + 4 * a];
-                interp_i64(A.code + G.dop_off, G.dn_ops, rf, A.consts + G.c_off, axv, s, outv, lane);
+                interp_i64_lanes(A.code + G.dop_off, G.dn_ops, nmax, rf, A.consts + G.c_off, axv, s, outv, lane);
 #pragma unroll
                 for (int i = 0; i < NS; ++i) stage[(j * NS + i) * 32 + lane] = outv[i * 32 + lane];
             }

@@ -227,8 +227,9 @@ int dr_batch_destroy(int32_t batch);
  * and shadow_buffer_mb fields are inputs); a candidate replaces the built-in
  * policy only when it is at least 2% faster, since shorter chunks cost host
  * build time on every batch.  With the chosen shape it then tries packing
- * the integer-difference shadow chains of depth <= 2, 3, 4 or 16 two warps
- * per scheduler (chain_pack_depth), kept by the same 2% rule.  The choice is remembered for the
+ * the integer-difference shadow chains of depth <= 1, 2, 3, 4 or 16 two
+ * warps per scheduler (chain_pack_depth), kept when at least 1% faster
+ * (packing costs the host nothing).  The choice is remembered for the
  * workload's shape (per launch class: log2 of the (walk, prime block) count
  * and of their steps, longest walk), so later batches of that shape built
  * with a zero chunk_steps and warps_per_block use it.  No reference
