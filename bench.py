@@ -380,11 +380,41 @@ def bench_rational(stream, torch):
     ms = _time_batch(batch, stream, torch)
     st = batch.stats()
     pl = batch.read_pipeline()
+    groups = _launch_groups(batch)
     batch.close()
     return {"walks": len(reqs), "prime_steps": st["prime_steps"], "ms": ms,
             "prime_steps_per_s": st["prime_steps"] / (ms * 1e-3), "launches": st["launches"],
             "autotuned": tuned,
+            "launch_groups": groups,
+            "span_ms_eager": max((g["end_ms"] for g in groups), default=None),
+            "walks_end_ms": max((g["end_ms"] for g in groups if g["kind"] == "walk"), default=None),
+            "shadows_end_ms": max((g["end_ms"] for g in groups if g["kind"] != "walk"), default=None),
             "top1_delta": float(pl["topk_val"][0]) if len(pl["topk_val"]) else None}
+
+
+def _launch_groups(batch):
+    """Balance across a batch's launch groups (one persistent launch per
+    class, m and difference depth, each on its own stream): every group's
+    span in one eager run of the batch (dr_debug_batch_timeline, ms after the
+    first launch; an interpreted shadow's span runs from its evaluation to
+    the end of its chain) beside its time alone (dr_batch_profile)."""
+    import ctypes
+    import numpy as np
+    from dreams_rns import _native as N
+    prof = batch.profile()
+    cnt = ctypes.c_int32()
+    spans = np.zeros(4 * 64, dtype=np.float32)
+    N.check(N.lib().dr_debug_batch_timeline(batch.handle, 64, ctypes.byref(cnt), N.ptr(spans)),
+            "dr_debug_batch_timeline")
+    kinds = {0: "walk", 1: "shadow (interpreted or split)", 2: "shadow (integer differences)"}
+    out = []
+    for i, p in enumerate(prof[:cnt.value]):
+        s = [float(x) for x in spans[4 * i:4 * i + 4]]
+        out.append({"kind": kinds.get(p["kind"], str(p["kind"])), "m": p["m"], "degree": p["degree"],
+                    "items": p["items"],
+                    "alone_ms": round(p["ms"] + (p["ms2"] if p["kind"] == 1 else 0.0), 3),
+                    "start_ms": round(s[0], 3), "end_ms": round(max(s[1], s[3]), 3)})
+    return out
 
 
 def bench_crt_stage(torch, n=1 << 20, reps=5):
