@@ -155,10 +155,10 @@ __device__ __forceinline__ void interp_f64(const uint4* __restrict__ code, uint3
 // different walks, whose programs differ in their op sequences).  Every lane
 // fetches its own instruction and the opcode selects the result and its
 // destination instead of a jump, so the warp stays converged however the
-// programs differ.  nmax = the warp's
-// longest program; a lane past its own n writes nothing.  Operand rows are
-// read at row 0 where the opcode has no such operand, so every access stays
-// inside the register file and axis rows.  The instructions (and the
+// programs differ.  nmax = the warp's longest program; a lane past its own n
+// writes nothing.  Operand rows are read at row 0 where the opcode has no
+// such operand, so every access stays inside the register file and axis
+// rows.  The instructions (and the
 // constants they load) come in batches of kBatch independent loads: with the
 // chain kernels' shared memory taking most of the SM, the lanes' 32 programs
 // do not stay in L1, and one fetch at a time waited on L2 for every op.
