@@ -2279,8 +2279,11 @@ int dr_autotune(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
     }
     // then two chain warps per scheduler for the integer-difference shadows of
     // depth up to d: worth it when those chains end before the walks do.
-    // Packing costs the host nothing, so 1% (above the replays' spread of
-    // ~0.5% for a best of 3) is enough to keep it
+    // Every depth is timed and the fastest kept if it beats no packing by 1%
+    // (above the replays' spread of ~0.5% for a best of 3; packing costs the
+    // host nothing)
+    dr_tune pt = bt;
+    float pms = bms;
     for (uint32_t d : {1u, 2u, 3u, 4u, 16u}) {
         dr_tune cand = bt;
         cand.chain_pack_depth = d;
@@ -2288,8 +2291,9 @@ int dr_autotune(const dr_walk_desc* walks, int32_t n_walks, const uint8_t* blobs
         rc = time_one(cand, &ms, nullptr, nullptr);
         if (rc == DR_ERR_UNSUPPORTED) continue;
         if (rc) return rc;
-        if (ms < 0.99f * bms) { bms = ms; bt = cand; }
+        if (ms < pms) { pms = ms; pt = cand; }
     }
+    if (pms < 0.99f * bms) { bms = pms; bt = pt; }
     {
         std::lock_guard<std::mutex> lk(C.cache_mu);
         C.tuned[sig] = {bt.chunk_steps, bt.warps_per_block, bt.chain_pack_depth};

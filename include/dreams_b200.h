@@ -228,12 +228,13 @@ int dr_batch_destroy(int32_t batch);
  * policy only when it is at least 2% faster, since shorter chunks cost host
  * build time on every batch.  With the chosen shape it then tries packing
  * the integer-difference shadow chains of depth <= 1, 2, 3, 4 or 16 two
- * warps per scheduler (chain_pack_depth), kept when at least 1% faster
- * (packing costs the host nothing).  The choice is remembered for the
- * workload's shape (per launch class: log2 of the (walk, prime block) count
- * and of their steps, longest walk), so later batches of that shape built
- * with a zero chunk_steps and warps_per_block use it.  No reference
- * counterpart (the reference fixes its launch shape, persistent_kernel.cu:877-888). */
+ * warps per scheduler (chain_pack_depth) and keeps the fastest when it is
+ * at least 1% faster than no packing (packing costs the host nothing).
+ * The choice is remembered for the workload's shape (per launch class:
+ * log2 of the (walk, prime block) count and of their steps, longest walk),
+ * so later batches of that shape built with a zero chunk_steps and
+ * warps_per_block use it.  No reference counterpart (the reference fixes its
+ * launch shape, persistent_kernel.cu:877-888). */
 int dr_autotune(const dr_walk_desc *walks, int32_t n_walks, const uint8_t *blobs,
                 const uint64_t *blob_offsets, int32_t n_programs, const int64_t *axis_params,
                 uint64_t n_axis_params, dr_tune *best, float *best_ms);
